@@ -1,0 +1,293 @@
+/*
+ * ngb.h -- C ABI of the B200-native batched multi-world sensor renderer.
+ *
+ * One renderer holds world_count worlds. Every world holds the same list of mesh instances, placed
+ * differently, and is seen by cameras_per_world cameras of width x height pixels. A camera only sees
+ * its own world's instances. This is the drop-in for the reference's batched path:
+ *
+ *   reference (C++)                                      this ABI
+ *   BatchRenderer::BatchRenderer   include/neraulgraphics/batch.h:65-68   ngb_create
+ *   detail::make_cuda_backend      src/backend.h:88                       ngb_create
+ *   BatchRenderer::set_instance_transforms  batch.h:79, backend.h:62      ngb_set_instance_transforms
+ *   BatchRenderer::bind_bodies     batch.h:84, backend.h:63               ngb_bind_bodies
+ *   BatchRenderer::set_body_poses  batch.h:90, backend.h:65               ngb_set_body_poses
+ *   BatchRenderer::render          batch.h:103-104, backend.h:67-68       ngb_render / ngb_render_into
+ *   BatchRenderer::render_host     batch.h:105-106                        ngb_render_host
+ *   BatchRenderer::cast_rays       batch.h:110-111, backend.h:69-70       ngb_cast_rays
+ *   Backend::copy_to_host          backend.h:54                           ngb_copy_to_host
+ *   BatchRenderer::last_kernel_ms  batch.h:123, backend.h:83              ngb_last_kernel_ms
+ *   BatchRenderer::set_ambient     batch.h:126                            ngb_set_ambient
+ *   BatchRenderer::set_environment batch.h:129 (gradient sky only)        ngb_set_environment
+ *   accessors                      batch.h:115-122                        ngb_width ... ngb_instances_per_world
+ *
+ * Every entry point returns a status: NGB_OK, or an error whose message ngb_last_error() gives.
+ * Validation runs before any state changes, so a rejected call leaves the renderer as it was
+ * (include/neraulgraphics/renderer.h:14-15). The messages of rejected input are the reference's
+ * (src/batch.cpp, src/validate.cpp, src/mesh_build.cpp).
+ *
+ * Pointers marked "in memory" are host pointers for NGB_MEMORY_HOST and CUDA device pointers for
+ * NGB_MEMORY_DEVICE. Host input is checked (finite, invertible); device input is trusted, as in the
+ * reference (batch.h:75-78). Device input is read on the renderer's stream.
+ *
+ * Completion: by default every call that launches work waits for it (with a bounded wait, after which
+ * it returns NGB_TIMEOUT) before returning, as the reference does. ngb_set_sync(h, 0, ...) makes calls
+ * stream-ordered instead: they return once the work is queued on the renderer's stream.
+ *
+ * All types here are plain C: no CUDA or C++ types cross this boundary.
+ */
+#ifndef NGB_H
+#define NGB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define NGB_OK 0
+#define NGB_INVALID_ARGUMENT 1 /* std::invalid_argument in the reference */
+#define NGB_CUDA_ERROR 2       /* neraulgraphics::CudaError (include/neraulgraphics/renderer.h:32-39) */
+#define NGB_TIMEOUT 3          /* a bounded wait on the device ran out */
+#define NGB_LOGIC_ERROR 4      /* std::logic_error: a null or destroyed renderer (src/batch.cpp:81-89) */
+
+/* Where an array lives (include/neraulgraphics/renderer.h:49). */
+#define NGB_MEMORY_HOST 0
+#define NGB_MEMORY_DEVICE 1
+
+/* Which images render() produces (include/neraulgraphics/renderer.h:53-58). */
+#define NGB_OUTPUT_RGB 1u
+#define NGB_OUTPUT_DEPTH 2u
+#define NGB_OUTPUT_NORMAL 4u
+#define NGB_OUTPUT_OBJECT_ID 8u
+
+/* Object IDs (include/neraulgraphics/scene.h:19-22). */
+#define NGB_MAX_SPHERES 32
+#define NGB_MAX_LIGHTS 8
+#define NGB_OBJECT_NONE 0
+#define NGB_OBJECT_SPHERE 1
+#define NGB_OBJECT_FLOOR (NGB_OBJECT_SPHERE + NGB_MAX_SPHERES)
+#define NGB_OBJECT_INSTANCE (NGB_OBJECT_FLOOR + 1)
+
+typedef struct {
+    float x, y, z;
+} ngb_vec3;
+
+/* Same fields, order and meaning as neraulgraphics::Material (include/neraulgraphics/scene.h:35-56). */
+typedef struct {
+    ngb_vec3 diffuse_color;
+    float diffuse_albedo;
+    float specular_albedo;
+    float reflectivity;
+    float specular_exponent;
+    float roughness;
+    float metallic;
+    ngb_vec3 emission;
+    float transmission;
+    float ior;
+} ngb_material;
+
+/* neraulgraphics::Sphere (scene.h:63-67). */
+typedef struct {
+    ngb_vec3 center;
+    float radius;
+    ngb_material material;
+} ngb_sphere;
+
+/* neraulgraphics::Light (scene.h:82-92). */
+typedef struct {
+    ngb_vec3 position;
+    float intensity;
+    float radius;
+    float falloff;
+    ngb_vec3 direction;
+    float spot_angle;
+    float spot_softness;
+    ngb_vec3 color;
+} ngb_light;
+
+/* neraulgraphics::Plane (scene.h:96-103). half_extent_x 0 is no floor. */
+typedef struct {
+    float y;
+    float half_extent_x;
+    float z_min;
+    float z_max;
+    float checker_scale;
+    ngb_material material;
+} ngb_plane;
+
+/* neraulgraphics::Mesh (include/neraulgraphics/mesh.h:160-171) without uvs: vertex_count x 3 floats,
+ * index_count uint32 (3 per triangle), and optionally vertex_count x 3 normals (NULL for none). */
+typedef struct {
+    const float *vertices;
+    int32_t vertex_count;
+    const uint32_t *indices;
+    int32_t index_count;
+    const float *normals;
+} ngb_mesh;
+
+/* neraulgraphics::Instance (mesh.h:207-222) without textures. transform: the top three rows of the
+ * 4x4, row-major (mesh.h:193-198). */
+typedef struct {
+    int32_t mesh;
+    float transform[12];
+    ngb_material material;
+} ngb_instance;
+
+/* The gradient sky of neraulgraphics::Environment (scene.h:109-121); maps are not supported. */
+typedef struct {
+    ngb_vec3 up;
+    ngb_vec3 color_up;
+    ngb_vec3 color_down;
+    float intensity;
+} ngb_environment;
+
+/* Everything BatchRenderer's constructor takes (batch.h:65-68), as plain data. */
+typedef struct {
+    int32_t width;
+    int32_t height;
+    int32_t world_count;
+    int32_t cameras_per_world;
+    const ngb_sphere *spheres;
+    int32_t sphere_count;
+    const ngb_light *lights;
+    int32_t light_count;
+    ngb_plane floor;
+    const ngb_mesh *meshes;
+    int32_t mesh_count;
+    const ngb_instance *instances; /* what one world holds */
+    int32_t instance_count;
+    int32_t device; /* CUDA device ordinal */
+} ngb_scene;
+
+/* neraulgraphics::BatchFrame (batch.h:27-37): the renderer's own buffers, valid until the next render. */
+typedef struct {
+    int32_t memory;
+    int32_t device_id;
+    int32_t views;
+    int32_t width;
+    int32_t height;
+    const uint8_t *rgb;
+    const float *depth;
+    const float *normal;
+    const int32_t *object_id;
+} ngb_batch_frame;
+
+/* neraulgraphics::RayHits (renderer.h:88-95): the renderer's own buffers, valid until the next ray query. */
+typedef struct {
+    int32_t memory;
+    int32_t device_id;
+    int32_t count;
+    const float *distance;
+    const float *normal;
+    const int32_t *object_id;
+} ngb_ray_hits;
+
+typedef struct ngb_renderer ngb_renderer;
+
+/* ---- lifetime -------------------------------------------------------------------------------------- */
+
+/* Builds the meshes' trees on the host, uploads them, and places every world's instances where the
+ * scene says. Replaces BatchRenderer::BatchRenderer (src/batch.cpp:47-75) with Device::Cuda and
+ * CudaBackend::CudaBackend (src/cuda_backend.cu:327-363). On failure *out is NULL and
+ * ngb_last_error(NULL) says why. */
+int ngb_create(const ngb_scene *scene, ngb_renderer **out);
+void ngb_destroy(ngb_renderer *r);
+
+/* The message of the last failed call on r, or of the last failed ngb_create on this thread when r is
+ * NULL. Empty after a success. */
+const char *ngb_last_error(const ngb_renderer *r);
+
+/* ---- placing the instances ------------------------------------------------------------------------- */
+
+/* world_count * instances_per_world matrices of 12 floats, world-major, in memory. Rebuilds every
+ * world's tree over its instances on the GPU. Replaces BatchRenderer::set_instance_transforms
+ * (src/batch.cpp:91-109) and CudaBackend::set_instance_matrices (src/cuda_backend.cu:457-469). */
+int ngb_set_instance_transforms(ngb_renderer *r, const float *matrices, int32_t memory);
+
+/* How simulator bodies carry the instances: per instance of a world, its body (-1 for none), its pose
+ * on the body (x, y, z, qx, qy, qz, qw) and its scale (x, y, z). Host arrays. Replaces
+ * BatchRenderer::bind_bodies (src/batch.cpp:111-129, src/cuda_backend.cu:472-491). */
+int ngb_bind_bodies(ngb_renderer *r, int32_t bodies_per_world, const int32_t *body_of_instance, const float *local_pose,
+    const float *scale);
+
+/* world_count * bodies_per_world poses of 7 floats, world-major, in memory. Composes every instance's
+ * matrix and rebuilds the trees, in one launch. Replaces BatchRenderer::set_body_poses
+ * (src/batch.cpp:131-144) and CudaBackend::set_body_poses (src/cuda_backend.cu:493-507). */
+int ngb_set_body_poses(ngb_renderer *r, const float *body_poses, int32_t memory);
+
+/* ---- rendering ------------------------------------------------------------------------------------- */
+
+/* Renders every view into the renderer's own device buffers, described in *out. view_count cameras of
+ * 12 floats (camera-to-world, OpenGL convention) in camera_memory. Replaces BatchRenderer::render
+ * (src/batch.cpp:146-162) and CudaBackend::render_batch (src/cuda_backend.cu:509-545). */
+int ngb_render(ngb_renderer *r, const float *camera_matrices, float fov, int32_t samples_per_pixel, uint32_t outputs,
+    int32_t frame, int32_t camera_memory, ngb_batch_frame *out);
+
+/* The same, writing into caller-owned device buffers (views x H x W x {3 u8, 1 f32, 3 f32, 1 i32}); a
+ * buffer may be NULL when its output is not asked for. For callers that own the memory, such as a
+ * framework's tensors. */
+int ngb_render_into(ngb_renderer *r, const float *camera_matrices, float fov, int32_t samples_per_pixel,
+    uint32_t outputs, int32_t frame, int32_t camera_memory, uint8_t *rgb, float *depth, float *normal,
+    int32_t *object_id);
+
+/* Renders from host cameras and copies the images into caller-owned host buffers. Replaces
+ * BatchRenderer::render_host (src/batch.cpp:164-178). */
+int ngb_render_host(ngb_renderer *r, const float *camera_matrices, float fov, int32_t samples_per_pixel,
+    uint32_t outputs, int32_t frame, uint8_t *rgb, float *depth, float *normal, int32_t *object_id);
+
+/* rays_per_world rays in every world (world-major, 3 floats each), in memory. Replaces
+ * BatchRenderer::cast_rays (src/batch.cpp:180-192) and CudaBackend::cast_rays_batch
+ * (src/cuda_backend.cu:547-585). */
+int ngb_cast_rays(ngb_renderer *r, const float *origins, const float *directions, int32_t rays_per_world,
+    float max_distance, int32_t memory, ngb_ray_hits *out);
+
+/* Copies bytes from one of the renderer's device arrays into host memory (src/backend.h:54). */
+int ngb_copy_to_host(ngb_renderer *r, const void *src, void *dst, size_t bytes);
+
+/* ---- settings ---------------------------------------------------------------------------------------- */
+
+int ngb_set_ambient(ngb_renderer *r, float ambient);      /* src/batch.cpp:230-233 */
+float ngb_ambient(const ngb_renderer *r);
+int ngb_set_environment(ngb_renderer *r, const ngb_environment *environment); /* src/batch.cpp:224-227 */
+
+/* The stream every later call queues its work on (a cudaStream_t; NULL for the renderer's own). */
+int ngb_set_stream(ngb_renderer *r, void *cuda_stream);
+/* synchronous 1: calls wait for their work, at most timeout_seconds (NGB_TIMEOUT after that).
+ * synchronous 0: calls return once the work is queued. */
+int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
+/* Waits for every call queued so far, at most timeout_seconds. */
+int ngb_synchronize(ngb_renderer *r, double timeout_seconds);
+
+/* ---- accessors (batch.h:115-123) ------------------------------------------------------------------- */
+
+int32_t ngb_width(const ngb_renderer *r);
+int32_t ngb_height(const ngb_renderer *r);
+int32_t ngb_world_count(const ngb_renderer *r);
+int32_t ngb_cameras_per_world(const ngb_renderer *r);
+int32_t ngb_view_count(const ngb_renderer *r);
+int32_t ngb_instances_per_world(const ngb_renderer *r);
+/* GPU time of the last render or ray query, from CUDA events around its launch (cuda_backend.cu:537-543). */
+float ngb_last_kernel_ms(const ngb_renderer *r);
+
+/* ---- inspection, for parity checks ------------------------------------------------------------------ */
+
+/* Copies the last tree build to host arrays (any may be NULL): the sort keys (world << 32 | Morton
+ * code) in instance order, the instance ids in sorted order, the 2n-1 nodes as 8 words each (lo xyz,
+ * left, hi xyz, right: the layout of bvh::TlasNode, src/bvh.h:44-49), the per-world roots, and the
+ * instance matrices (12 floats each). n = world_count * instances_per_world. */
+int ngb_inspect_tlas(ngb_renderer *r, uint64_t *keys, int32_t *sorted_ids, int32_t *nodes, int32_t *roots,
+    float *matrices);
+
+/* Per pixel of the last render's centre (depth/normal/ID) rays: the instance hit (over all worlds, -1
+ * for none), the triangle hit (its index in its mesh's own list, -1 for none) and the barycentrics u, v.
+ * Host arrays of view_count * height * width; any may be NULL. Only filled by renders that asked for
+ * NGB_OUTPUT_DEPTH, NGB_OUTPUT_NORMAL or NGB_OUTPUT_OBJECT_ID. */
+int ngb_inspect_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *u, float *v);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NGB_H */

@@ -1,0 +1,147 @@
+"""Seeded synthetic scenes for the batched sensor-rendering path.
+
+The reference benchmarks on recorded simulator poses that are not available offline, so these seeded
+scenes stand in for them, with the sizes and value distributions of the workloads the path is measured
+on. Every generator is deterministic in its seed (numpy's default_rng).
+
+- `icosphere_worlds`: 16 worlds at 64x64, each a floor and 8 icospheres (320 triangles) placed by matrices.
+- `body_worlds`: 4096 worlds at 64x64, 20 simulator bodies each carrying one instance of three shared
+  meshes (icosphere 1280, box 12, capped cylinder 512 triangles), moved by a Gaussian random walk.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .scene import (Instance, Light, Material, Plane, SceneDesc, cylinder, make_box, make_camera, make_icosphere,
+                    make_transform)
+
+LIGHT = Light((-10.0, 20.0, 10.0), 1.6, 1.0)
+
+
+@dataclass
+class Workload:
+    name: str
+    desc: SceneDesc
+    cameras: np.ndarray                      # (views, 3, 4) float32
+    fov: float = 1.0
+    spp: int = 1
+    rgb: bool = True
+    depth: bool = True
+    normals: bool = False
+    object_ids: bool = True
+    matrices: np.ndarray | None = None       # (worlds, per_world, 3, 4) when placed by matrices
+    binding: dict | None = None              # bind_bodies arguments when placed by bodies
+    poses: np.ndarray | None = None          # (worlds, bodies, 7) initial body poses
+    info: dict = field(default_factory=dict)
+
+
+def uniform_quaternions(rng, n) -> np.ndarray:
+    """n unit quaternions (x, y, z, w), uniform on S^3: normalised 4-d Gaussians."""
+    q = rng.normal(size=(n, 4))
+    return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+def camera_matrix(position, target, width, height, fov) -> np.ndarray:
+    return make_camera(position, target, width=width, height=height, fov=fov).matrix
+
+
+def icosphere_worlds(worlds=16, per_world=8, width=64, height=64, seed=0) -> Workload:
+    """16 worlds x 8 icospheres (subdivision 2, radius 0.5) over a floor, placed by matrices.
+
+    Floor y = -2, half-extent 12 in x, z in (-30, -2), no checker. Per instance: position U[-2, 2]^3 + (0, 0, -6),
+    rotation uniform on S^3, uniform scale U[0.5, 1.5]. One camera per world at (0, 1, 0) + U[-0.2, 0.2]^3 aimed at
+    (0, 0, -6); fov 1.0 rad. One light at (-10, 20, 10), intensity 1.6, radius 1.0. Reflectivity 0.
+    """
+    rng = np.random.default_rng(seed)
+    meshes = [make_icosphere(0.5, 2)]
+    instances = [Instance(0, material=Material()) for _ in range(per_world)]
+    floor = Plane(y=-2.0, half_extent_x=12.0, z_min=-30.0, z_max=-2.0, checker_scale=0.0)
+    desc = SceneDesc(width, height, worlds, 1, lights=[LIGHT], floor=floor, meshes=meshes, instances=instances)
+    mats = np.empty((worlds, per_world, 3, 4), np.float32)
+    for w in range(worlds):
+        pos = rng.uniform(-2.0, 2.0, size=(per_world, 3)) + np.array([0.0, 0.0, -6.0])
+        q = uniform_quaternions(rng, per_world)
+        sc = rng.uniform(0.5, 1.5, size=per_world)
+        for i in range(per_world):
+            mats[w, i] = make_transform(pos[i], q[i], sc[i]).matrix
+    cams = np.empty((worlds, 3, 4), np.float32)
+    for w in range(worlds):
+        eye = np.array([0.0, 1.0, 0.0]) + rng.uniform(-0.2, 0.2, size=3)
+        cams[w] = camera_matrix(eye, (0.0, 0.0, -6.0), width, height, 1.0)
+    return Workload("icosphere_worlds", desc, cams, 1.0, 1, matrices=mats,
+                    info={"worlds": worlds, "per_world": per_world, "width": width, "height": height, "seed": seed,
+                          "triangles_per_instance": 320})
+
+
+PALETTE = [(0.80, 0.25, 0.20), (0.20, 0.55, 0.80), (0.25, 0.70, 0.30), (0.85, 0.75, 0.20), (0.60, 0.30, 0.75),
+           (0.90, 0.50, 0.15), (0.30, 0.75, 0.70), (0.75, 0.75, 0.75)]
+
+
+def body_worlds(worlds=4096, bodies=20, width=64, height=64, seed=0) -> Workload:
+    """4096 worlds x 20 bodies, one instance per body, of three shared meshes.
+
+    Meshes: icosphere radius 0.5 subdivision 3 (1280 triangles), box of half-extent 0.4 (12), capped cylinder
+    radius 1 half-height 1 with 128 segments (512). Instance i uses mesh i % 3 and sits on body i with a
+    local offset U[-0.1, 0.1]^3 and a random local rotation; scale: icospheres U[0.6, 1.2] (uniform), boxes
+    U[0.6, 1.2]^3, cylinders (0.3, 0.3, 0.5) * U[0.8, 1.2]. Initial body positions U[-2, 2]^3, rotations
+    uniform on S^3. Floor y = -2.5, half-extent 8, z in (-8, 8), checker 1. Cameras: one per world on a
+    ring of radius 4 at height 1.0, world w at angle 2 pi w / worlds, looking at the origin; fov 1.0 rad.
+    Light as in icosphere_worlds. Outputs RGB, depth and object IDs, 1 sample per pixel.
+    """
+    rng = np.random.default_rng(seed)
+    meshes = [make_icosphere(0.5, 3), make_box((0.4, 0.4, 0.4)), cylinder(1.0, 1.0, 128)]
+    instances = [Instance(i % 3, material=Material(diffuse_color=PALETTE[i % len(PALETTE)])) for i in range(bodies)]
+    floor = Plane(y=-2.5, half_extent_x=8.0, z_min=-8.0, z_max=8.0, checker_scale=1.0)
+    desc = SceneDesc(width, height, worlds, 1, lights=[LIGHT], floor=floor, meshes=meshes, instances=instances)
+    local = np.zeros((bodies, 7), np.float32)
+    local[:, :3] = rng.uniform(-0.1, 0.1, size=(bodies, 3))
+    local[:, 3:] = uniform_quaternions(rng, bodies)
+    scale = np.zeros((bodies, 3), np.float32)
+    for i in range(bodies):
+        if i % 3 == 0:
+            scale[i] = rng.uniform(0.6, 1.2)
+        elif i % 3 == 1:
+            scale[i] = rng.uniform(0.6, 1.2, size=3)
+        else:
+            scale[i] = np.array([0.3, 0.3, 0.5]) * rng.uniform(0.8, 1.2)
+    binding = dict(body_of_instance=np.arange(bodies, dtype=np.int32), local_pose=local, scale=scale,
+                   bodies_per_world=bodies)
+    poses = np.zeros((worlds, bodies, 7), np.float32)
+    poses[..., :3] = rng.uniform(-2.0, 2.0, size=(worlds, bodies, 3))
+    poses[..., 3:] = uniform_quaternions(rng, worlds * bodies).reshape(worlds, bodies, 4)
+    cams = np.empty((worlds, 3, 4), np.float32)
+    for w in range(worlds):
+        a = 2.0 * np.pi * w / worlds
+        cams[w] = camera_matrix((4.0 * np.cos(a), 1.0, 4.0 * np.sin(a)), (0.0, 0.0, 0.0), width, height, 1.0)
+    return Workload("body_worlds", desc, cams, 1.0, 1, binding=binding, poses=poses,
+                    info={"worlds": worlds, "bodies": bodies, "width": width, "height": height, "seed": seed,
+                          "triangles": [1280, 12, 512]})
+
+
+def quat_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Hamilton product of (..., 4) quaternions stored (x, y, z, w)."""
+    ax, ay, az, aw = np.moveaxis(a, -1, 0)
+    bx, by, bz, bw = np.moveaxis(b, -1, 0)
+    return np.stack([aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+                     aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz], axis=-1)
+
+
+def random_walk(poses: np.ndarray, steps: int, seed=1, sigma_pos=0.02, sigma_rot=0.05) -> np.ndarray:
+    """(steps, worlds, bodies, 7): each step adds N(0, sigma_pos^2) to every position and turns every body by an
+    angle N(0, sigma_rot^2) about a random unit axis (q <- q * dq)."""
+    rng = np.random.default_rng(seed)
+    cur = poses.astype(np.float64).copy()
+    out = np.empty((steps,) + poses.shape, np.float32)
+    for s in range(steps):
+        cur[..., :3] += rng.normal(0.0, sigma_pos, size=cur[..., :3].shape)
+        axis = rng.normal(size=cur[..., :3].shape)
+        axis /= np.linalg.norm(axis, axis=-1, keepdims=True)
+        ang = rng.normal(0.0, sigma_rot, size=cur.shape[:-1] + (1,))
+        dq = np.concatenate([axis * np.sin(ang / 2), np.cos(ang / 2)], axis=-1)
+        q = quat_mul(cur[..., 3:], dq)
+        cur[..., 3:] = q / np.linalg.norm(q, axis=-1, keepdims=True)
+        out[s] = cur
+    return out
