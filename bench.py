@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the batched sensor-rendering path: images/s at 4096 worlds x 64x64, RGB + depth + object ID.
+
+One step = one simulation step of the workload: every body of every world moves (a seeded Gaussian random
+walk), the instance matrices are composed and every world's tree is rebuilt (set_body_poses), then every
+view is rendered (render). Scenes are seeded synthetic stand-ins for recorded simulator poses
+(neraulgraphics_b200.workloads.body_worlds).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU: each rank renders its own 4096 worlds (weak scaling, no
+collective on the data path); the time is the max over ranks.
+
+value: device-resident inputs (poses and cameras already on the GPU), CUDA events per step, L2 flushed
+between steps. e2e: the public API with host buffers: pinned host poses in, images copied back to pinned
+host memory, every step. --impl reference times the reference's own CPU backend (compiled from its sources
+into oracle/_ref/) on a bounded sample of worlds per step, with every host core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "images/s at 4096x64x64 RGB+depth+ID (body poses -> LBVH rebuild -> render, per step)"
+UNIT = "images/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--worlds", type=int, default=4096)
+    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-reference-cuda", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(worlds, extra=None):
+    cfg = {"workload": f"body_worlds: {worlds} worlds x 20 bodies (icosphere 1280 / box 12 / cylinder 512 tris), "
+                       f"64x64, 1 light (soft shadows), spp 1, RGB+depth+ID, random-walk poses every step",
+           "worlds_per_gpu": worlds, "width": 64, "height": 64, "instances_per_world": 20}
+    cfg.update(extra or {})
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_image():
+    """DRAM bytes per image of the render kernel, from the committed ncu summary (or None)."""
+    path = os.path.join(ROOT, "profiles", "render_kernel_body_worlds.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_image:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def render_algorithmic_bytes(wl, per_world, blas_bytes):
+    """Compulsory bytes of one render launch: outputs, cameras, each world's tree and instance records, and the
+    shared meshes once."""
+    d = wl.desc
+    views = d.view_count
+    out = views * d.height * d.width * (3 + 4 + 4)
+    cams = views * 48
+    trees = d.world_count * ((2 * per_world - 1) * 32 + per_world * 64)
+    return out + cams + trees + blas_bytes
+
+
+def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64):
+    """The reference's own CPU backend (oracle/_ref/libngref.so) on the first sample_worlds worlds of the
+    workload, every host core: images/s."""
+    import oracle as O
+    from neraulgraphics_b200.scene import SceneDesc
+    if not O.reference_available():
+        return None
+    d = wl.desc
+    desc = SceneDesc(d.width, d.height, sample_worlds, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    cores = os.cpu_count() or 1
+    ref = O.Reference(desc, threads=cores)
+    ref.bind_bodies(**wl.binding)
+    cams = wl.cameras[:sample_worlds]
+    ref.set_body_poses(steps_poses[0][:sample_worlds])
+    ref.render(cams, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        ref.set_body_poses(steps_poses[(n + 1) % len(steps_poses)][:sample_worlds])
+        ref.render(cams, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    return {"value": sample_worlds * n / el, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{n} steps of {sample_worlds} of the {d.world_count} worlds (set_body_poses + render_host, "
+                      f"RGB+depth+ID), NERAULGRAPHICS_THREADS={cores}, {el:.1f} s"}
+
+
+def reference_cuda(wl, torch, poses_dev, cams_dev, steps, warmup):
+    """The reference's own CUDA backend (src/cuda_backend.cu built for sm_100 with its flags) on the same
+    workload and the same device-resident inputs: images/s, CUDA events on its (legacy default) stream."""
+    import oracle as O
+    if not O.reference_available(cuda=True):
+        return None
+    ref = O.Reference(wl.desc, cuda=True)
+    ref.bind_bodies(**wl.binding)
+    outputs = 1 | 2 | 8
+    for s in range(warmup):
+        ref.set_body_poses(poses_dev[s].data_ptr(), device=True)
+        ref.render_device(cams_dev.data_ptr(), wl.fov, 1, outputs)
+    torch.cuda.synchronize()
+    stream = torch.cuda.default_stream()
+    times = []
+    for s in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ref.set_body_poses(poses_dev[warmup + s].data_ptr(), device=True)
+        ref.render_device(cams_dev.data_ptr(), wl.fov, 1, outputs)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    return {"value": wl.desc.view_count / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+            "kernel_ms_render": ref.last_kernel_ms,
+            "what": "neraulgraphics 0.5.0 CudaBackend (set_body_poses + render_batch, RGB+depth+ID), sm_100, "
+                    "-use_fast_math, same inputs on the device, median step"}
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import torch
+
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    wl = workloads.body_worlds(worlds=args.worlds, seed=rank)
+    steps_np = workloads.random_walk(wl.poses, W + K, seed=1 + rank)
+    d = wl.desc
+    r = ng.BatchRenderer(d.width, d.height, d.world_count, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances,
+                         device=dev)
+    r.bind_bodies(**wl.binding)
+    poses_dev = torch.from_numpy(steps_np).to(dev)
+    cams_dev = torch.from_numpy(wl.cameras).to(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
+    for s in range(W):
+        r.set_body_poses(poses_dev[s])
+        r.render(cams_dev, wl.fov, 1, **kw)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    with ClockSampler(local_rank) as clocks:
+        for s in range(K):
+            flush.zero_()
+            e0, e1, e2 = ev[s]
+            e0.record()
+            r.set_body_poses(poses_dev[W + s])
+            e1.record()
+            r.render(cams_dev, wl.fov, 1, **kw)
+            e2.record()
+        torch.cuda.synchronize()
+    build_ms = [a.elapsed_time(b) for a, b, _ in ev]
+    render_ms = [b.elapsed_time(c) for _, b, c in ev]
+    total_ms = sum(build_ms) + sum(render_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    views = d.view_count
+    value = world * views * K / (total_ms / 1000.0)
+
+    # End to end through the public API with host buffers.
+    pinned_poses = torch.from_numpy(steps_np).pin_memory().numpy()
+    out = {"rgb": torch.empty((views, 64, 64, 3), dtype=torch.uint8).pin_memory().numpy(),
+           "depth": torch.empty((views, 64, 64), dtype=torch.float32).pin_memory().numpy(),
+           "object_ids": torch.empty((views, 64, 64), dtype=torch.int32).pin_memory().numpy()}
+    hkw = dict(rgb=True, depth=True, object_ids=True, out=out)
+    KE = max(1, min(args.e2e_steps, K))
+    for s in range(2):
+        r.set_body_poses(pinned_poses[s])
+        r.render(wl.cameras, wl.fov, 1, **hkw)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for s in range(KE):
+        r.set_body_poses(pinned_poses[W + s % K])
+        r.render(wl.cameras, wl.fov, 1, **hkw)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * views * KE / e2e_s
+    h2d = pinned_poses[0].nbytes + wl.cameras.nbytes
+    d2h = sum(a.nbytes for a in out.values())
+
+    ref_cuda = cpu = None
+    if rank == 0 and not args.no_reference_cuda:
+        try:
+            ref_cuda = reference_cuda(wl, torch, poses_dev, cams_dev, min(K, 10), min(W, 3))
+        except Exception as e:  # reported, not fatal: the comparison arm is optional
+            ref_cuda = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(wl, steps_np, args.cpu_seconds)
+
+    if rank != 0:
+        return None
+    peak, peak_kind = peaks()
+    built = ng.build_meshes(d.meshes)
+    blas_bytes = built["nodes"].nbytes + built["triangles"].nbytes
+    alg = render_algorithmic_bytes(wl, d.per_world, blas_bytes)
+    rmed = statistics.median(render_ms)
+    achieved = alg / (rmed / 1000.0) / 1e9
+    tr = traffic_per_image()
+    clk = clocks.summary()
+    return {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(total_ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded body_worlds scene and random-walk poses)",
+        "config": workload_config(args.worlds, {"parallelism": f"worlds sharded, {args.worlds} per GPU, no collective",
+                                                "l2": "flushed between timed steps (256 MiB write)"}),
+        "stages_ms": {"set_body_poses": round(statistics.median(build_ms), 4),
+                      "render": round(rmed, 4)},
+        "rays_per_s_estimate": None,
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "steps": KE, "path": "BatchRenderer.set_body_poses(pinned host poses) + render(host cameras, out=pinned)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": None if tr is None else int(tr * views),
+                     "kernel": "render_kernel", "algorithmic_bytes_per_launch": int(alg)},
+        "cpu_baseline": cpu,
+        "reference_cuda": ref_cuda,
+        "gpu_launches": 3 * K,
+        "clocks": clk,
+    }
+
+
+def run_reference(args, rank):
+    """The reference's own CPU implementation, rank 0 only, with every host core."""
+    from neraulgraphics_b200 import workloads
+    import oracle as O
+    if rank != 0:
+        return None
+    if not O.reference_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libngref.so is not built (make -C oracle ref)"}
+    from neraulgraphics_b200.scene import SceneDesc
+    wl = workloads.body_worlds(worlds=args.worlds, seed=0)
+    sample = 64
+    steps_np = workloads.random_walk(wl.poses[:sample], args.warmup + args.steps, seed=1)
+    d = wl.desc
+    desc = SceneDesc(d.width, d.height, sample, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    cores = os.cpu_count() or 1
+    ref = O.Reference(desc, threads=cores)
+    ref.bind_bodies(**wl.binding)
+    cams = wl.cameras[:sample]
+    for s in range(args.warmup):
+        ref.set_body_poses(steps_np[s])
+        ref.render(cams, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        ref.set_body_poses(steps_np[args.warmup + s])
+        ref.render(cams, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+    el = time.perf_counter() - t0
+    value = sample * args.steps / el
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * el / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded body_worlds scene and random-walk poses)",
+        "config": workload_config(args.worlds, {"sample": f"{sample} of the {args.worlds} worlds per step"}),
+        "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{sample} worlds per step, {args.steps} steps, neraulgraphics 0.5.0 CPU backend"},
+        "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device(f"cuda:{local_rank}"))
+        line = run_ours(args, rank, world, local_rank, dist)
+        if dist:
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

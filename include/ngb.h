@@ -31,7 +31,11 @@
  *
  * Completion: by default every call that launches work waits for it (with a bounded wait, after which
  * it returns NGB_TIMEOUT) before returning, as the reference does. ngb_set_sync(h, 0, ...) makes calls
- * stream-ordered instead: they return once the work is queued on the renderer's stream.
+ * stream-ordered instead: they return once the work is queued on the renderer's stream; a host input
+ * in pinned memory must then stay unchanged until the stream has passed the call.
+ *
+ * Calls on one renderer are serialised by a lock of its own; the calling thread's current CUDA device is
+ * left as it was.
  *
  * All types here are plain C: no CUDA or C++ types cross this boundary.
  */
@@ -243,6 +247,10 @@ int ngb_render_host(ngb_renderer *r, const float *camera_matrices, float fov, in
 int ngb_cast_rays(ngb_renderer *r, const float *origins, const float *directions, int32_t rays_per_world,
     float max_distance, int32_t memory, ngb_ray_hits *out);
 
+/* The same, writing into caller-owned device buffers: rays x {1 f32 distance, 3 f32 normal, 1 i32 ID}. */
+int ngb_cast_rays_into(ngb_renderer *r, const float *origins, const float *directions, int32_t rays_per_world,
+    float max_distance, int32_t memory, float *distance, float *normal, int32_t *object_id);
+
 /* Copies bytes from one of the renderer's device arrays into host memory (src/backend.h:54). */
 int ngb_copy_to_host(ngb_renderer *r, const void *src, void *dst, size_t bytes);
 
@@ -280,11 +288,22 @@ float ngb_last_kernel_ms(const ngb_renderer *r);
 int ngb_inspect_tlas(ngb_renderer *r, uint64_t *keys, int32_t *sorted_ids, int32_t *nodes, int32_t *roots,
     float *matrices);
 
+/* on 1: later renders that ask for depth, normals or IDs also record each centre ray's hit (see
+ * ngb_inspect_hits). Off by default: it writes 16 more bytes per pixel. */
+int ngb_record_hits(ngb_renderer *r, int32_t on);
+
 /* Per pixel of the last render's centre (depth/normal/ID) rays: the instance hit (over all worlds, -1
  * for none), the triangle hit (its index in its mesh's own list, -1 for none) and the barycentrics u, v.
- * Host arrays of view_count * height * width; any may be NULL. Only filled by renders that asked for
- * NGB_OUTPUT_DEPTH, NGB_OUTPUT_NORMAL or NGB_OUTPUT_OBJECT_ID. */
+ * Host arrays of view_count * height * width; any may be NULL. Filled by renders made with
+ * ngb_record_hits on that asked for NGB_OUTPUT_DEPTH, NGB_OUTPUT_NORMAL or NGB_OUTPUT_OBJECT_ID. */
 int ngb_inspect_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *u, float *v);
+
+/* The meshes' bottom-level trees exactly as ngb_create builds them, on the host only (no GPU needed): call
+ * with NULL arrays for the counts, then with arrays of node_count x 8 words (bvh::Node: lo xyz, a,
+ * hi xyz, count), triangle_count x 12 floats (v0, e1, e2 padded to 4), mesh_count roots,
+ * mesh_count x 6 bounds and triangle_count original triangle indices. Errors: ngb_last_error(NULL). */
+int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_count, int32_t *triangle_count,
+    int32_t *nodes, float *triangles, int32_t *roots, float *bounds, int32_t *triangle_index);
 
 #ifdef __cplusplus
 }

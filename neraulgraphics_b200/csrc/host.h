@@ -1,0 +1,57 @@
+// Host-side pieces of the renderer: input validation (with the reference's messages) and the meshes'
+// bottom-level trees. No CUDA here.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ngb.h"
+
+namespace ngb {
+
+// A rejected argument: NGB_INVALID_ARGUMENT, std::invalid_argument in the reference.
+struct InvalidArgument : std::invalid_argument {
+    using std::invalid_argument::invalid_argument;
+};
+// A failed CUDA call: NGB_CUDA_ERROR, neraulgraphics::CudaError in the reference.
+struct CudaFailure : std::runtime_error {
+    int code;
+    CudaFailure(int c, const std::string &what) : std::runtime_error(what), code(c) {}
+};
+// A bounded device wait that ran out: NGB_TIMEOUT.
+struct Timeout : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void require(bool ok, const std::string &message);
+bool finite(float v);
+bool all_finite(const float *v, size_t count);
+std::string fstr(float v);  // std::to_string(float): "%f"
+
+void check_frame_size(int width, int height);                          // src/validate.cpp:34-40
+void check_scene(const ngb_scene &s);                                   // src/validate.cpp:61-78, 42-59
+void check_meshes(const ngb_scene &s);                                  // src/mesh_build.cpp:31-89
+void check_material(const ngb_material &m, const std::string &name);   // src/validate.cpp:22-31
+bool invert_affine(const float *m, float *out);                         // src/mesh_build.cpp:159-183
+bool transform_ok(const float *m);                                      // src/mesh_build.cpp:18-23
+void check_transform(const float *m, const std::string &name);          // src/mesh_build.cpp:25-29
+bool quaternion_is_usable(const float *q);                              // src/batch.cpp:29-32
+void check_environment(const ngb_environment &e);                       // src/environment.cpp:9-27
+
+// Every mesh's tree, concatenated (src/mesh_build.h:16-29): nodes as bvh::Node (lo.xyz, a, hi.xyz, count),
+// triangles in leaf order as v0, e1, e2 padded to float4, per-triangle vertex normals when any mesh has
+// them, each packed triangle's index in its own mesh, and per mesh its root and its box in its own space.
+struct BuiltMeshes {
+    std::vector<float> nodes;        // 8 words per node (a and count stored as int bits)
+    std::vector<float> triangles;    // 12 per triangle
+    std::vector<float> attributes;   // 16 per triangle, or empty
+    std::vector<int32_t> triangle_index;
+    std::vector<int32_t> roots;
+    std::vector<float> bounds;       // 6 per mesh
+};
+
+BuiltMeshes build_meshes(const ngb_scene &s);
+
+}  // namespace ngb

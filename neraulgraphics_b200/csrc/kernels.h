@@ -1,0 +1,79 @@
+// Launch interfaces of the kernels, shared by the host code (renderer.cpp) and the .cu files.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace ngb {
+
+// The tree build of every world, optionally composing the matrices from body poses first.
+struct BuildArgs {
+    int worlds;
+    int per_world;
+    long long n;                   // worlds * per_world
+    int compose;                   // 1: matrices from body poses; 0: matrices_in
+    const float *matrices_in;      // n x 12, when !compose
+    const float *body_poses;       // worlds x bodies_per_world x 7, when compose
+    const int *body_of_instance;   // per slot
+    const float *local_pose;       // per slot, 7
+    const float *local_scale;      // per slot, 3
+    int bodies_per_world;
+    float *matrices_out;           // n x 12, written when compose
+    const float *slot_bounds;      // per slot: its mesh's box in mesh space, 6
+    const int *slot_blas_root;     // per slot
+    float4 *inst;                  // n x 4
+    unsigned long long *keys;      // n, instance order
+    int *sorted_ids;               // n, sorted order
+    float4 *tlas;                  // (2n - 1) x 2
+    int *roots;                    // worlds
+    int *parent;                   // 2n - 1; parent[0] stays -1
+    int *arrivals;                 // n - 1 counters, zero between builds
+    int *error_flag;               // set nonzero if a climb runs longer than any valid tree allows
+};
+
+// Group size (threads per world) of the per-world build: a power of two, at least 32.
+int build_group_size(int per_world);
+// Largest instance count per world the per-world build handles.
+constexpr int MAX_PER_WORLD = 1024;
+cudaError_t launch_build_worlds(const BuildArgs &a, cudaStream_t stream);
+
+// Rendering every view of a batch.
+struct RenderArgs {
+    const float *cameras;          // views x 12, camera-to-world
+    float fov_scale;               // tanf(fov / 2), computed on the host
+    float aspect;                  // width / height
+    int width;
+    int height;
+    int cameras_per_world;
+    int views;
+    int frame;
+    int spp;
+    uint8_t *rgb;                  // views x H x W x 3, or null
+    float *depth;                  // views x H x W, or null
+    float *normal;                 // views x H x W x 3, or null
+    int32_t *object_id;            // views x H x W, or null
+    int32_t *hit_instance;         // centre ray's hit record, or null
+    int32_t *hit_triangle;
+    float *hit_u;
+    float *hit_v;
+    int *error_flag;               // set nonzero if a traversal stack would overflow
+};
+cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream);
+
+// Ray queries over the worlds of a batch: ray i belongs to world i / rays_per_world.
+struct RayArgs {
+    const float *origins;
+    const float *directions;
+    float max_distance;
+    int rays_per_world;
+    int count;
+    float *distance;
+    float *normal;
+    int32_t *object_id;
+    int *error_flag;
+};
+cudaError_t launch_rays(const SceneParams &s, const RayArgs &a, cudaStream_t stream);
+
+}  // namespace ngb

@@ -1,0 +1,370 @@
+// Pose compose and the per-world top-level tree build, fused into one launch.
+//
+// The tree is the reference's GPU LBVH (src/cuda_tlas.cuh:27-211) node for node: keys world << 32 | Morton
+// code of the instance's box centre inside its world's centre bounds, a stable sort, the Karras radix tree
+// over all worlds' sorted keys (ties broken by global position), boxes filled bottom-up, and each world's
+// root. The reference runs that as ten launches over global memory plus a CUB radix sort. Here, because
+// the world sits in the key's top bits, the sorted array is every world's own sorted run laid end to end,
+// and every node of a world's subtree depends only on that world's keys and on world numbers. So one group
+// of threads per world (a warp, or a whole CTA for up to 1024 instances) does the whole build in shared
+// memory: compose the matrix, invert it, box it, reduce the world's centre bounds, make the keys, rank-sort
+// them, emit the Karras nodes, and refit the boxes bottom-up with shared-memory atomics. The only nodes a
+// group cannot finish are the inter-world ones (never traversed: every ray starts at its world's root);
+// their links are emitted by the group that owns their index, and a second small launch fits their boxes
+// by climbing from the world roots, as fit_boxes does (cuda_tlas.cuh:179-196).
+#include "device.cuh"
+#include "kernels.h"
+
+namespace ngb {
+namespace {
+
+// quat_matrix (src/cuda_backend.cu:165-172): rotation of a quaternion x, y, z, w, normalised first.
+__device__ __forceinline__ void quat_matrix(const float *q, float *r) {
+    float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float n = sqrtf(x * x + y * y + z * z + w * w);
+    if (n > 0.0f) {
+        x /= n;
+        y /= n;
+        z /= n;
+        w /= n;
+    } else {
+        x = y = z = 0.0f;
+        w = 1.0f;
+    }
+    r[0] = 1 - 2 * (y * y + z * z);
+    r[1] = 2 * (x * y - z * w);
+    r[2] = 2 * (x * z + y * w);
+    r[3] = 2 * (x * y + z * w);
+    r[4] = 1 - 2 * (x * x + z * z);
+    r[5] = 2 * (y * z - x * w);
+    r[6] = 2 * (x * z - y * w);
+    r[7] = 2 * (y * z + x * w);
+    r[8] = 1 - 2 * (x * x + y * y);
+}
+
+// An instance's matrix from its body's pose, its own offset and its scale (src/cuda_backend.cu:176-202).
+__device__ __forceinline__ void compose(const BuildArgs &a, long long w, int i, float *m) {
+    const float *lp = a.local_pose + 7 * i, *sc = a.local_scale + 3 * i;
+    float lpv[7], scv[3];
+    for (int k = 0; k < 7; ++k) lpv[k] = __ldg(lp + k);
+    for (int k = 0; k < 3; ++k) scv[k] = __ldg(sc + k);
+    float rl[9], r[9], p[3] = {lpv[0], lpv[1], lpv[2]};
+    quat_matrix(lpv + 3, rl);
+    const int body = __ldg(a.body_of_instance + i);
+    if (body < 0) {
+        for (int k = 0; k < 9; ++k) r[k] = rl[k];
+    } else {
+        const float *bpp = a.body_poses + 7 * (w * a.bodies_per_world + body);
+        float bp[7];
+        for (int k = 0; k < 7; ++k) bp[k] = __ldg(bpp + k);
+        float rb[9];
+        quat_matrix(bp + 3, rb);
+        for (int row = 0; row < 3; ++row) {
+            for (int col = 0; col < 3; ++col)
+                r[3 * row + col] = rb[3 * row] * rl[col] + rb[3 * row + 1] * rl[3 + col] + rb[3 * row + 2] * rl[6 + col];
+            p[row] = bp[row] + rb[3 * row] * lpv[0] + rb[3 * row + 1] * lpv[1] + rb[3 * row + 2] * lpv[2];
+        }
+    }
+    for (int row = 0; row < 3; ++row) {
+        for (int col = 0; col < 3; ++col) m[4 * row + col] = r[3 * row + col] * scv[col];
+        m[4 * row + 3] = p[row];
+    }
+}
+
+// invert_affine (src/cuda_tlas.cuh:35-47), IEEE division.
+__device__ __forceinline__ void invert_affine(const float *m, float *out) {
+    const float c00 = m[5] * m[10] - m[6] * m[9];
+    const float c01 = m[6] * m[8] - m[4] * m[10];
+    const float c02 = m[4] * m[9] - m[5] * m[8];
+    const float inv = 1.0f / (m[0] * c00 + m[1] * c01 + m[2] * c02);
+    const float r[9] = {c00 * inv, (m[2] * m[9] - m[1] * m[10]) * inv, (m[1] * m[6] - m[2] * m[5]) * inv, c01 * inv,
+        (m[0] * m[10] - m[2] * m[8]) * inv, (m[2] * m[4] - m[0] * m[6]) * inv, c02 * inv,
+        (m[1] * m[8] - m[0] * m[9]) * inv, (m[0] * m[5] - m[1] * m[4]) * inv};
+    for (int row = 0; row < 3; ++row) {
+        for (int col = 0; col < 3; ++col) out[4 * row + col] = r[3 * row + col];
+        out[4 * row + 3] = -(r[3 * row] * m[3] + r[3 * row + 1] * m[7] + r[3 * row + 2] * m[11]);
+    }
+}
+
+// Shared memory of one world's group, G threads (G >= instances per world).
+template <int G>
+struct GroupSmem {
+    uint32_t key_in[G];    // Morton code of local instance i
+    uint32_t key[G];       // Morton code at sorted position r
+    float box[2 * G][6];   // internal node j at j, leaf of sorted position r at G + r
+    int child[G][2];       // local ids of internal node j's children
+    int parent[2 * G];     // local id of a node's parent, -1 when it is outside the world
+    int arrive[G];
+    int bounds[6];         // ordered-int centre bounds
+};
+
+// The reference's common_prefix (cuda_tlas.cuh:119-124) between sorted positions p (in this world) and x,
+// from this world's keys in shared memory and, for a position in another world, from the world numbers
+// alone: keys of different worlds first differ in the world bits, so their shared prefix is clz32(w ^ wx).
+template <int G>
+__device__ __forceinline__ int delta(const GroupSmem<G> &sm, int p, long long x, long long n, long long base, int P,
+    uint32_t world, uint32_t key_p) {
+    if (x < 0 || x >= n) return -1;
+    if (x >= base && x < base + P) {
+        const uint32_t kx = sm.key[x - base];
+        if (kx == key_p) return 64 + __clz(static_cast<int>(static_cast<uint32_t>(p) ^ static_cast<uint32_t>(x)));
+        return 32 + __clz(static_cast<int>(key_p ^ kx));
+    }
+    const uint32_t wx = static_cast<uint32_t>(x / P);
+    return __clz(static_cast<int>(world ^ wx));
+}
+
+template <int G>
+__global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const BuildArgs a) {
+    constexpr int CTA = G < 128 ? 128 : G;
+    constexpr int WPC = CTA / G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int grp = threadIdx.x / G, i = threadIdx.x % G;
+    GroupSmem<G> &sm = reinterpret_cast<GroupSmem<G> *>(smem_raw)[grp];
+    const long long w = static_cast<long long>(blockIdx.x) * WPC + grp;
+    const int P = a.per_world;
+    const long long n = a.n;
+    const bool world_ok = w < a.worlds;
+    const bool valid = world_ok && i < P;
+    const long long base = w * P;
+    const long long g = base + i;
+
+    for (int k = i; k < 2 * G; k += G) sm.parent[k] = -1;
+    sm.arrive[i] = 0;
+    if (i == 0)
+        for (int k = 0; k < 3; ++k) {
+            sm.bounds[k] = to_ordered(1e30f);
+            sm.bounds[3 + k] = to_ordered(-1e30f);
+        }
+    __syncthreads();
+
+    // Matrix, inverse, world box (place_instances, cuda_tlas.cuh:69-96).
+    float lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    if (valid) {
+        float m[12];
+        if (a.compose) {
+            compose(a, w, i, m);
+            float *mo = a.matrices_out + 12 * g;
+            for (int k = 0; k < 12; ++k) mo[k] = m[k];
+        } else {
+            const float *mi = a.matrices_in + 12 * g;
+            for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+        }
+        float inv[12];
+        invert_affine(m, inv);
+        float4 *rec = a.inst + 4 * g;
+        rec[0] = make_float4(inv[0], inv[1], inv[2], inv[3]);
+        rec[1] = make_float4(inv[4], inv[5], inv[6], inv[7]);
+        rec[2] = make_float4(inv[8], inv[9], inv[10], inv[11]);
+        rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + i)), __int_as_float(i), 0.0f, 0.0f);
+        const float *lb = a.slot_bounds + 6 * i;
+        float b[6];
+        for (int k = 0; k < 6; ++k) b[k] = __ldg(lb + k);
+        for (int corner = 0; corner < 8; ++corner) {
+            const float p[3] = {(corner & 1) ? b[3] : b[0], (corner & 2) ? b[4] : b[1], (corner & 4) ? b[5] : b[2]};
+            for (int ax = 0; ax < 3; ++ax) {
+                const float v = m[4 * ax] * p[0] + m[4 * ax + 1] * p[1] + m[4 * ax + 2] * p[2] + m[4 * ax + 3];
+                lo[ax] = fminf(lo[ax], v);
+                hi[ax] = fmaxf(hi[ax], v);
+            }
+        }
+        for (int ax = 0; ax < 3; ++ax) {
+            const int c = to_ordered(0.5f * (lo[ax] + hi[ax]));
+            atomicMin(&sm.bounds[ax], c);
+            atomicMax(&sm.bounds[3 + ax], c);
+        }
+    }
+    __syncthreads();
+
+    // Key (make_keys, cuda_tlas.cuh:99-115).
+    uint32_t morton = 0;
+    if (valid) {
+        uint32_t q[3];
+        for (int ax = 0; ax < 3; ++ax) {
+            const float blo = from_ordered(sm.bounds[ax]), bhi = from_ordered(sm.bounds[3 + ax]);
+            const float centre = 0.5f * (lo[ax] + hi[ax]);
+            const float extent = bhi - blo;
+            const float t = extent > 1e-20f ? (centre - blo) / extent : 0.0f;
+            q[ax] = static_cast<uint32_t>(fminf(fmaxf(t, 0.0f), 1.0f) * 1023.0f);
+        }
+        morton = (spread_bits(q[0]) << 2) | (spread_bits(q[1]) << 1) | spread_bits(q[2]);
+        a.keys[g] = (static_cast<unsigned long long>(w) << 32) | morton;
+        sm.key_in[i] = morton;
+    }
+    __syncthreads();
+
+    // Stable sort by rank: the sorted position of (key, i) is the number of (key, j) before it. The same
+    // order as cub::DeviceRadixSort::SortPairs over (key, id) with ids ascending (cuda_tlas.cuh:273-274).
+    int rank = 0;
+    if (valid) {
+        for (int j = 0; j < P; ++j) {
+            const uint32_t kj = sm.key_in[j];
+            rank += (kj < morton) || (kj == morton && j < i);
+        }
+        sm.key[rank] = morton;
+        a.sorted_ids[base + rank] = static_cast<int>(g);
+        for (int ax = 0; ax < 3; ++ax) {
+            sm.box[G + rank][ax] = lo[ax];
+            sm.box[G + rank][3 + ax] = hi[ax];
+        }
+        // The leaf (make_leaves, cuda_tlas.cuh:162-175).
+        float4 *leaf = a.tlas + 2 * (n - 1 + base + rank);
+        leaf[0] = make_float4(lo[0], lo[1], lo[2], __int_as_float(~static_cast<int>(g)));
+        leaf[1] = make_float4(hi[0], hi[1], hi[2], __int_as_float(-1));
+    }
+    __syncthreads();
+
+    // The internal node at sorted position p = base + i (build_radix_tree, cuda_tlas.cuh:128-159).
+    const long long p = base + i;
+    bool within = false, is_root = false;
+    int left = 0, right = 0;
+    if (valid && p < n - 1) {
+        const uint32_t kp = sm.key[i];
+        const uint32_t wu = static_cast<uint32_t>(w);
+        const int ip = static_cast<int>(p);
+        auto dlt = [&](long long x) { return delta<G>(sm, ip, x, n, base, P, wu, kp); };
+        const int d = dlt(p + 1) > dlt(p - 1) ? 1 : -1;
+        const int min_prefix = dlt(p - d);
+        long long max_length = 2;
+        while (dlt(p + max_length * d) > min_prefix) max_length *= 2;
+        long long length = 0;
+        for (long long t = max_length / 2; t >= 1; t /= 2)
+            if (dlt(p + (length + t) * d) > min_prefix) length += t;
+        const long long j = p + length * d;
+        const int node_prefix = dlt(j);
+        long long s = 0;
+        for (long long t = (length + 1) / 2;; t = (t + 1) / 2) {
+            if (dlt(p + (s + t) * d) > node_prefix) s += t;
+            if (t == 1) break;
+        }
+        const long long gamma = p + s * d + (d < 0 ? d : 0);
+        const long long rlo = p < j ? p : j, rhi = p < j ? j : p;
+        left = static_cast<int>((rlo == gamma) ? n - 1 + gamma : gamma);
+        right = static_cast<int>((rhi == gamma + 1) ? n - 1 + gamma + 1 : gamma + 1);
+        a.parent[left] = ip;
+        a.parent[right] = ip;
+        within = rlo >= base && rhi <= base + P - 1;
+        if (within) {
+            auto local = [&](long long c) { return static_cast<int>(c >= n - 1 ? G + (c - (n - 1) - base) : c - base); };
+            const int cl = local(left), cr = local(right);
+            sm.child[i][0] = cl;
+            sm.child[i][1] = cr;
+            sm.parent[cl] = i;
+            sm.parent[cr] = i;
+            is_root = rlo == base && rhi == base + P - 1;
+        } else {
+            // An inter-world node: its links now, its box from the climb over worlds.
+            float4 *nd = a.tlas + 2 * p;
+            reinterpret_cast<float *>(nd)[3] = __int_as_float(left);
+            reinterpret_cast<float *>(nd + 1)[3] = __int_as_float(right);
+        }
+        if (is_root) a.roots[w] = ip;
+    }
+    if (valid && P == 1) a.roots[w] = static_cast<int>(n - 1 + base);
+    __syncthreads();
+
+    // Boxes from the leaves up (fit_boxes, cuda_tlas.cuh:179-196): the second of two arrivals at a node
+    // knows both children are done, and climbs on.
+    if (valid) {
+        int node = G + rank;
+        volatile float(*vbox)[6] = sm.box;
+        for (int steps = 0;; ++steps) {
+            const int par = sm.parent[node];
+            if (par < 0) break;
+            if (steps > 2 * G) {  // longer than any tree over G leaves: the links are malformed
+                *a.error_flag = 3;
+                break;
+            }
+            __threadfence_block();
+            if (atomicAdd(&sm.arrive[par], 1) == 0) break;
+            __threadfence_block();
+            const int cl = sm.child[par][0], cr = sm.child[par][1];
+            for (int ax = 0; ax < 3; ++ax) {
+                vbox[par][ax] = fminf(vbox[cl][ax], vbox[cr][ax]);
+                vbox[par][3 + ax] = fmaxf(vbox[cl][3 + ax], vbox[cr][3 + ax]);
+            }
+            node = par;
+        }
+    }
+    __syncthreads();
+
+    if (valid && p < n - 1 && within) {
+        float4 *nd = a.tlas + 2 * p;
+        nd[0] = make_float4(sm.box[i][0], sm.box[i][1], sm.box[i][2], __int_as_float(left));
+        nd[1] = make_float4(sm.box[i][3], sm.box[i][4], sm.box[i][5], __int_as_float(right));
+    }
+}
+
+// The boxes of the inter-world nodes: one thread per world climbs from its root; the second arrival at a
+// node computes its box from its children's and climbs on (fit_boxes, cuda_tlas.cuh:179-196). The
+// counters are left at zero for the next build.
+__global__ void __launch_bounds__(128) fit_world_links_kernel(const int *roots, const int *parent, int *arrivals,
+    float4 *tlas, int worlds, int *error_flag) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= worlds) return;
+    int node = roots[w];
+    // Keys of different worlds differ in their 32 world bits, so the tree over worlds is at most 33 deep.
+    for (int steps = 0;; ++steps) {
+        const int p = parent[node];
+        if (p < 0) return;
+        if (steps > 64) {
+            *error_flag = 4;
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1) == 0) return;
+        __threadfence();
+        arrivals[p] = 0;
+        const float4 p0 = __ldcg(tlas + 2 * p), p1 = __ldcg(tlas + 2 * p + 1);
+        const int l = __float_as_int(p0.w), r = __float_as_int(p1.w);
+        const float4 l0 = __ldcg(tlas + 2 * l), l1 = __ldcg(tlas + 2 * l + 1);
+        const float4 r0 = __ldcg(tlas + 2 * r), r1 = __ldcg(tlas + 2 * r + 1);
+        tlas[2 * p] = make_float4(fminf(l0.x, r0.x), fminf(l0.y, r0.y), fminf(l0.z, r0.z), p0.w);
+        tlas[2 * p + 1] = make_float4(fmaxf(l1.x, r1.x), fmaxf(l1.y, r1.y), fmaxf(l1.z, r1.z), p1.w);
+        node = p;
+    }
+}
+
+template <int G>
+cudaError_t launch_group(const BuildArgs &a, cudaStream_t stream) {
+    constexpr int CTA = G < 128 ? 128 : G;
+    constexpr int WPC = CTA / G;
+    const size_t smem = sizeof(GroupSmem<G>) * WPC;
+    cudaError_t e = cudaFuncSetAttribute(build_worlds_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = (a.worlds + WPC - 1) / WPC;
+    build_worlds_kernel<G><<<static_cast<unsigned>(blocks), CTA, smem, stream>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int build_group_size(int per_world) {
+    int g = 32;
+    while (g < per_world) g *= 2;
+    return g;
+}
+
+cudaError_t launch_build_worlds(const BuildArgs &a, cudaStream_t stream) {
+    if (a.n == 0) return cudaSuccess;
+    cudaError_t e;
+    switch (build_group_size(a.per_world)) {
+    case 32: e = launch_group<32>(a, stream); break;
+    case 64: e = launch_group<64>(a, stream); break;
+    case 128: e = launch_group<128>(a, stream); break;
+    case 256: e = launch_group<256>(a, stream); break;
+    case 512: e = launch_group<512>(a, stream); break;
+    case 1024: e = launch_group<1024>(a, stream); break;
+    default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    if (a.worlds > 1) {
+        fit_world_links_kernel<<<(a.worlds + 127) / 128, 128, 0, stream>>>(a.roots, a.parent, a.arrivals, a.tlas,
+            a.worlds, a.error_flag);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+}  // namespace ngb

@@ -1,0 +1,800 @@
+// The renderer behind the C ABI (include/ngb.h): validation, device buffers, the stream, launches and
+// bounded waits. Replaces BatchRenderer (src/batch.cpp) over CudaBackend (src/cuda_backend.cu:325-793).
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <type_traits>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "host.h"
+#include "kernels.h"
+
+namespace ngb {
+
+[[noreturn]] void cuda_fail(cudaError_t e, const char *call, const char *file, int line) {
+    throw CudaFailure(static_cast<int>(e), std::string(file) + ":" + std::to_string(line) + ": " + call + " failed: " +
+        cudaGetErrorString(e) + " (" + cudaGetErrorName(e) + ")");
+}
+#define CK(call)                                                                 \
+    do {                                                                         \
+        const cudaError_t err_ = (call);                                         \
+        if (err_ != cudaSuccess) ngb::cuda_fail(err_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+// What the kernels' error flag means. It stays set: the renderer's later results are not trusted.
+std::string device_error_message(int code) {
+    switch (code) {
+    case 1: return "a traversal stack overflowed; the images of that call are incomplete";
+    case 2: return "a tree walk ran longer than the tree allows (malformed tree); the images are incomplete";
+    case 3: return "a world's box refit ran longer than its tree allows (malformed tree)";
+    case 4: return "the refit of the inter-world nodes ran longer than the tree allows (malformed tree)";
+    default: return "the GPU kernels reported error " + std::to_string(code);
+    }
+}
+
+namespace {
+
+// A device array, grown on demand and freed with its owner.
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    T *ensure(size_t count) {
+        if (count == 0) return p;
+        if (p && count <= n) return p;
+        release();
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+        return p;
+    }
+};
+
+// Makes the renderer's GPU current for the call and restores the caller's afterwards.
+struct DeviceGuard {
+    int previous = -1;
+    explicit DeviceGuard(int device) {
+        CK(cudaGetDevice(&previous));
+        if (previous != device) CK(cudaSetDevice(device));
+    }
+    ~DeviceGuard() {
+        int now = -1;
+        if (cudaGetDevice(&now) == cudaSuccess && now != previous && previous >= 0) cudaSetDevice(previous);
+    }
+};
+
+DevMaterial dev_material(const ngb_material &m) {
+    return DevMaterial{make_float3(m.diffuse_color.x, m.diffuse_color.y, m.diffuse_color.z), m.diffuse_albedo,
+        m.specular_albedo, m.reflectivity, m.specular_exponent, 0.0f};
+}
+
+}  // namespace
+
+struct Renderer {
+    std::mutex mutex;
+    std::string last_error;
+    int width = 0, height = 0, worlds = 0, cpw = 0, per_world = 0, device = 0;
+    long long n = 0;
+    SceneParams params{};
+
+    // The scene: shared meshes and what each slot of a world holds.
+    DevBuf<float4> blas, tris, attrs;
+    DevBuf<int> tri_index, slot_blas_root;
+    DevBuf<float> slot_bounds;
+    DevBuf<DevMaterial> slot_material;
+    // Per build.
+    DevBuf<float> matrices;
+    DevBuf<float4> inst, tlas;
+    DevBuf<unsigned long long> keys;
+    DevBuf<int> sorted_ids, roots, parent, arrivals;
+    // Bodies.
+    bool bound = false;
+    int bodies_per_world = 0;
+    DevBuf<int> body_of_instance;
+    DevBuf<float> local_pose, local_scale, body_poses;
+    // Staging for host inputs and the renderer's own outputs.
+    DevBuf<float> cameras, ray_origins, ray_directions;
+    DevBuf<uint8_t> out_rgb;
+    DevBuf<float> out_depth, out_normal;
+    DevBuf<int32_t> out_id;
+    DevBuf<float> ray_distance, ray_normal;
+    DevBuf<int32_t> ray_id;
+    bool record_hits = false;
+    DevBuf<int32_t> hit_instance, hit_triangle;
+    DevBuf<float> hit_u, hit_v;
+    DevBuf<int> error_flag;
+    int *host_error = nullptr;  // pinned: the device error flag, copied back after every launch
+
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_done = nullptr;
+    bool synchronous = true;
+    double timeout = 120.0;
+    float kernel_ms = 0.0f;
+    bool timing_pending = false;
+
+    explicit Renderer(const ngb_scene &s);
+    ~Renderer();
+
+    void build(const float *matrices_in, bool compose, const float *poses);
+    void finish();
+    void wait(cudaEvent_t ev, double seconds);
+    void set_instance_transforms(const float *m, int memory);
+    void bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc);
+    void set_body_poses(const float *poses, int memory);
+    void check_render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory);
+    void render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
+        float *depth, float *normal, int32_t *ids);
+    void cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory, ngb_ray_hits *out,
+        float *distance, float *normal, int32_t *ids);
+    size_t pixels() const { return static_cast<size_t>(worlds) * cpw * height * width; }
+};
+
+Renderer::Renderer(const ngb_scene &s) {
+    check_frame_size(s.width, s.height);
+    require(s.world_count >= 1, "world_count must be 1 or more, got " + std::to_string(s.world_count));
+    require(s.cameras_per_world >= 1, "cameras_per_world must be 1 or more, got " + std::to_string(s.cameras_per_world));
+    const long long views = static_cast<long long>(s.world_count) * s.cameras_per_world;
+    require(views * s.height <= INT32_MAX, std::to_string(views) + " views of height " + std::to_string(s.height) +
+        " are too many");
+    check_scene(s);
+    check_meshes(s);
+    require(s.instance_count <= MAX_PER_WORLD, "a world holds " + std::to_string(s.instance_count) +
+        " instances, at most " + std::to_string(MAX_PER_WORLD) + " fit the per-world tree build");
+    require(static_cast<long long>(s.world_count) * s.instance_count <= (INT32_MAX - 1) / 2,
+        "too many instances over all worlds");
+    int device_count = 0;
+    CK(cudaGetDeviceCount(&device_count));
+    require(s.device >= 0 && s.device < device_count, "device " + std::to_string(s.device) + " does not exist");
+    width = s.width;
+    height = s.height;
+    worlds = s.world_count;
+    cpw = s.cameras_per_world;
+    per_world = s.instance_count;
+    device = s.device;
+    n = static_cast<long long>(worlds) * per_world;
+    DeviceGuard guard(device);
+    CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
+    CK(cudaEventCreate(&ev_start));
+    CK(cudaEventCreate(&ev_stop));
+    CK(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    CK(cudaHostAlloc(&host_error, sizeof(int), cudaHostAllocDefault));
+    *host_error = 0;
+    error_flag.ensure(1);
+    CK(cudaMemsetAsync(error_flag.p, 0, sizeof(int), stream));
+
+    // The classic scene: spheres, lights (as the reference's to_device: src/device_scene.h:265-272), floor, sky.
+    for (int i = 0; i < s.sphere_count; ++i) {
+        const ngb_sphere &sp = s.spheres[i];
+        params.spheres[i] = DevSphere{make_float3(sp.center.x, sp.center.y, sp.center.z), sp.radius, dev_material(sp.material)};
+    }
+    for (int i = 0; i < s.light_count; ++i) {
+        const ngb_light &l = s.lights[i];
+        float dx = l.direction.x, dy = l.direction.y, dz = l.direction.z;
+        const float nn = std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (nn > 0.0f) {
+            dx = dx / nn;
+            dy = dy / nn;
+            dz = dz / nn;
+        } else {
+            dx = 0.0f;
+            dy = 0.0f;
+            dz = -1.0f;
+        }
+        const bool spot = l.spot_angle > 0.0f;
+        params.lights[i] = DevLight{make_float3(l.position.x, l.position.y, l.position.z), l.intensity, l.radius, l.falloff,
+            make_float3(dx, dy, dz), spot ? std::cos(l.spot_angle) : -2.0f,
+            spot ? std::cos(l.spot_angle * (1.0f - l.spot_softness)) : -2.0f, make_float3(l.color.x, l.color.y, l.color.z)};
+    }
+    params.sphere_count = s.sphere_count;
+    params.light_count = s.light_count;
+    params.floor = DevPlane{s.floor.y, s.floor.half_extent_x, s.floor.z_min, s.floor.z_max, s.floor.checker_scale,
+        dev_material(s.floor.material)};
+    params.env_up = make_float3(0.0f, 1.0f, 0.0f);
+    params.env_color_up = make_float3(0.10f, 0.26f, 0.60f);
+    params.env_color_down = make_float3(0.35f, 0.52f, 0.70f);
+    params.env_intensity = 1.0f;
+    params.ambient = 0.0f;
+    params.instance_count = static_cast<int>(n);
+    params.per_world = per_world;
+    if (per_world == 0) {
+        CK(cudaEventRecord(ev_done, stream));
+        wait(ev_done, timeout);
+        return;
+    }
+
+    // The meshes' trees, built once on the host (src/mesh_build.cpp:91-157), and the slots' tables.
+    const BuiltMeshes built = build_meshes(s);
+    auto upload = [&](auto &buf, const auto &vec) {
+        using T = std::remove_pointer_t<decltype(buf.p)>;
+        const size_t bytes = vec.size() * sizeof(typename std::decay_t<decltype(vec)>::value_type);
+        buf.ensure(bytes / sizeof(T));
+        CK(cudaMemcpy(buf.p, vec.data(), bytes, cudaMemcpyHostToDevice));
+    };
+    upload(blas, built.nodes);
+    upload(tris, built.triangles);
+    if (!built.attributes.empty()) upload(attrs, built.attributes);
+    upload(tri_index, built.triangle_index);
+    std::vector<int> root_of_slot(per_world);
+    std::vector<float> bounds_of_slot(6 * static_cast<size_t>(per_world));
+    std::vector<DevMaterial> material_of_slot(per_world);
+    for (int i = 0; i < per_world; ++i) {
+        const int mesh = s.instances[i].mesh;
+        root_of_slot[i] = built.roots[mesh];
+        std::copy(built.bounds.begin() + 6 * mesh, built.bounds.begin() + 6 * mesh + 6, bounds_of_slot.begin() + 6 * i);
+        material_of_slot[i] = dev_material(s.instances[i].material);
+    }
+    upload(slot_blas_root, root_of_slot);
+    upload(slot_bounds, bounds_of_slot);
+    upload(slot_material, material_of_slot);
+    matrices.ensure(12 * n);
+    inst.ensure(4 * n);
+    tlas.ensure(2 * (2 * n - 1));
+    keys.ensure(n);
+    sorted_ids.ensure(n);
+    roots.ensure(worlds);
+    parent.ensure(2 * n - 1);
+    arrivals.ensure(std::max<long long>(n - 1, 1));
+    CK(cudaMemset(parent.p, 0xFF, (2 * n - 1) * sizeof(int)));
+    CK(cudaMemset(arrivals.p, 0, arrivals.n * sizeof(int)));
+    params.tlas = tlas.p;
+    params.roots = roots.p;
+    params.inst = inst.p;
+    params.blas = blas.p;
+    params.tris = tris.p;
+    params.attrs = built.attributes.empty() ? nullptr : attrs.p;
+    params.tri_index = tri_index.p;
+    params.slot_material = slot_material.p;
+    params.blas_node_count = static_cast<int>(built.nodes.size() / 8);
+
+    // Every world starts with the transforms the instances were given (src/cuda_backend.cu:765-770).
+    std::vector<float> initial(12 * n);
+    for (int w = 0; w < worlds; ++w)
+        for (int i = 0; i < per_world; ++i)
+            std::memcpy(&initial[12 * (static_cast<size_t>(w) * per_world + i)], s.instances[i].transform, 48);
+    CK(cudaMemcpy(matrices.p, initial.data(), initial.size() * sizeof(float), cudaMemcpyHostToDevice));
+    build(matrices.p, false, nullptr);
+    CK(cudaEventRecord(ev_done, stream));
+    wait(ev_done, timeout);
+}
+
+Renderer::~Renderer() {
+    // Destructors must not throw; errors after a sticky fault are ignored.
+    int previous = -1;
+    cudaGetDevice(&previous);
+    if (previous != device) cudaSetDevice(device);
+    if (own_stream) cudaStreamSynchronize(own_stream);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    if (ev_done) cudaEventDestroy(ev_done);
+    if (host_error) cudaFreeHost(host_error);
+    if (own_stream) cudaStreamDestroy(own_stream);
+    // The DevBufs free themselves; the device must be current while they do, so release them here.
+    blas.release(), tris.release(), attrs.release(), tri_index.release(), slot_blas_root.release();
+    slot_bounds.release(), slot_material.release(), matrices.release(), inst.release(), tlas.release();
+    keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
+    body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
+    cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
+    out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
+    hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
+    if (previous >= 0 && previous != device) cudaSetDevice(previous);
+}
+
+// Waits for an event with a limit: polls, and gives up with NGB_TIMEOUT after `seconds`.
+void Renderer::wait(cudaEvent_t ev, double seconds) {
+    const auto start = std::chrono::steady_clock::now();
+    for (int spin = 0;; ++spin) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return;
+        if (e != cudaErrorNotReady) CK(e);
+        const double waited = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+        if (waited > seconds)
+            throw Timeout("the GPU work did not finish within " + std::to_string(seconds) + " seconds");
+        if (spin > 1000) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+// Called after every launch: brings the device's error flag back with the work and, when synchronous,
+// waits for both.
+void Renderer::finish() {
+    CK(cudaMemcpyAsync(host_error, error_flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventRecord(ev_done, stream));
+    if (!synchronous) return;
+    wait(ev_done, timeout);
+    if (timing_pending) {
+        CK(cudaEventElapsedTime(&kernel_ms, ev_start, ev_stop));
+        timing_pending = false;
+    }
+    if (*host_error) throw CudaFailure(-1, device_error_message(*host_error));
+}
+
+// Queues the tree build of every world: from matrices in device memory, or composed from body poses.
+void Renderer::build(const float *matrices_in, bool compose, const float *poses) {
+    BuildArgs a{};
+    a.worlds = worlds;
+    a.per_world = per_world;
+    a.n = n;
+    a.compose = compose ? 1 : 0;
+    a.matrices_in = matrices_in;
+    a.body_poses = poses;
+    a.body_of_instance = body_of_instance.p;
+    a.local_pose = local_pose.p;
+    a.local_scale = local_scale.p;
+    a.bodies_per_world = bodies_per_world;
+    // Composed matrices, and matrices given in the caller's device memory, are kept for inspection.
+    a.matrices_out = (compose || matrices_in != matrices.p) ? matrices.p : nullptr;
+    a.slot_bounds = slot_bounds.p;
+    a.slot_blas_root = slot_blas_root.p;
+    a.inst = inst.p;
+    a.keys = keys.p;
+    a.sorted_ids = sorted_ids.p;
+    a.tlas = tlas.p;
+    a.roots = roots.p;
+    a.parent = parent.p;
+    a.arrivals = arrivals.p;
+    a.error_flag = error_flag.p;
+    CK(launch_build_worlds(a, stream));
+}
+
+// src/batch.cpp:91-109 and src/cuda_backend.cu:457-469.
+void Renderer::set_instance_transforms(const float *m, int memory) {
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    if (per_world == 0) return;
+    require(m != nullptr, "matrices must not be null");
+    if (memory == NGB_MEMORY_HOST) {
+        for (long long g = 0; g < n; ++g)
+            if (!transform_ok(m + 12 * g))
+                check_transform(m + 12 * g, "world " + std::to_string(g / per_world) + " instance " +
+                    std::to_string(g % per_world) + " transform");
+        CK(cudaMemcpyAsync(matrices.p, m, static_cast<size_t>(n) * 12 * sizeof(float), cudaMemcpyHostToDevice, stream));
+        build(matrices.p, false, nullptr);
+    } else {
+        build(m, false, nullptr);
+    }
+    finish();
+}
+
+// src/batch.cpp:111-129 and src/cuda_backend.cu:472-491.
+void Renderer::bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc) {
+    const int P = per_world;
+    require(bpw >= 0, "bodies_per_world must be 0 or more");
+    require(P == 0 || (boi != nullptr && lp != nullptr && sc != nullptr),
+        "a body binding needs one body index, 7 pose floats and 3 scale floats for each of the " + std::to_string(P) +
+        " instances of a world");
+    for (int i = 0; i < P; ++i) {
+        const int b = boi[i];
+        require(b >= -1 && b < bpw, "instance " + std::to_string(i) + " is on body " + std::to_string(b) +
+            ", but there are " + std::to_string(bpw) + " bodies per world");
+        require(all_finite(lp + 7 * i, 7) && quaternion_is_usable(lp + 7 * i + 3),
+            "instance " + std::to_string(i) + " has a pose with a NaN or infinite value, or a zero quaternion");
+        require(all_finite(sc + 3 * i, 3), "instance " + std::to_string(i) + " has a scale with a NaN or infinite value");
+    }
+    require(static_cast<long long>(worlds) * bpw * 7 <= INT32_MAX, "too many bodies");
+    if (P > 0) {
+        body_of_instance.ensure(P);
+        local_pose.ensure(7 * static_cast<size_t>(P));
+        local_scale.ensure(3 * static_cast<size_t>(P));
+        CK(cudaMemcpyAsync(body_of_instance.p, boi, P * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(local_pose.p, lp, 7 * P * sizeof(float), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(local_scale.p, sc, 3 * P * sizeof(float), cudaMemcpyHostToDevice, stream));
+        body_poses.ensure(7 * static_cast<size_t>(worlds) * bpw);
+        CK(cudaEventRecord(ev_done, stream));
+        wait(ev_done, timeout);  // the host arrays are the caller's; the copies must be done
+    }
+    bodies_per_world = bpw;
+    bound = true;
+}
+
+// src/batch.cpp:131-144 and src/cuda_backend.cu:493-507.
+void Renderer::set_body_poses(const float *poses, int memory) {
+    require(bound, "set_body_poses needs bind_bodies to be called first");
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    const size_t bodies = static_cast<size_t>(worlds) * bodies_per_world;
+    require(bodies == 0 || poses != nullptr, "body_poses must not be null");
+    if (memory == NGB_MEMORY_HOST)
+        for (size_t b = 0; b < bodies; ++b)
+            require(all_finite(poses + 7 * b, 7) && quaternion_is_usable(poses + 7 * b + 3),
+                "body " + std::to_string(b) + " has a NaN or infinite value, or a zero quaternion");
+    if (per_world == 0) return;
+    const float *src = poses;
+    if (memory == NGB_MEMORY_HOST && bodies > 0) {
+        CK(cudaMemcpyAsync(body_poses.p, poses, bodies * 7 * sizeof(float), cudaMemcpyHostToDevice, stream));
+        src = body_poses.p;
+    }
+    build(nullptr, true, src);
+    finish();
+}
+
+// src/batch.cpp:146-162: every argument check, in the reference's order.
+void Renderer::check_render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory) {
+    constexpr unsigned ALL = NGB_OUTPUT_RGB | NGB_OUTPUT_DEPTH | NGB_OUTPUT_NORMAL | NGB_OUTPUT_OBJECT_ID;
+    require(outputs != 0, "render needs at least one output");
+    require((outputs & ~ALL) == 0, "unknown output bits in " + std::to_string(outputs));
+    require(spp >= 1, "samples_per_pixel must be 1 or more, got " + std::to_string(spp));
+    require(frame >= 0, "frame must be 0 or more, got " + std::to_string(frame));
+    require(fov > 0.0f && fov < 3.14159265f, "fov must be between 0 and pi radians, got " + fstr(fov));
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    require(cams != nullptr, "camera_matrices must not be null");
+    if (memory == NGB_MEMORY_HOST)
+        require(all_finite(cams, 12 * static_cast<size_t>(worlds) * cpw), "a camera has a NaN or infinite value");
+}
+
+void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
+    float *depth, float *normal, int32_t *ids) {
+    const int views = worlds * cpw;
+    const float *cam = cams;
+    if (memory == NGB_MEMORY_HOST) {
+        cameras.ensure(12 * static_cast<size_t>(views));
+        CK(cudaMemcpyAsync(cameras.p, cams, 12 * static_cast<size_t>(views) * sizeof(float), cudaMemcpyHostToDevice, stream));
+        cam = cameras.p;
+    }
+    RenderArgs a{};
+    a.cameras = cam;
+    a.fov_scale = std::tan(fov * 0.5f);  // tanf on the host, as the reference's CPU backend computes it
+    a.aspect = static_cast<float>(width) / static_cast<float>(height);
+    a.width = width;
+    a.height = height;
+    a.cameras_per_world = cpw;
+    a.views = views;
+    a.frame = frame;
+    a.spp = spp;
+    a.rgb = (outputs & NGB_OUTPUT_RGB) ? rgb : nullptr;
+    a.depth = (outputs & NGB_OUTPUT_DEPTH) ? depth : nullptr;
+    a.normal = (outputs & NGB_OUTPUT_NORMAL) ? normal : nullptr;
+    a.object_id = (outputs & NGB_OUTPUT_OBJECT_ID) ? ids : nullptr;
+    if (record_hits && (outputs & (NGB_OUTPUT_DEPTH | NGB_OUTPUT_NORMAL | NGB_OUTPUT_OBJECT_ID))) {
+        a.hit_instance = hit_instance.ensure(pixels());
+        a.hit_triangle = hit_triangle.ensure(pixels());
+        a.hit_u = hit_u.ensure(pixels());
+        a.hit_v = hit_v.ensure(pixels());
+    }
+    a.error_flag = error_flag.p;
+    CK(cudaEventRecord(ev_start, stream));
+    CK(launch_render(params, a, stream));
+    CK(cudaEventRecord(ev_stop, stream));
+    timing_pending = true;
+    finish();
+}
+
+// src/batch.cpp:180-192 and src/cuda_backend.cu:547-585.
+void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory,
+    ngb_ray_hits *out, float *distance, float *normal, int32_t *ids) {
+    require(rays_per_world >= 0, "rays_per_world must be 0 or more, got " + std::to_string(rays_per_world));
+    const long long count = static_cast<long long>(rays_per_world) * worlds;
+    require(count <= INT32_MAX / 3, "too many rays: " + std::to_string(count));
+    require(count == 0 || (o != nullptr && d != nullptr), "ray origins and directions must not be null");
+    require(max_distance > 0.0f, "max_distance must be positive, got " + fstr(max_distance));
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    if (memory == NGB_MEMORY_HOST) require(all_finite(o, static_cast<size_t>(count) * 3), "a ray origin has a NaN or infinite value");
+    *out = ngb_ray_hits{NGB_MEMORY_DEVICE, device, static_cast<int32_t>(count), nullptr, nullptr, nullptr};
+    if (count == 0) return;
+    const float *po = o, *pd = d;
+    if (memory == NGB_MEMORY_HOST) {
+        ray_origins.ensure(3 * count);
+        ray_directions.ensure(3 * count);
+        CK(cudaMemcpyAsync(ray_origins.p, o, 3 * count * sizeof(float), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(ray_directions.p, d, 3 * count * sizeof(float), cudaMemcpyHostToDevice, stream));
+        po = ray_origins.p;
+        pd = ray_directions.p;
+    }
+    RayArgs a{};
+    a.origins = po;
+    a.directions = pd;
+    a.max_distance = max_distance;
+    a.rays_per_world = rays_per_world;
+    a.count = static_cast<int>(count);
+    a.distance = distance ? distance : ray_distance.ensure(count);
+    a.normal = normal ? normal : ray_normal.ensure(3 * count);
+    a.object_id = ids ? ids : ray_id.ensure(count);
+    a.error_flag = error_flag.p;
+    CK(cudaEventRecord(ev_start, stream));
+    CK(launch_rays(params, a, stream));
+    CK(cudaEventRecord(ev_stop, stream));
+    timing_pending = true;
+    finish();
+    out->distance = a.distance;
+    out->normal = a.normal;
+    out->object_id = a.object_id;
+}
+
+}  // namespace ngb
+
+// ------------------------------------------------------------------------------------------- C ABI --
+
+struct ngb_renderer {
+    ngb::Renderer r;
+    explicit ngb_renderer(const ngb_scene &s) : r(s) {}
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(ngb_renderer *h, F &&f) {
+    if (h == nullptr) {
+        g_create_error = "the renderer is null (destroyed or never created)";
+        return NGB_LOGIC_ERROR;
+    }
+    std::lock_guard<std::mutex> lock(h->r.mutex);
+    try {
+        ngb::DeviceGuard guard(h->r.device);
+        f(h->r);
+        h->r.last_error.clear();
+        return NGB_OK;
+    } catch (const ngb::InvalidArgument &e) {
+        h->r.last_error = e.what();
+        return NGB_INVALID_ARGUMENT;
+    } catch (const ngb::Timeout &e) {
+        h->r.last_error = e.what();
+        return NGB_TIMEOUT;
+    } catch (const std::bad_alloc &) {
+        h->r.last_error = "out of host memory";
+        return NGB_CUDA_ERROR;
+    } catch (const std::exception &e) {
+        h->r.last_error = e.what();
+        return NGB_CUDA_ERROR;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ngb_create(const ngb_scene *scene, ngb_renderer **out) {
+    if (out) *out = nullptr;
+    try {
+        ngb::require(scene != nullptr && out != nullptr, "scene and out must not be null");
+        *out = new ngb_renderer(*scene);
+        g_create_error.clear();
+        return NGB_OK;
+    } catch (const ngb::InvalidArgument &e) {
+        g_create_error = e.what();
+        return NGB_INVALID_ARGUMENT;
+    } catch (const ngb::Timeout &e) {
+        g_create_error = e.what();
+        return NGB_TIMEOUT;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return NGB_CUDA_ERROR;
+    }
+}
+
+void ngb_destroy(ngb_renderer *r) { delete r; }
+
+const char *ngb_last_error(const ngb_renderer *r) { return r ? r->r.last_error.c_str() : g_create_error.c_str(); }
+
+int ngb_set_instance_transforms(ngb_renderer *h, const float *m, int32_t memory) {
+    return guarded(h, [&](ngb::Renderer &r) { r.set_instance_transforms(m, memory); });
+}
+
+int ngb_bind_bodies(ngb_renderer *h, int32_t bpw, const int32_t *boi, const float *lp, const float *sc) {
+    return guarded(h, [&](ngb::Renderer &r) { r.bind_bodies(bpw, boi, lp, sc); });
+}
+
+int ngb_set_body_poses(ngb_renderer *h, const float *poses, int32_t memory) {
+    return guarded(h, [&](ngb::Renderer &r) { r.set_body_poses(poses, memory); });
+}
+
+int ngb_render(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint32_t outputs, int32_t frame,
+    int32_t camera_memory, ngb_batch_frame *out) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.check_render(cams, fov, spp, outputs, frame, camera_memory);
+        ngb::require(out != nullptr, "out must not be null");
+        const size_t px = r.pixels();
+        uint8_t *rgb = (outputs & NGB_OUTPUT_RGB) ? r.out_rgb.ensure(3 * px) : nullptr;
+        float *depth = (outputs & NGB_OUTPUT_DEPTH) ? r.out_depth.ensure(px) : nullptr;
+        float *normal = (outputs & NGB_OUTPUT_NORMAL) ? r.out_normal.ensure(3 * px) : nullptr;
+        int32_t *ids = (outputs & NGB_OUTPUT_OBJECT_ID) ? r.out_id.ensure(px) : nullptr;
+        r.render(cams, fov, spp, outputs, frame, camera_memory, rgb, depth, normal, ids);
+        *out = ngb_batch_frame{NGB_MEMORY_DEVICE, r.device, r.worlds * r.cpw, r.width, r.height, rgb, depth, normal, ids};
+    });
+}
+
+int ngb_render_into(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint32_t outputs, int32_t frame,
+    int32_t camera_memory, uint8_t *rgb, float *depth, float *normal, int32_t *object_id) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.check_render(cams, fov, spp, outputs, frame, camera_memory);
+        ngb::require(!(outputs & NGB_OUTPUT_RGB) || rgb, "rgb must not be null when the picture is asked for");
+        ngb::require(!(outputs & NGB_OUTPUT_DEPTH) || depth, "depth must not be null when depth is asked for");
+        ngb::require(!(outputs & NGB_OUTPUT_NORMAL) || normal, "normal must not be null when normals are asked for");
+        ngb::require(!(outputs & NGB_OUTPUT_OBJECT_ID) || object_id, "object_id must not be null when IDs are asked for");
+        r.render(cams, fov, spp, outputs, frame, camera_memory, rgb, depth, normal, object_id);
+    });
+}
+
+int ngb_render_host(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint32_t outputs, int32_t frame,
+    uint8_t *rgb, float *depth, float *normal, int32_t *object_id) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.check_render(cams, fov, spp, outputs, frame, NGB_MEMORY_HOST);
+        const size_t px = r.pixels();
+        uint8_t *drgb = (outputs & NGB_OUTPUT_RGB) ? r.out_rgb.ensure(3 * px) : nullptr;
+        float *ddepth = (outputs & NGB_OUTPUT_DEPTH) ? r.out_depth.ensure(px) : nullptr;
+        float *dnormal = (outputs & NGB_OUTPUT_NORMAL) ? r.out_normal.ensure(3 * px) : nullptr;
+        int32_t *dids = (outputs & NGB_OUTPUT_OBJECT_ID) ? r.out_id.ensure(px) : nullptr;
+        r.render(cams, fov, spp, outputs, frame, NGB_MEMORY_HOST, drgb, ddepth, dnormal, dids);
+        if (drgb && rgb) CK(cudaMemcpyAsync(rgb, drgb, 3 * px, cudaMemcpyDeviceToHost, r.stream));
+        if (ddepth && depth) CK(cudaMemcpyAsync(depth, ddepth, px * sizeof(float), cudaMemcpyDeviceToHost, r.stream));
+        if (dnormal && normal) CK(cudaMemcpyAsync(normal, dnormal, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, r.stream));
+        if (dids && object_id) CK(cudaMemcpyAsync(object_id, dids, px * sizeof(int32_t), cudaMemcpyDeviceToHost, r.stream));
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+    });
+}
+
+int ngb_cast_rays(ngb_renderer *h, const float *o, const float *d, int32_t rays_per_world, float max_distance,
+    int32_t memory, ngb_ray_hits *out) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(out != nullptr, "out must not be null");
+        r.cast_rays(o, d, rays_per_world, max_distance, memory, out, nullptr, nullptr, nullptr);
+    });
+}
+
+int ngb_cast_rays_into(ngb_renderer *h, const float *o, const float *d, int32_t rays_per_world, float max_distance,
+    int32_t memory, float *distance, float *normal, int32_t *object_id) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(distance != nullptr && normal != nullptr && object_id != nullptr,
+            "distance, normal and object_id must not be null");
+        ngb_ray_hits out{};
+        r.cast_rays(o, d, rays_per_world, max_distance, memory, &out, distance, normal, object_id);
+    });
+}
+
+int ngb_copy_to_host(ngb_renderer *h, const void *src, void *dst, size_t bytes) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(bytes == 0 || (src != nullptr && dst != nullptr), "src and dst must not be null");
+        if (bytes == 0) return;
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, r.stream));
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+    });
+}
+
+int ngb_set_ambient(ngb_renderer *h, float ambient) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(ngb::finite(ambient) && ambient >= 0.0f, "ambient must be 0 or more, got " + ngb::fstr(ambient));
+        r.params.ambient = ambient;
+    });
+}
+
+float ngb_ambient(const ngb_renderer *h) { return h ? h->r.params.ambient : 0.0f; }
+
+int ngb_set_environment(ngb_renderer *h, const ngb_environment *e) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(e != nullptr, "environment must not be null");
+        ngb::check_environment(*e);
+        // The gradient's up axis, normalised in double (src/environment.cpp:31-38).
+        const double u[3] = {e->up.x, e->up.y, e->up.z};
+        const double un = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        r.params.env_up = make_float3(static_cast<float>(u[0] / un), static_cast<float>(u[1] / un), static_cast<float>(u[2] / un));
+        r.params.env_color_up = make_float3(e->color_up.x, e->color_up.y, e->color_up.z);
+        r.params.env_color_down = make_float3(e->color_down.x, e->color_down.y, e->color_down.z);
+        r.params.env_intensity = e->intensity;
+    });
+}
+
+int ngb_set_stream(ngb_renderer *h, void *stream) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.stream = stream ? static_cast<cudaStream_t>(stream) : r.own_stream;
+    });
+}
+
+int ngb_set_sync(ngb_renderer *h, int32_t synchronous, double timeout_seconds) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(timeout_seconds > 0.0, "timeout_seconds must be positive");
+        r.synchronous = synchronous != 0;
+        r.timeout = timeout_seconds;
+    });
+}
+
+int ngb_synchronize(ngb_renderer *h, double timeout_seconds) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, timeout_seconds > 0.0 ? timeout_seconds : r.timeout);
+        if (r.timing_pending) {
+            CK(cudaEventElapsedTime(&r.kernel_ms, r.ev_start, r.ev_stop));
+            r.timing_pending = false;
+        }
+        if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
+    });
+}
+
+int32_t ngb_width(const ngb_renderer *h) { return h ? h->r.width : 0; }
+int32_t ngb_height(const ngb_renderer *h) { return h ? h->r.height : 0; }
+int32_t ngb_world_count(const ngb_renderer *h) { return h ? h->r.worlds : 0; }
+int32_t ngb_cameras_per_world(const ngb_renderer *h) { return h ? h->r.cpw : 0; }
+int32_t ngb_view_count(const ngb_renderer *h) { return h ? h->r.worlds * h->r.cpw : 0; }
+int32_t ngb_instances_per_world(const ngb_renderer *h) { return h ? h->r.per_world : 0; }
+
+float ngb_last_kernel_ms(const ngb_renderer *ch) {
+    ngb_renderer *h = const_cast<ngb_renderer *>(ch);
+    if (!h) return 0.0f;
+    float ms = 0.0f;
+    guarded(h, [&](ngb::Renderer &r) {
+        if (r.timing_pending) {
+            r.wait(r.ev_stop, r.timeout);
+            CK(cudaEventElapsedTime(&r.kernel_ms, r.ev_start, r.ev_stop));
+            r.timing_pending = false;
+        }
+        ms = r.kernel_ms;
+    });
+    return ms;
+}
+
+int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_count, int32_t *triangle_count,
+    int32_t *nodes, float *triangles, int32_t *roots, float *bounds, int32_t *triangle_index) {
+    try {
+        ngb::require(mesh_count >= 0 && (mesh_count == 0 || meshes) && node_count && triangle_count,
+            "meshes, node_count and triangle_count must not be null");
+        ngb_scene s{};
+        s.meshes = meshes;
+        s.mesh_count = mesh_count;
+        ngb::check_meshes(s);
+        const ngb::BuiltMeshes b = ngb::build_meshes(s);
+        *node_count = static_cast<int32_t>(b.nodes.size() / 8);
+        *triangle_count = static_cast<int32_t>(b.triangle_index.size());
+        if (nodes) std::memcpy(nodes, b.nodes.data(), b.nodes.size() * sizeof(float));
+        if (triangles) std::memcpy(triangles, b.triangles.data(), b.triangles.size() * sizeof(float));
+        if (roots) std::memcpy(roots, b.roots.data(), b.roots.size() * sizeof(int32_t));
+        if (bounds) std::memcpy(bounds, b.bounds.data(), b.bounds.size() * sizeof(float));
+        if (triangle_index) std::memcpy(triangle_index, b.triangle_index.data(), b.triangle_index.size() * sizeof(int32_t));
+        g_create_error.clear();
+        return NGB_OK;
+    } catch (const ngb::InvalidArgument &e) {
+        g_create_error = e.what();
+        return NGB_INVALID_ARGUMENT;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return NGB_CUDA_ERROR;
+    }
+}
+
+int ngb_record_hits(ngb_renderer *h, int32_t on) {
+    return guarded(h, [&](ngb::Renderer &r) { r.record_hits = on != 0; });
+}
+
+int ngb_inspect_tlas(ngb_renderer *h, uint64_t *keys, int32_t *sorted_ids, int32_t *nodes, int32_t *roots,
+    float *matrices) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+        const size_t n = static_cast<size_t>(r.n);
+        if (n == 0) return;
+        if (keys) CK(cudaMemcpy(keys, r.keys.p, n * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        if (sorted_ids) CK(cudaMemcpy(sorted_ids, r.sorted_ids.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (nodes) CK(cudaMemcpy(nodes, r.tlas.p, (2 * n - 1) * 32, cudaMemcpyDeviceToHost));
+        if (roots) CK(cudaMemcpy(roots, r.roots.p, r.worlds * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (matrices) CK(cudaMemcpy(matrices, r.matrices.p, n * 48, cudaMemcpyDeviceToHost));
+    });
+}
+
+int ngb_inspect_hits(ngb_renderer *h, int32_t *instance, int32_t *triangle, float *u, float *v) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(r.hit_instance.p != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+        const size_t px = r.pixels();
+        if (instance) CK(cudaMemcpy(instance, r.hit_instance.p, px * 4, cudaMemcpyDeviceToHost));
+        if (triangle) CK(cudaMemcpy(triangle, r.hit_triangle.p, px * 4, cudaMemcpyDeviceToHost));
+        if (u) CK(cudaMemcpy(u, r.hit_u.p, px * 4, cudaMemcpyDeviceToHost));
+        if (v) CK(cudaMemcpy(v, r.hit_v.p, px * 4, cudaMemcpyDeviceToHost));
+    });
+}
+
+}  // extern "C"

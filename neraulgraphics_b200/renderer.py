@@ -1,0 +1,311 @@
+"""BatchRenderer: the reference's Python class (python/bindings.cpp:667-799), over the C ABI.
+
+Arrays may be NumPy arrays (host: checked, then copied) or CUDA tensors from PyTorch (device: used where
+they are, on PyTorch's current stream, unchecked, as in the reference). With zero_copy=True the images
+come back as CUDA tensors that alias the renderer's own buffers, overwritten by the next render; work is
+queued on PyTorch's current stream, so PyTorch code on that stream sees it in order. Otherwise they come
+back as NumPy copies.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+from ._lib import CudaError, check, lib
+from .scene import Environment, Plane, SceneDesc
+
+_TIMEOUT_S = 120.0
+
+
+def _torch():
+    import torch  # plumbing only: device memory and streams
+    return torch
+
+
+def _is_cuda_tensor(a) -> bool:
+    return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
+
+
+def _count(a) -> int:
+    return int(np.prod(a.shape)) if len(a.shape) else 1
+
+
+def _require_count(a, expected, what, shape):
+    if _count(a) != expected:
+        raise ValueError(f"{what} has {_count(a)} values, but {expected} are needed: {shape}")
+
+
+def _parse_device(device) -> int:
+    if device in ("auto", "cuda", None):
+        return 0
+    if isinstance(device, int):
+        return device
+    if isinstance(device, str) and device.startswith("cuda:"):
+        return int(device.split(":", 1)[1])
+    if device == "cpu":
+        raise ValueError("device 'cpu' is not available: this renderer runs on CUDA GPUs only")
+    raise ValueError(f"device must be 'auto', 'cuda' or 'cuda:N', got '{device}'")
+
+
+class BatchRenderer:
+    """Many worlds rendered at once: thousands of copies of one environment, each seen by its own camera(s).
+
+    All worlds share the meshes, lights, spheres and floor. Each holds the same list of instances, placed
+    differently, and a camera sees only its own world's. Views are numbered world-major: view v looks at
+    world v // cameras_per_world.
+    """
+
+    def __init__(self, width, height, world_count, cameras_per_world=1, spheres=(), lights=(), floor=None,
+                 meshes=(), instances=(), textures=(), device="auto"):
+        if textures:
+            raise ValueError("textures are not supported by this renderer")
+        self._device = _parse_device(device)
+        self._desc = SceneDesc(width, height, world_count, cameras_per_world, spheres, lights,
+                               floor if floor is not None else Plane(), meshes, instances, self._device)
+        self._lib = lib()
+        h = C.c_void_p()
+        check(self._lib.ngb_create(C.byref(self._desc.c), C.byref(h)), None)
+        self._h = h
+        # Stream-ordered on PyTorch's current stream.
+        check(self._lib.ngb_set_sync(self._h, 0, _TIMEOUT_S), self._h)
+        self._out = {}
+        self._rays = {}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.ngb_destroy(h)
+            self._h = None
+
+    # ------------------------------------------------------------------------------------------- plumbing --
+
+    def _stream(self):
+        torch = _torch()
+        s = torch.cuda.current_stream(self._device).cuda_stream
+        check(self._lib.ngb_set_stream(self._h, C.c_void_p(s)), self._h)
+
+    def _input(self, a, what):
+        """(pointer, memory, keep-alive) for a float32 input: a CUDA tensor in place, else a host copy."""
+        if _is_cuda_tensor(a):
+            torch = _torch()
+            if a.device.index != self._device:
+                raise ValueError(f"{what} is on cuda:{a.device.index}, but the renderer is on cuda:{self._device}")
+            t = a if (a.dtype == torch.float32 and a.is_contiguous()) else a.to(torch.float32).contiguous()
+            return C.c_void_p(t.data_ptr()), _abi.MEMORY_DEVICE, t
+        if type(a).__module__.startswith("torch"):
+            a = a.numpy()
+        arr = np.ascontiguousarray(a, dtype=np.float32)
+        return arr.ctypes.data_as(C.c_void_p), _abi.MEMORY_HOST, arr
+
+    # ----------------------------------------------------------------------------------------- placement --
+
+    def set_instance_transforms(self, matrices):
+        """Place every instance of every world: (world_count, instances_per_world, 3, 4) float32."""
+        expected = self.world_count * self.instances_per_world * 12
+        _require_count(matrices, expected, "matrices",
+                       "(world_count, instances_per_world, 3, 4), the top three rows of each 4x4")
+        p, mem, keep = self._input(matrices, "matrices")
+        self._stream()
+        check(self._lib.ngb_set_instance_transforms(self._h, p, mem), self._h)
+        self._keep = keep
+
+    def bind_bodies(self, body_of_instance, local_pose, scale, bodies_per_world):
+        """How simulator bodies carry the instances (per instance: body or -1, x y z qx qy qz qw, scale xyz)."""
+        b = np.ascontiguousarray(body_of_instance, np.int32)
+        lp = np.ascontiguousarray(local_pose, np.float32)
+        sc = np.ascontiguousarray(scale, np.float32)
+        n = self.instances_per_world
+        if b.size != n or lp.size != 7 * n or sc.size != 3 * n:
+            raise ValueError(f"a body binding needs one body index, 7 pose floats and 3 scale floats for each of the "
+                             f"{n} instances of a world")
+        self._stream()
+        check(self._lib.ngb_bind_bodies(self._h, int(bodies_per_world), b.ctypes.data_as(C.POINTER(C.c_int32)),
+                                        lp.ctypes.data_as(C.POINTER(C.c_float)),
+                                        sc.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+        self._bodies_per_world = int(bodies_per_world)
+
+    def set_body_poses(self, body_poses):
+        """Place every instance from body poses: (world_count, bodies_per_world, 7) floats, x y z qx qy qz qw."""
+        p, mem, keep = self._input(body_poses, "body poses")
+        bpw = getattr(self, "_bodies_per_world", None)
+        if bpw is not None:
+            _require_count(body_poses, self.world_count * bpw * 7, "body poses", "(world_count, bodies_per_world, 7)")
+        self._stream()
+        check(self._lib.ngb_set_body_poses(self._h, p, mem), self._h)
+        self._keep = keep
+
+    # ------------------------------------------------------------------------------------------ rendering --
+
+    def _buffer(self, key, shape, dtype):
+        torch = _torch()
+        t = self._out.get(key)
+        if t is None or tuple(t.shape) != shape:
+            t = torch.empty(shape, dtype=dtype, device=f"cuda:{self._device}")
+            self._out[key] = t
+        return t
+
+    def render(self, cameras, fov=1.0, samples_per_pixel=1, *, rgb=True, depth=False, normals=False,
+               object_ids=False, frame=0, zero_copy=False, out=None):
+        """Render every view; returns a dict of 'rgb' (V,H,W,3) uint8, 'depth' (V,H,W) float32, 'normals'
+        (V,H,W,3) float32, 'object_ids' (V,H,W) int32, for the images asked for.
+
+        out: optional dict of preallocated host (NumPy) arrays, pinned or not, to copy the images into
+        (BatchRenderer::render_host, src/batch.cpp:164-178); cameras must then be on the host."""
+        torch = _torch()
+        views, h, w = self.view_count, self.height, self.width
+        if out is not None:
+            return self._render_host(cameras, fov, samples_per_pixel, rgb, depth, normals, object_ids, frame, out)
+        _require_count(cameras, views * 12, "cameras", f"{views} cameras of 3 x 4 numbers (camera-to-world)")
+        if not zero_copy and _is_cuda_tensor(cameras):
+            raise ValueError("cameras on the GPU need zero_copy=True: the results then stay on the GPU too")
+        outputs = ((_abi.OUTPUT_RGB if rgb else 0) | (_abi.OUTPUT_DEPTH if depth else 0) |
+                   (_abi.OUTPUT_NORMAL if normals else 0) | (_abi.OUTPUT_OBJECT_ID if object_ids else 0))
+        bufs = {}
+        if rgb:
+            bufs["rgb"] = self._buffer("rgb", (views, h, w, 3), torch.uint8)
+        if depth:
+            bufs["depth"] = self._buffer("depth", (views, h, w), torch.float32)
+        if normals:
+            bufs["normals"] = self._buffer("normals", (views, h, w, 3), torch.float32)
+        if object_ids:
+            bufs["object_ids"] = self._buffer("object_ids", (views, h, w), torch.int32)
+        p, mem, keep = self._input(cameras, "cameras")
+        ptr = lambda k: C.c_void_p(bufs[k].data_ptr()) if k in bufs else None
+        self._stream()
+        check(self._lib.ngb_render_into(self._h, p, float(fov), int(samples_per_pixel), outputs, int(frame), mem,
+                                        ptr("rgb"), ptr("depth"), ptr("normals"), ptr("object_ids")), self._h)
+        self._keep = keep
+        if zero_copy:
+            return dict(bufs)
+        return {k: v.cpu().numpy() for k, v in bufs.items()}
+
+    def _render_host(self, cameras, fov, spp, rgb, depth, normals, object_ids, frame, out):
+        views, h, w = self.view_count, self.height, self.width
+        _require_count(cameras, views * 12, "cameras", f"{views} cameras of 3 x 4 numbers (camera-to-world)")
+        if _is_cuda_tensor(cameras):
+            raise ValueError("render(out=...) copies to host memory and takes cameras in host memory")
+        want = {"rgb": ((views, h, w, 3), np.uint8, rgb), "depth": ((views, h, w), np.float32, depth),
+                "normals": ((views, h, w, 3), np.float32, normals), "object_ids": ((views, h, w), np.int32, object_ids)}
+        ptrs = {}
+        for k, (shape, dtype, on) in want.items():
+            if not on:
+                ptrs[k] = None
+                continue
+            a = out.get(k)
+            if a is None or a.shape != shape or a.dtype != dtype or not a.flags.c_contiguous:
+                raise ValueError(f"out['{k}'] must be a C-contiguous {np.dtype(dtype).name} array of shape {shape}")
+            ptrs[k] = a.ctypes.data_as(C.c_void_p)
+        outputs = ((_abi.OUTPUT_RGB if rgb else 0) | (_abi.OUTPUT_DEPTH if depth else 0) |
+                   (_abi.OUTPUT_NORMAL if normals else 0) | (_abi.OUTPUT_OBJECT_ID if object_ids else 0))
+        cams = np.ascontiguousarray(cameras, np.float32)
+        self._stream()
+        check(self._lib.ngb_render_host(self._h, cams.ctypes.data_as(C.c_void_p), float(fov), int(spp), outputs,
+                                        int(frame), ptrs["rgb"], ptrs["depth"], ptrs["normals"], ptrs["object_ids"]),
+              self._h)
+        return {k: out[k] for k, v in ptrs.items() if v is not None}
+
+    def cast_rays(self, origins, directions, max_distance=math.inf):
+        """Rays in every world: (world_count, rays_per_world, 3) origins and directions. Returns distance
+        (W, R), normal (W, R, 3) and object_id (W, R); CUDA tensors in give CUDA tensors out."""
+        torch = _torch()
+        worlds = self.world_count
+        if _count(origins) % (3 * worlds) != 0:
+            raise ValueError(f"origins must hold 3 floats for each ray of each of the {worlds} worlds: "
+                             f"(world_count, rays_per_world, 3)")
+        _require_count(directions, _count(origins), "directions", "the same as origins")
+        rpw = _count(origins) // (3 * worlds)
+        po, mo, ko = self._input(origins, "origins")
+        pd, md, kd = self._input(directions, "directions")
+        if mo != md:
+            raise ValueError("origins and directions must be on the same device")
+        dev = f"cuda:{self._device}"
+        out = {"distance": torch.empty((worlds, rpw), dtype=torch.float32, device=dev),
+               "normal": torch.empty((worlds, rpw, 3), dtype=torch.float32, device=dev),
+               "object_id": torch.empty((worlds, rpw), dtype=torch.int32, device=dev)}
+        ptr = lambda k: C.c_void_p(out[k].data_ptr()) if out[k].numel() else C.c_void_p(1)
+        self._stream()
+        check(self._lib.ngb_cast_rays_into(self._h, po, pd, rpw, float(max_distance), mo, ptr("distance"),
+                                           ptr("normal"), ptr("object_id")), self._h)
+        self._keep = (ko, kd)
+        if mo == _abi.MEMORY_DEVICE:
+            return out
+        return {k: v.cpu().numpy() for k, v in out.items()}
+
+    # ------------------------------------------------------------------------------------------- settings --
+
+    def set_environment(self, environment: Environment):
+        e = environment.to_abi()
+        check(self._lib.ngb_set_environment(self._h, C.byref(e)), self._h)
+
+    @property
+    def ambient(self) -> float:
+        return float(self._lib.ngb_ambient(self._h))
+
+    @ambient.setter
+    def ambient(self, value):
+        check(self._lib.ngb_set_ambient(self._h, float(value)), self._h)
+
+    @property
+    def width(self) -> int:
+        return int(self._lib.ngb_width(self._h))
+
+    @property
+    def height(self) -> int:
+        return int(self._lib.ngb_height(self._h))
+
+    @property
+    def world_count(self) -> int:
+        return int(self._lib.ngb_world_count(self._h))
+
+    @property
+    def cameras_per_world(self) -> int:
+        return int(self._lib.ngb_cameras_per_world(self._h))
+
+    @property
+    def view_count(self) -> int:
+        return int(self._lib.ngb_view_count(self._h))
+
+    @property
+    def instances_per_world(self) -> int:
+        return int(self._lib.ngb_instances_per_world(self._h))
+
+    @property
+    def device(self) -> str:
+        return "cuda"
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return float(self._lib.ngb_last_kernel_ms(self._h))
+
+    def synchronize(self, timeout=_TIMEOUT_S):
+        check(self._lib.ngb_synchronize(self._h, float(timeout)), self._h)
+
+    # ----------------------------------------------------------------------------------------- inspection --
+
+    def record_hits(self, on=True):
+        check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
+
+    def inspect_tlas(self) -> dict:
+        """The last tree build: keys (instance order), sorted ids, nodes (8 words), roots, matrices."""
+        n = self.world_count * self.instances_per_world
+        keys = np.zeros(n, np.uint64)
+        ids = np.zeros(n, np.int32)
+        nodes = np.zeros((max(2 * n - 1, 0), 8), np.int32)
+        roots = np.zeros(self.world_count, np.int32)
+        mats = np.zeros((n, 12), np.float32)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(self._lib.ngb_inspect_tlas(self._h, vp(keys), vp(ids), vp(nodes), vp(roots), vp(mats)), self._h)
+        return {"keys": keys, "sorted_ids": ids, "nodes": nodes, "roots": roots, "matrices": mats}
+
+    def inspect_hits(self) -> dict:
+        shape = (self.view_count, self.height, self.width)
+        inst, tri = np.zeros(shape, np.int32), np.zeros(shape, np.int32)
+        u, v = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(self._lib.ngb_inspect_hits(self._h, vp(inst), vp(tri), vp(u), vp(v)), self._h)
+        return {"hit_instance": inst, "hit_triangle": tri, "hit_u": u, "hit_v": v}
+

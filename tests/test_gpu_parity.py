@@ -1,0 +1,270 @@
+"""GPU parity tests: the CUDA path, through the C ABI, against the oracle and the reference's own outputs.
+
+The bar: tree keys, sorted orders, links and roots bit-exact; object IDs, hit triangles, depth and normals
+bit-exact against the oracle on the same trees (and against the reference except where the two nearest hits
+of a ray lie within 1e-6 relative t, which the oracle flags); RGB within one uint8 level (CUDA's sinf, cosf
+and powf are within a few ulp of the host's).
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+import neraulgraphics_b200 as ng
+import oracle as O
+import scenes
+from neraulgraphics_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+ALL = dict(rgb=True, depth=True, normals=True, object_ids=True)
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def product(desc):
+    return ng.BatchRenderer(desc.width, desc.height, desc.world_count, desc.cameras_per_world, desc.spheres,
+                            desc.lights, desc.floor, desc.meshes, desc.instances, device="cuda:0")
+
+
+def assert_same_images(got, want, rgb_tol=1):
+    for k in ("object_ids",):
+        if k in want:
+            assert np.array_equal(got[k], want[k]), k
+    for k in ("depth", "normals"):
+        if k in want:
+            assert np.array_equal(bits(got[k]), bits(want[k])), k
+    if "rgb" in want:
+        d = np.abs(got["rgb"].astype(int) - want["rgb"].astype(int))
+        assert d.max() <= rgb_tol, f"rgb differs by up to {d.max()} levels at {(d.max(-1) > rgb_tol).sum()} pixels"
+
+
+def assert_same_tlas(got, want):
+    assert np.array_equal(got["keys"], want["keys"])
+    assert np.array_equal(got["sorted_ids"], want["sorted_ids"])
+    assert np.array_equal(got["roots"], want["roots"])
+    assert np.array_equal(got["nodes"][:, [3, 7]], want["nodes"][:, [3, 7]])
+    gb, wb = got["nodes"][:, [0, 1, 2, 4, 5, 6]].view(np.float32), want["nodes"][:, [0, 1, 2, 4, 5, 6]].view(np.float32)
+    assert np.array_equal(gb, wb)  # float equality: -0 and +0 are the same box
+    assert np.array_equal(bits(got["matrices"]), bits(want["matrices"]))
+
+
+@pytest.mark.parametrize("case", ["icospheres", "scattered", "coincident", "single_leaf", "bodies", "one_world"])
+def test_tree_build_is_the_oracles(torch_cuda, case):
+    if case == "icospheres":
+        wl = workloads.icosphere_worlds()
+        desc, mats = wl.desc, wl.matrices
+    elif case == "scattered":
+        desc, mats, _ = scenes.scattered_boxes(300, 40)
+    elif case == "coincident":
+        desc, mats, _ = scenes.coincident_boxes()
+    elif case == "single_leaf":
+        desc, mats, _ = scenes.single_leaf_worlds()
+    elif case == "one_world":
+        desc, mats, _ = scenes.scattered_boxes(1, 1000)
+    else:
+        wl = workloads.body_worlds(worlds=256)
+        desc, mats = wl.desc, None
+    r, o = product(desc), O.Oracle(desc)
+    if mats is not None:
+        r.set_instance_transforms(mats)
+        o.set_instance_transforms(mats)
+    else:
+        steps = workloads.random_walk(wl.poses, 2)
+        r.bind_bodies(**wl.binding)
+        o.bind_bodies(**wl.binding)
+        for s in steps:
+            r.set_body_poses(s)
+            o.set_body_poses(s)
+    assert_same_tlas(r.inspect_tlas(), o.tlas())
+
+
+def test_render_icospheres_is_the_oracles_and_the_references(torch_cuda):
+    f = np.load(os.path.join(GOLDEN, "icosphere_16x8_seed0.npz"))
+    wl = workloads.icosphere_worlds()
+    r, o = product(wl.desc), O.Oracle(wl.desc)
+    r.set_instance_transforms(f["matrices"])
+    o.set_instance_transforms(f["matrices"])
+    r.record_hits(True)
+    got = r.render(f["cameras"], float(f["fov"]), 1, **ALL)
+    want = o.render(f["cameras"], float(f["fov"]), 1, **ALL, hits=True)
+    assert_same_images(got, want)
+    assert_same_images(got, {k: f[k] for k in ("rgb", "depth", "normals", "object_ids")})
+    h = r.inspect_hits()
+    for k in ("hit_instance", "hit_triangle"):
+        assert np.array_equal(h[k], want[k]), k
+    for k in ("hit_u", "hit_v"):
+        assert np.array_equal(bits(h[k]), bits(want[k])), k
+
+
+def test_render_reference_test_scene(torch_cuda):
+    """Spheres, a mirror sphere (reflection bounces), two hard-shadow lights, a checker floor, smooth normals,
+    ambient 0.1, 2 samples per pixel, frame 5: against the reference's own images."""
+    f = np.load(os.path.join(GOLDEN, "template_6w_spp2_frame5.npz"))
+    r = product(scenes.template(worlds=6))
+    r.set_instance_transforms(f["matrices"])
+    r.ambient = float(f["ambient"])
+    got = r.render(f["cameras"], float(f["fov"]), 2, **ALL, frame=5)
+    assert_same_images(got, {k: f[k] for k in ("rgb", "depth", "normals", "object_ids")})
+
+
+def test_body_poses_and_rays_against_the_reference(torch_cuda):
+    f = np.load(os.path.join(GOLDEN, "body_16x20_seed0.npz"))
+    wl = workloads.body_worlds(worlds=16, seed=0)
+    r = product(wl.desc)
+    r.bind_bodies(**wl.binding)
+    r.set_body_poses(f["poses"])
+    assert np.array_equal(bits(r.inspect_tlas()["matrices"].reshape(f["matrices"].shape)), bits(f["matrices"]))
+    got = r.render(f["cameras"], float(f["fov"]), 1, rgb=True, depth=True, object_ids=True)
+    assert_same_images(got, {k: f[k] for k in ("rgb", "depth", "object_ids")})
+    hits = r.cast_rays(f["ray_origins"], f["ray_directions"], 20.0)
+    assert np.array_equal(hits["object_id"], f["ray_object_id"])
+    assert np.array_equal(bits(hits["distance"]), bits(f["ray_distance"]))
+    assert np.array_equal(bits(hits["normal"]), bits(f["ray_normal"]))
+
+
+def test_scattered_worlds_against_the_oracle(torch_cuda):
+    desc, mats, cams = scenes.scattered_boxes(300, 40)
+    r, o = product(desc), O.Oracle(desc)
+    r.set_instance_transforms(mats)
+    o.set_instance_transforms(mats)
+    assert_same_images(r.render(cams, scenes.FOV, 1, **ALL), o.render(cams, scenes.FOV, 1, **ALL))
+
+
+def test_known_answers(torch_cuda):
+    desc, mats, cams = scenes.one_box_worlds()
+    r = product(desc)
+    r.set_instance_transforms(mats)
+    d = r.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[:, scenes.H // 2, scenes.W // 2] == pytest.approx([7.0, 2.0], abs=0.02)
+    hits = r.cast_rays(np.zeros((2, 1, 3), np.float32), np.tile(np.float32([0, 0, -1]), (2, 1, 1)), 100.0)
+    assert hits["distance"][:, 0] == pytest.approx([7.0, 2.0], abs=1e-3)
+    assert (hits["object_id"] == ng.OBJECT_INSTANCE).all()
+    desc, mats, cams = scenes.single_leaf_worlds()
+    r = product(desc)
+    r.set_instance_transforms(mats)
+    d = r.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[:, scenes.H // 2, scenes.W // 2] == pytest.approx([3.0, 4.0, 5.0, 6.0], abs=0.02)
+    desc, mats, cams = scenes.coincident_boxes()
+    r = product(desc)
+    r.set_instance_transforms(mats)
+    d = r.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[0, scenes.H // 2, scenes.W // 2] == pytest.approx(4.8, abs=0.02)
+
+
+def test_worlds_without_instances(torch_cuda):
+    desc = scenes.template(worlds=3)
+    desc = ng.SceneDesc(desc.width, desc.height, 3, 1, desc.spheres, desc.lights, desc.floor)
+    r = product(desc)
+    r.set_instance_transforms(np.zeros((0,), np.float32))
+    cams = np.stack([scenes.camera()] * 3)
+    got = r.render(cams, scenes.FOV, 1, **ALL)
+    want = O.Oracle(desc).render(cams, scenes.FOV, 1, **ALL)
+    assert_same_images(got, want)
+
+
+def test_many_worlds_several_cameras(torch_cuda):
+    desc = scenes.template(worlds=200, cameras_per_world=2)
+    mats = scenes.template_matrices(200)
+    cams = np.stack([scenes.camera((0.3 * (v % 2), 0.5, 0)) for v in range(400)])
+    r, o = product(desc), O.Oracle(desc)
+    r.set_instance_transforms(mats)
+    o.set_instance_transforms(mats)
+    out = dict(rgb=False, depth=True, object_ids=True)
+    assert_same_images(r.render(cams, scenes.FOV, 1, **out), o.render(cams, scenes.FOV, 1, **out))
+
+
+def test_device_inputs_and_zero_copy(torch_cuda):
+    torch = torch_cuda
+    wl = workloads.icosphere_worlds()
+    d = wl.desc
+    host, dev = product(d), product(d)
+    host.set_instance_transforms(wl.matrices)
+    dev.set_instance_transforms(torch.from_numpy(wl.matrices).cuda())
+    want = host.render(wl.cameras, wl.fov, 1, **ALL)
+    got = dev.render(torch.from_numpy(wl.cameras).cuda(), wl.fov, 1, **ALL, zero_copy=True)
+    assert all(v.is_cuda for v in got.values()) and tuple(got["rgb"].shape) == (16, 64, 64, 3)
+    assert_same_images({k: v.cpu().numpy() for k, v in got.items()}, want, rgb_tol=0)
+    first = got["depth"]
+    kept = first.clone()
+    second = dev.render(torch.from_numpy(wl.cameras[::-1].copy()).cuda(), wl.fov, 1, rgb=False, depth=True,
+                        zero_copy=True)["depth"]
+    assert second.data_ptr() == first.data_ptr() and not torch.equal(first, kept)
+    with pytest.raises(ValueError, match="cameras on the GPU need zero_copy=True"):
+        dev.render(torch.from_numpy(wl.cameras).cuda(), wl.fov)
+
+
+def test_body_poses_from_a_gpu_tensor(torch_cuda):
+    torch = torch_cuda
+    wl = workloads.body_worlds(worlds=64)
+    a, b, o = product(wl.desc), product(wl.desc), O.Oracle(wl.desc)
+    for x in (a, b, o):
+        x.bind_bodies(**wl.binding)
+    a.set_body_poses(wl.poses)
+    b.set_body_poses(torch.from_numpy(wl.poses).cuda())
+    o.set_body_poses(wl.poses)
+    assert_same_tlas(b.inspect_tlas(), o.tlas())
+    out = dict(rgb=True, depth=True, object_ids=True)
+    assert_same_images(b.render(wl.cameras, 1.0, 1, **out), a.render(wl.cameras, 1.0, 1, **out), rgb_tol=0)
+    assert_same_images(b.render(wl.cameras, 1.0, 1, **out), o.render(wl.cameras, 1.0, 1, **out))
+
+
+def test_rejected_input_changes_nothing(torch_cuda):
+    desc = scenes.template(worlds=2)
+    mats = scenes.template_matrices(2)
+    r = product(desc)
+    r.set_instance_transforms(mats)
+    cams = np.stack([scenes.camera((0, 0, 0))] * 2)
+    before = r.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"].copy()
+    singular = mats.copy()
+    singular[1, 1] = 0
+    with pytest.raises(ValueError, match="world 1 instance 1 transform is singular"):
+        r.set_instance_transforms(singular)
+    bad = mats.copy()
+    bad[0, 2, 1, 3] = np.nan
+    with pytest.raises(ValueError, match="world 0 instance 2 transform has a NaN or infinite value"):
+        r.set_instance_transforms(bad)
+    with pytest.raises(ValueError, match="matrices has 12 values, but 72 are needed"):
+        r.set_instance_transforms(np.zeros((1, 3, 4), np.float32))
+    with pytest.raises(ValueError, match="render needs at least one output"):
+        r.render(cams, scenes.FOV, rgb=False)
+    with pytest.raises(ValueError, match="samples_per_pixel must be 1 or more, got 0"):
+        r.render(cams, scenes.FOV, 0)
+    for fov in (0.0, 4.0, float("nan")):
+        with pytest.raises(ValueError, match="fov must be between 0 and pi radians"):
+            r.render(cams, fov)
+    with pytest.raises(ValueError, match="frame must be 0 or more, got -1"):
+        r.render(cams, scenes.FOV, frame=-1)
+    nan_cam = cams.copy()
+    nan_cam[0, 0, 3] = np.nan
+    with pytest.raises(ValueError, match="a camera has a NaN or infinite value"):
+        r.render(nan_cam, scenes.FOV)
+    with pytest.raises(ValueError, match="2 cameras of 3 x 4"):
+        r.render(cams[:1], scenes.FOV)
+    with pytest.raises(ValueError, match="set_body_poses needs bind_bodies to be called first"):
+        r.set_body_poses(np.zeros((2, 2, 7), np.float32))
+    with pytest.raises(ValueError, match="instance 2 is on body 5, but there are 1 bodies per world"):
+        r.bind_bodies([0, 0, 5], np.tile(np.float32([0, 0, 0, 0, 0, 0, 1]), (3, 1)), np.ones((3, 3)), 1)
+    with pytest.raises(ValueError, match="origins must hold 3 floats for each ray"):
+        r.cast_rays(np.zeros((1, 3), np.float32), np.zeros((1, 3), np.float32))
+    with pytest.raises(ValueError, match="max_distance must be positive"):
+        r.cast_rays(np.zeros((2, 1, 3), np.float32), np.ones((2, 1, 3), np.float32), 0.0)
+    with pytest.raises(ValueError, match="ambient must be 0 or more"):
+        r.ambient = -1.0
+    after = r.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert np.array_equal(bits(after), bits(before))
+
+
+def test_a_thousand_worlds_stay_in_gpu_memory(torch_cuda):
+    torch = torch_cuda
+    desc = scenes.template(worlds=1000)
+    r = product(desc)
+    r.set_instance_transforms(torch.from_numpy(scenes.template_matrices(1000)).cuda())
+    cams = torch.from_numpy(np.stack([scenes.camera()] * 1000)).cuda()
+    depth = r.render(cams, scenes.FOV, 1, rgb=False, depth=True, zero_copy=True)["depth"]
+    assert tuple(depth.shape) == (1000, scenes.H, scenes.W) and depth.is_cuda
+    assert float(torch.isfinite(depth).float().mean()) > 0.1
+    assert r.last_kernel_ms > 0

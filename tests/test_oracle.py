@@ -1,0 +1,229 @@
+"""CPU tests: the oracle is pinned to the reference (golden fixtures made by the reference itself, and the
+reference library when it is built here), and the product's host pieces match the reference bit-exactly."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle as O
+from neraulgraphics_b200 import scene as S, workloads
+import scenes
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+needs_ref = pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref/libngref.so is not built")
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def assert_images_equal(got, want, rgb_tol=0):
+    for k in ("object_ids", "depth", "normals"):
+        if k in want and k in got:
+            assert np.array_equal(bits(got[k]) if got[k].dtype == np.float32 else got[k],
+                                  bits(want[k]) if want[k].dtype == np.float32 else want[k]), k
+    if "rgb" in want and "rgb" in got:
+        d = np.abs(got["rgb"].astype(int) - want["rgb"].astype(int))
+        assert d.max() <= rgb_tol, f"rgb differs by {d.max()}"
+
+
+# ------------------------------------------------------------------------------- oracle vs golden --
+
+def test_oracle_matches_reference_fixture_icospheres():
+    f = np.load(os.path.join(GOLDEN, "icosphere_16x8_seed0.npz"))
+    wl = workloads.icosphere_worlds(worlds=16, per_world=8, seed=0)
+    assert np.array_equal(wl.matrices, f["matrices"]) and np.array_equal(wl.cameras, f["cameras"])
+    o = O.Oracle(wl.desc)
+    o.set_instance_transforms(f["matrices"])
+    got = o.render(f["cameras"], float(f["fov"]), 1, rgb=True, depth=True, normals=True, object_ids=True)
+    assert_images_equal(got, f)
+    assert (f["object_ids"] >= S._abi.OBJECT_INSTANCE).mean() > 0.05
+
+
+def test_oracle_matches_reference_fixture_template():
+    """Spheres, a mirror (reflection bounces), two hard-shadow lights, a checker floor, smooth normals,
+    ambient 0.1, 2 samples per pixel, frame 5."""
+    f = np.load(os.path.join(GOLDEN, "template_6w_spp2_frame5.npz"))
+    o = O.Oracle(scenes.template(worlds=6))
+    o.set_instance_transforms(f["matrices"])
+    o.set_ambient(float(f["ambient"]))
+    got = o.render(f["cameras"], float(f["fov"]), 2, rgb=True, depth=True, normals=True, object_ids=True, frame=5)
+    assert_images_equal(got, f)
+
+
+def test_oracle_matches_reference_fixture_bodies_and_rays():
+    f = np.load(os.path.join(GOLDEN, "body_16x20_seed0.npz"))
+    wl = workloads.body_worlds(worlds=16, seed=0)
+    o = O.Oracle(wl.desc)
+    o.bind_bodies(**wl.binding)
+    o.set_body_poses(f["poses"])
+    assert np.array_equal(bits(o.tlas()["matrices"].reshape(f["matrices"].shape)), bits(f["matrices"]))
+    got = o.render(f["cameras"], float(f["fov"]), 1, rgb=True, depth=True, object_ids=True)
+    assert_images_equal(got, f)
+    hits = o.cast_rays(f["ray_origins"], f["ray_directions"], 20.0)
+    assert np.array_equal(hits["object_id"], f["ray_object_id"])
+    assert np.array_equal(bits(hits["distance"]), bits(f["ray_distance"]))
+    assert np.array_equal(bits(hits["normal"]), bits(f["ray_normal"]))
+
+
+# --------------------------------------------------------------------------- known answers (oracle) --
+
+def test_oracle_known_answers():
+    desc, mats, cams = scenes.one_box_worlds()
+    o = O.Oracle(desc)
+    o.set_instance_transforms(mats)
+    d = o.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[:, scenes.H // 2, scenes.W // 2] == pytest.approx([7.0, 2.0], abs=0.02)
+    hits = o.cast_rays(np.zeros((2, 1, 3), np.float32), np.tile(np.float32([0, 0, -1]), (2, 1, 1)), 100.0)
+    assert hits["distance"][:, 0] == pytest.approx([7.0, 2.0], abs=1e-3)
+    assert (hits["object_id"] == S._abi.OBJECT_INSTANCE).all()
+    desc, mats, cams = scenes.single_leaf_worlds()
+    o = O.Oracle(desc)
+    o.set_instance_transforms(mats)
+    d = o.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[:, scenes.H // 2, scenes.W // 2] == pytest.approx([3.0, 4.0, 5.0, 6.0], abs=0.02)
+    desc, mats, cams = scenes.coincident_boxes()
+    o = O.Oracle(desc)
+    o.set_instance_transforms(mats)
+    d = o.render(cams, scenes.FOV, 1, rgb=False, depth=True)["depth"]
+    assert d[0, scenes.H // 2, scenes.W // 2] == pytest.approx(4.8, abs=0.02)
+
+
+def test_oracle_lbvh_structure():
+    """Every world's tree reaches each of its leaves once, links are consistent and boxes contain children."""
+    desc, mats, cams = scenes.scattered_boxes(30, 40)
+    o = O.Oracle(desc)
+    o.set_instance_transforms(mats)
+    t = o.tlas()
+    nodes, roots, n = t["nodes"], t["roots"], 30 * 40
+    lo = nodes[:, :3].view(np.float32)
+    hi = nodes[:, 4:7].view(np.float32)
+    for w in range(30):
+        seen, stack = [], [roots[w]]
+        while stack:
+            v = stack.pop()
+            left, right = nodes[v, 3], nodes[v, 7]
+            if left < 0:
+                seen.append(~left)
+                continue
+            for c in (left, right):
+                assert (lo[v] <= lo[c]).all() and (hi[v] >= hi[c]).all()
+                stack.append(c)
+        assert sorted(seen) == list(range(w * 40, (w + 1) * 40))
+    assert sorted(t["sorted_ids"]) == list(range(n))
+    keys = t["keys"][t["sorted_ids"]]
+    assert (np.diff(keys.astype(np.float64)) >= 0).all()
+
+
+# ------------------------------------------------------------------- host pieces vs the reference --
+
+@needs_ref
+@pytest.mark.parametrize("radius,sub", [(0.5, 2), (0.5, 3), (1.0, 1), (2.0, 4)])
+def test_icosphere_generator_is_the_references(radius, sub):
+    a, b = S.make_icosphere(radius, sub), O.ref_make_icosphere(radius, sub)
+    assert np.array_equal(bits(a.vertices), bits(b.vertices)) and np.array_equal(a.triangles, b.triangles)
+
+
+@needs_ref
+def test_transform_and_box_generators_are_the_references():
+    rng = np.random.default_rng(0)
+    for _ in range(500):
+        p, q, s = rng.uniform(-3, 3, 3), rng.normal(size=4), rng.uniform(0.2, 2)
+        assert np.array_equal(bits(S.make_transform(p, q, s).matrix), bits(O.ref_make_transform(p, q, s)))
+    a, b = S.make_box((0.4, 0.5, 0.6)), O.ref_make_box((0.4, 0.5, 0.6))
+    assert np.array_equal(a.vertices, b.vertices) and np.array_equal(a.triangles, b.triangles)
+    m = S.make_camera((0.1, 1.2, 0.3), (0, 0, -6), width=64, height=48, fov=1.0).matrix
+    assert np.array_equal(bits(m), bits(O.ref_camera_matrix((0.1, 1.2, 0.3), (0, 0, -6), (0, 1, 0), 1.0, 64, 48)))
+
+
+@needs_ref
+def test_blas_builders_are_the_references():
+    """The product's host builder (libngb.so) and the oracle's both give the reference's trees bit for bit."""
+    import neraulgraphics_b200 as ng
+    smooth = S.make_icosphere(1.0, 2)
+    meshes = [S.make_icosphere(0.5, 3), S.make_box((0.4, 0.4, 0.4)), S.cylinder(1.0, 1.0, 128),
+              S.Mesh(smooth.vertices, smooth.triangles, normals=smooth.vertices), S.make_icosphere(1.0, 5)]
+    want = O.ref_build_meshes(meshes)
+    got = ng.build_meshes(meshes)
+    inst = [S.Instance(i) for i in range(len(meshes))]
+    orc = O.Oracle(S.SceneDesc(8, 8, 1, meshes=meshes, instances=inst)).blas()
+    for k in ("nodes", "triangles", "roots", "bounds"):
+        w = bits(want[k]) if want[k].dtype == np.float32 else want[k]
+        for g in (got, orc):
+            x = bits(g[k]) if g[k].dtype == np.float32 else g[k]
+            assert np.array_equal(x, w), k
+    assert np.array_equal(got["triangle_index"], orc["triangle_index"])
+
+
+@needs_ref
+def test_oracle_compose_against_reference_double_compose():
+    """The single-precision compose (the reference's GPU path) is within float rounding of its host twin
+    (double precision, src/instances.cpp:137-164)."""
+    wl = workloads.body_worlds(worlds=8)
+    b = wl.binding
+    m32 = O.compose(8, 20, 20, b["body_of_instance"], b["local_pose"], b["scale"], wl.poses)
+    m64 = O.ref_body_poses_to_matrices(b["body_of_instance"], b["local_pose"], b["scale"], 20, 8, wl.poses)
+    assert np.abs(m32 - m64).max() <= 1e-6 * max(1.0, np.abs(m64).max())
+
+
+@needs_ref
+def test_oracle_matches_reference_on_scattered_worlds_except_near_ties():
+    desc, mats, cams = scenes.scattered_boxes(50, 40)
+    o, r = O.Oracle(desc), O.Reference(desc)
+    o.set_instance_transforms(mats)
+    r.set_instance_transforms(mats)
+    a = o.render(cams, scenes.FOV, 1, rgb=True, depth=True, normals=True, object_ids=True, ties=True)
+    b = r.render(cams, scenes.FOV, 1, rgb=True, depth=True, normals=True, object_ids=True)
+    tie = (a["ties"] & O.TIE_AOV_INSTANCE) != 0
+    assert ((a["object_ids"] != b["object_ids"]) & ~tie).sum() == 0
+    same = (a["object_ids"] == b["object_ids"]) & ~tie
+    assert np.array_equal(bits(a["depth"][same]), bits(b["depth"][same]))
+    rgb_tie = (a["ties"] & O.TIE_RGB_INSTANCE) != 0
+    assert (np.abs(a["rgb"].astype(int) - b["rgb"].astype(int)).max(-1)[~rgb_tie] == 0).all()
+
+
+# ----------------------------------------------------------------------------------------- the ABI --
+
+def test_library_exports_every_declared_entry_point():
+    import ctypes
+    header = open(os.path.join(ROOT, "include", "ngb.h")).read()
+    declared = sorted(set(re.findall(r"^\w[\w\s\*]*?\b(ngb_\w+)\(", header, re.M)))
+    assert len(declared) >= 28
+    lib = ctypes.CDLL(os.path.join(ROOT, "neraulgraphics_b200", "libngb.so"))
+    missing = [name for name in declared if not hasattr(lib, name)]
+    assert not missing, missing
+
+
+def test_construction_rejects_bad_scenes_with_the_reference_messages():
+    import neraulgraphics_b200 as ng
+    with pytest.raises(ValueError, match="world_count must be 1 or more, got 0"):
+        ng.BatchRenderer(64, 64, 0)
+    with pytest.raises(ValueError, match="cameras_per_world must be 1 or more, got 0"):
+        ng.BatchRenderer(64, 64, 1, 0)
+    with pytest.raises(ValueError, match="frame size must be positive, got 0x64"):
+        ng.BatchRenderer(0, 64, 1)
+    with pytest.raises(ValueError, match="instance 0 uses mesh 2, but there are 1 meshes"):
+        ng.BatchRenderer(64, 64, 1, meshes=[ng.make_box((1, 1, 1))], instances=[ng.Instance(2)])
+    with pytest.raises(ValueError, match="instance 0 transform is singular"):
+        ng.BatchRenderer(64, 64, 1, meshes=[ng.make_box((1, 1, 1))],
+                         instances=[ng.Instance(0, ng.Transform(np.zeros((3, 4), np.float32)))])
+    with pytest.raises(ValueError, match="light 0 radius must be 0 or more"):
+        ng.BatchRenderer(64, 64, 1, lights=[ng.Light((0, 1, 0), 1.0, -1.0)])
+    with pytest.raises(ValueError, match="scene has 9 lights, at most 8 fit"):
+        ng.BatchRenderer(64, 64, 1, lights=[ng.Light((0, 1, 0))] * 9)
+    with pytest.raises(ValueError, match="mesh 0 index 2 is 7, but there are only 3 vertices"):
+        ng.BatchRenderer(64, 64, 1, meshes=[ng.Mesh(np.zeros((3, 3)), [[0, 1, 7]])], instances=[ng.Instance(0)])
+    with pytest.raises(ValueError, match="device 'cpu' is not available"):
+        ng.BatchRenderer(64, 64, 1, device="cpu")
+
+
+def test_workloads_are_deterministic():
+    a, b = workloads.body_worlds(worlds=4, seed=3), workloads.body_worlds(worlds=4, seed=3)
+    assert np.array_equal(a.poses, b.poses) and np.array_equal(a.cameras, b.cameras)
+    s1 = workloads.random_walk(a.poses, 3, seed=1)
+    s2 = workloads.random_walk(b.poses, 3, seed=1)
+    assert np.array_equal(s1, s2) and s1.shape == (3, 4, 20, 7)
+    assert np.allclose(np.linalg.norm(s1[..., 3:], axis=-1), 1.0, atol=1e-6)
