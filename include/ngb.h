@@ -260,12 +260,15 @@ int ngb_set_ambient(ngb_renderer *r, float ambient);      /* src/batch.cpp:230-2
 float ngb_ambient(const ngb_renderer *r);
 int ngb_set_environment(ngb_renderer *r, const ngb_environment *environment); /* src/batch.cpp:224-227 */
 
-/* The stream every later call queues its work on (a cudaStream_t; NULL for the renderer's own). */
+/* The stream every later call queues its work on: a cudaStream_t, or NULL for the renderer's own stream
+ * (created non-blocking at ngb_create). CUDA's legacy default stream is named by its handle,
+ * cudaStreamLegacy ((void *)0x1), since NULL here means the renderer's own. */
 int ngb_set_stream(ngb_renderer *r, void *cuda_stream);
 /* synchronous 1: calls wait for their work, at most timeout_seconds (NGB_TIMEOUT after that).
  * synchronous 0: calls return once the work is queued. */
 int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
-/* Waits for every call queued so far, at most timeout_seconds. */
+/* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
+ * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */
 int ngb_synchronize(ngb_renderer *r, double timeout_seconds);
 
 /* ---- accessors (batch.h:115-123) ------------------------------------------------------------------- */

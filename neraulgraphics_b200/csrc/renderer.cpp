@@ -635,6 +635,7 @@ int ngb_render_host(ngb_renderer *h, const float *cams, float fov, int32_t spp, 
         if (dids && object_id) CK(cudaMemcpyAsync(object_id, dids, px * sizeof(int32_t), cudaMemcpyDeviceToHost, r.stream));
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, r.timeout);
+        if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
     });
 }
 

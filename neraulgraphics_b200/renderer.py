@@ -86,7 +86,9 @@ class BatchRenderer:
     def _stream(self):
         torch = _torch()
         s = torch.cuda.current_stream(self._device).cuda_stream
-        check(self._lib.ngb_set_stream(self._h, C.c_void_p(s)), self._h)
+        # PyTorch's default stream is CUDA's legacy default stream, handle 0; the C ABI takes NULL as the
+        # renderer's own stream, so the legacy stream is named by its CUDA handle, cudaStreamLegacy (0x1).
+        check(self._lib.ngb_set_stream(self._h, C.c_void_p(s if s else 1)), self._h)
 
     def _input(self, a, what):
         """(pointer, memory, keep-alive) for a float32 input: a CUDA tensor in place, else a host copy."""
@@ -181,7 +183,9 @@ class BatchRenderer:
         self._keep = keep
         if zero_copy:
             return dict(bufs)
-        return {k: v.cpu().numpy() for k, v in bufs.items()}
+        host = {k: v.cpu().numpy() for k, v in bufs.items()}
+        self.synchronize()  # reports a device-side error of this render
+        return host
 
     def _render_host(self, cameras, fov, spp, rgb, depth, normals, object_ids, frame, out):
         views, h, w = self.view_count, self.height, self.width
@@ -233,7 +237,9 @@ class BatchRenderer:
         self._keep = (ko, kd)
         if mo == _abi.MEMORY_DEVICE:
             return out
-        return {k: v.cpu().numpy() for k, v in out.items()}
+        host = {k: v.cpu().numpy() for k, v in out.items()}
+        self.synchronize()
+        return host
 
     # ------------------------------------------------------------------------------------------- settings --
 
@@ -282,6 +288,7 @@ class BatchRenderer:
         return float(self._lib.ngb_last_kernel_ms(self._h))
 
     def synchronize(self, timeout=_TIMEOUT_S):
+        """Waits for the queued work (at most timeout seconds) and raises CudaError if a kernel reported an error."""
         check(self._lib.ngb_synchronize(self._h, float(timeout)), self._h)
 
     # ----------------------------------------------------------------------------------------- inspection --
