@@ -308,6 +308,24 @@ int ngb_inspect_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, floa
 int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_count, int32_t *triangle_count,
     int32_t *nodes, float *triangles, int32_t *roots, float *bounds, int32_t *triangle_index);
 
+/* ---- a tree build that allocates nothing ------------------------------------------------------------- */
+
+/* No counterpart in the reference. The per-world instance-tree build of ngb_set_instance_transforms, for
+ * callers that cannot call cudaMalloc: a loop captured into a CUDA graph (no allocation during capture), or
+ * a framework whose own pool holds the GPU's memory. Inputs and outputs are the caller's device buffers:
+ * matrices (world_count * P * 12 floats), per slot its mesh's box in mesh space (P * 6) and its mesh's
+ * BLAS root (P); out: instance records (n * 16 floats: three world->mesh rows, then blas_root and slot as
+ * int bits), keys (n), sorted_ids (n), tlas_nodes ((2n - 1) * 8 words, bvh::TlasNode) and roots
+ * (world_count), with n = world_count * P. instance_records and tlas_nodes must be 16-byte aligned.
+ * Queued on `stream` (a cudaStream_t; NULL is the default stream), not waited for.
+ * The build's scratch lives in a static device array of the library: at most 65536 instances over all
+ * worlds (and 1024 per world); larger calls return NGB_INVALID_ARGUMENT. Every GPU that loads the library
+ * keeps that array (about 0.8 MB) until exit. The first call on a device looks up the array's address, so
+ * make it before any stream capture. All calls share the array: calls that overlap on the GPU race. */
+int ngb_build_tlas_noalloc(int32_t world_count, int32_t instances_per_world, const float *matrices,
+    const float *slot_bounds, const int32_t *slot_blas_root, float *instance_records, uint64_t *keys,
+    int32_t *sorted_ids, float *tlas_nodes, int32_t *roots, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -526,6 +526,14 @@ namespace {
 
 thread_local std::string g_create_error;
 
+}  // namespace
+
+namespace ngb {
+void set_global_error(const std::string &message) { g_create_error = message; }
+}  // namespace ngb
+
+namespace {
+
 template <class F>
 int guarded(ngb_renderer *h, F &&f) {
     if (h == nullptr) {
