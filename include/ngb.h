@@ -267,6 +267,12 @@ int ngb_set_stream(ngb_renderer *r, void *cuda_stream);
 /* synchronous 1: calls wait for their work, at most timeout_seconds (NGB_TIMEOUT after that).
  * synchronous 0: calls return once the work is queued. */
 int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
+/* How renders run. kernel: 0 automatic (the persistent kernel whenever it applies: one sample per pixel, at
+ * most one light, no material with reflectivity >= 1e-3), 1 the per-pixel kernel, 2 the persistent kernel
+ * where it applies. threads_per_block (32..256, a multiple of 32) and refill_lanes (1..32: a warp takes new
+ * pixels once this many of its lanes are free) tune the persistent kernel. Defaults: 0, 256, 16. */
+int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes);
+
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
  * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */
 int ngb_synchronize(ngb_renderer *r, double timeout_seconds);

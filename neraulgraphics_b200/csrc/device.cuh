@@ -95,6 +95,13 @@ struct SceneParams {
     int instance_count;
     int per_world;
     int blas_node_count;  // caps a mesh-tree walk: a correct walk visits each node at most once
+    // Child-pair records (both children's boxes and references in 64 bytes; see host.h and lbvh.cu):
+    // every mesh node, and every world's internal LBVH nodes by their Karras index.
+    const float4 *blas_pairs;
+    const float4 *tlas_pairs;
+    const int2 *slot_root;     // per slot: its mesh root's reference (node, 0) or (first triangle, count)
+    const float *slot_bounds;  // per slot: its mesh's box in mesh space, 6 floats
+    int tlas_internal;         // n - 1: nodes below this index are internal
 };
 
 // ---------------------------------------------------------------------------------------------- math --

@@ -350,6 +350,25 @@ BuiltMeshes build_meshes(const ngb_scene &s) {
             std::memcpy(words, &nd, sizeof(words));
             out.nodes.insert(out.nodes.end(), words, words + 8);
         }
+        auto ref_of = [&](const Node &nd, int index) {
+            return nd.count > 0 ? std::array<int32_t, 2>{nd.a + tri_base, nd.count} : std::array<int32_t, 2>{index + node_base, 0};
+        };
+        for (size_t i = 0; i < tree.size(); ++i) {
+            float rec[16] = {};
+            const Node &nd = tree[i];
+            if (nd.count == 0) {
+                const Node &l = tree[nd.a], &r = tree[nd.a + 1];
+                const std::array<int32_t, 2> lr = ref_of(l, nd.a), rr = ref_of(r, nd.a + 1);
+                const float v[12] = {l.lo[0], l.lo[1], l.lo[2], l.hi[0], l.hi[1], l.hi[2], r.lo[0], r.lo[1], r.lo[2],
+                    r.hi[0], r.hi[1], r.hi[2]};
+                std::memcpy(rec, v, sizeof(v));
+                const int32_t refs[4] = {lr[0], lr[1], rr[0], rr[1]};
+                std::memcpy(rec + 12, refs, sizeof(refs));
+            }
+            out.pairs.insert(out.pairs.end(), rec, rec + 16);
+        }
+        const std::array<int32_t, 2> root = ref_of(tree[0], 0);
+        out.root_refs.insert(out.root_refs.end(), root.begin(), root.end());
         for (const uint32_t t : order) {
             const float *a = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t]);
             const float *b = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t + 1]);

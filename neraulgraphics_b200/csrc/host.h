@@ -50,6 +50,12 @@ struct BuiltMeshes {
     std::vector<int32_t> triangle_index;
     std::vector<int32_t> roots;
     std::vector<float> bounds;       // 6 per mesh
+    // The same trees as child-pair records, one per node (used for internal nodes only): both children's
+    // boxes and references in 64 bytes, (c0.lo.xyz, c0.hi.x) (c0.hi.yz, c1.lo.xy) (c1.lo.z, c1.hi.xyz)
+    // (c0.ref, c0.count, c1.ref, c1.count). A reference is (node, 0) for an internal child and (first
+    // triangle, count) for a leaf. Per mesh, its root's reference.
+    std::vector<float> pairs;        // 16 per node
+    std::vector<int32_t> root_refs;  // 2 per mesh
 };
 
 BuiltMeshes build_meshes(const ngb_scene &s);

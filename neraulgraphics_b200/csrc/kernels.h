@@ -31,6 +31,7 @@ struct BuildArgs {
     int *parent;                   // 2n - 1; parent[0] stays -1
     int *arrivals;                 // n - 1 counters, zero between builds
     int *error_flag;               // set nonzero if a climb runs longer than any valid tree allows
+    float4 *tlas_pairs;            // (n - 1) x 4 child-pair records of the internal nodes, or null
 };
 
 // Group size (threads per world) of the per-world build: a power of two, at least 32.
@@ -75,5 +76,13 @@ struct RayArgs {
     int *error_flag;
 };
 cudaError_t launch_rays(const SceneParams &s, const RayArgs &a, cudaStream_t stream);
+
+// The persistent render: spp 1, at most one light, no mirror bounces (see persistent.cu).
+struct PersistentTuning {
+    int threads;      // per CTA, a multiple of 32
+    int refill;       // a warp fetches new pixels once this many of its lanes are idle
+};
+cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
+    const PersistentTuning &t, cudaStream_t stream);
 
 }  // namespace ngb

@@ -95,6 +95,7 @@ struct GroupSmem {
     int child[G][2];       // local ids of internal node j's children
     int parent[2 * G];     // local id of a node's parent, -1 when it is outside the world
     int arrive[G];
+    int sorted[G];         // local instance at sorted position r
     int bounds[6];         // ordered-int centre bounds
 };
 
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
             rank += (kj < morton) || (kj == morton && j < i);
         }
         sm.key[rank] = morton;
+        sm.sorted[rank] = i;
         a.sorted_ids[base + rank] = static_cast<int>(g);
         for (int ax = 0; ax < 3; ++ax) {
             sm.box[G + rank][ax] = lo[ax];
@@ -292,6 +294,20 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
         float4 *nd = a.tlas + 2 * p;
         nd[0] = make_float4(sm.box[i][0], sm.box[i][1], sm.box[i][2], __int_as_float(left));
         nd[1] = make_float4(sm.box[i][3], sm.box[i][4], sm.box[i][5], __int_as_float(right));
+        if (a.tlas_pairs) {
+            // The same node as a child-pair record: both children's boxes and references, (internal node, 0)
+            // or (instance, -1) for a leaf.
+            const int cl = sm.child[i][0], cr = sm.child[i][1];
+            const int rl = cl >= G ? static_cast<int>(base) + sm.sorted[cl - G] : left;
+            const int rr = cr >= G ? static_cast<int>(base) + sm.sorted[cr - G] : right;
+            const float *bl = sm.box[cl], *br = sm.box[cr];
+            float4 *q = a.tlas_pairs + 4 * p;
+            q[0] = make_float4(bl[0], bl[1], bl[2], bl[3]);
+            q[1] = make_float4(bl[4], bl[5], br[0], br[1]);
+            q[2] = make_float4(br[2], br[3], br[4], br[5]);
+            q[3] = make_float4(__int_as_float(rl), __int_as_float(cl >= G ? -1 : 0), __int_as_float(rr),
+                __int_as_float(cr >= G ? -1 : 0));
+        }
     }
 }
 

@@ -1,0 +1,451 @@
+// The persistent render kernel: the batched path's common case (one sample per pixel, at most one light,
+// no mirror bounces) with full SIMD lanes.
+//
+// The first render kernel (trace.cu) gives each thread a pixel and walks its rays one after another, the
+// world's tree and a mesh's tree in nested loops; a warp then waits for its slowest lane at every level and
+// every ray, and only a quarter of the lanes did work per instruction. Here every lane holds one ray job and
+// all jobs share one walk loop:
+//   - a pixel gives two jobs, the jittered picture ray and the centre ray of the depth/normal/ID images
+//     (two neighbouring lanes trace nearly the same ray); a picture ray that hits a lit surface turns into
+//     its shadow ray in the same lane;
+//   - warps are persistent: when enough of a warp's lanes are free (ballot), one lane takes that many new jobs
+//     from a global counter with one atomic and the free lanes start them (warp-ballot compaction, persistent
+//     per-warp ray fetch);
+//   - the walk is one loop over both levels: entering an instance pushes a marker and moves the ray to mesh
+//     space, popping the marker moves it back, so lanes at different levels run the same instructions;
+//   - nodes are child-pair records, both children's boxes and references in 64 bytes (four 16-byte loads
+//     instead of the six a node plus its two children cost in the reference's layout).
+// The walk order is the reference's exactly (nearer child first by dl <= dr, the farther one pushed with its
+// entry distance, dropped at pop time once a hit is closer; src/mesh_dev.h:113-159), over the same boxes, so
+// every hit, including which of two tied hits wins, is the reference's. The shading arithmetic is the
+// reference's, term by term (src/render_core.h:202-283).
+#include <climits>
+
+#include "kernels.h"
+#include "trace_common.cuh"
+
+namespace ngb {
+namespace {
+
+using namespace tr;
+
+constexpr int STACK = 112;        // world tree (<= 41 deep for 1024 instances) + marker + mesh tree (<= 64)
+constexpr int MARKER = INT_MIN;   // stack entry that returns the walk from a mesh to its world's tree
+constexpr int ST_IDLE = 0, ST_WALK = 1, ST_DONE = 2;
+constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3;
+constexpr unsigned FULL = 0xffffffffu;
+
+struct Lane {
+    int state, job;
+    long long pix;      // output index (view * H + y) * W + x
+    int world;
+    uint32_t rng;
+    float3 fwd;         // camera forward, for depth along the view axis
+    float3 c_lit, c_shadow;
+    int best_sphere;
+    bool hit_floor;
+    // the walk
+    float3 o, d, inv;   // world-space ray
+    float3 lo, ld, linv;  // mesh-space ray, inside an instance
+    float tmax;
+    int ref, count;     // current node: (internal, 0), (instance, -1) or (first triangle, count)
+    int sp;
+    int inst;
+    bool in_blas, any, blocked;
+    int hit_inst, hit_tri;
+    float hu, hv;
+    int steps, max_steps;
+};
+
+__device__ __forceinline__ float3 camera_dir(float3 right, float3 up, float3 fwd, float px, float py, float fw, float fh,
+    float fov_scale, float aspect) {
+    const float sx = (2.0f * px / fw - 1.0f) * fov_scale * aspect;
+    const float sy = -(2.0f * py / fh - 1.0f) * fov_scale;
+    return normalize(right * sx + up * sy + fwd);
+}
+
+// Starts a walk of the world's meshes from the ray in L (o, d) with tmax: the root box test of
+// traverse<true> (src/mesh_dev.h:117), then the root itself.
+__device__ __forceinline__ void start_walk(const SceneParams &s, Lane &L) {
+    L.inv = safe_inverse(L.d);
+    L.sp = 0;
+    L.in_blas = false;
+    L.blocked = false;
+    L.hit_inst = -1;
+    L.steps = 0;
+    if (s.instance_count <= 0) {
+        L.state = ST_DONE;
+        return;
+    }
+    const int root = __ldg(s.roots + L.world);
+    const float4 r0 = __ldg(s.tlas + 2 * root), r1 = __ldg(s.tlas + 2 * root + 1);
+    if (box_entry(r0, r1, L.o, L.inv, L.tmax) >= NO_HIT) {
+        L.state = ST_DONE;
+        return;
+    }
+    if (root < s.tlas_internal) {
+        L.ref = root;
+        L.count = 0;
+    } else {
+        L.ref = ~__float_as_int(r0.w);  // a world of one instance: its root is that instance's leaf
+        L.count = -1;
+    }
+    L.state = ST_WALK;
+}
+
+// One node of the walk: the body of traverse's loop at either level, then its pop.
+__device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st_ref, int *st_cnt, float *st_t, int *err) {
+    if (++L.steps > L.max_steps) {  // only a malformed tree gets here
+        *err = 2;
+        L.state = ST_DONE;
+        return;
+    }
+    if (L.count == 0) {
+        const float4 *rec = (L.in_blas ? s.blas_pairs : s.tlas_pairs) + 4 * static_cast<long long>(L.ref);
+        const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
+        const float3 o = L.in_blas ? L.lo : L.o;
+        const float3 inv = L.in_blas ? L.linv : L.inv;
+        const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o, inv, L.tmax);
+        const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), o, inv, L.tmax);
+        if (dl < NO_HIT || dr < NO_HIT) {
+            const bool left_first = dl <= dr;
+            const float far_t = left_first ? dr : dl;
+            if (far_t < NO_HIT) {
+                if (L.sp >= STACK) {
+                    *err = 1;
+                    L.state = ST_DONE;
+                    return;
+                }
+                st_ref[L.sp] = __float_as_int(left_first ? q3.z : q3.x);
+                st_cnt[L.sp] = __float_as_int(left_first ? q3.w : q3.y);
+                st_t[L.sp] = far_t;
+                ++L.sp;
+            }
+            L.ref = __float_as_int(left_first ? q3.x : q3.z);
+            L.count = __float_as_int(left_first ? q3.y : q3.w);
+            return;
+        }
+    } else if (L.count < 0) {
+        // An instance: into its mesh's space, and its mesh's root box test (blas_walk's first line).
+        const InstanceRec r = load_instance(s.inst, L.ref);
+        const int slot = __float_as_int(__ldg(s.inst + 4 * L.ref + 3).y);
+        L.lo = to_local_point(r, L.o);
+        L.ld = to_local_dir(r, L.d);
+        L.linv = safe_inverse(L.ld);
+        const float *b = s.slot_bounds + 6 * slot;
+        const float4 blo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), 0.0f);
+        const float4 bhi = make_float4(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5), 0.0f);
+        if (box_entry(blo, bhi, L.lo, L.linv, L.tmax) < NO_HIT) {
+            if (L.sp >= STACK) {
+                *err = 1;
+                L.state = ST_DONE;
+                return;
+            }
+            st_ref[L.sp] = MARKER;
+            st_cnt[L.sp] = MARKER;
+            st_t[L.sp] = -INFINITY;  // never dropped by the tmax test
+            ++L.sp;
+            const int2 root = __ldg(s.slot_root + slot);
+            L.inst = L.ref;
+            L.in_blas = true;
+            L.ref = root.x;
+            L.count = root.y;
+            return;
+        }
+    } else {
+        for (int j = L.ref; j < L.ref + L.count; ++j) {
+            float t, bu, bv;
+            if (triangle_hit(s.tris, j, L.lo, L.ld, L.tmax, t, bu, bv)) {
+                if (L.any) {
+                    L.blocked = true;
+                    L.state = ST_DONE;
+                    return;
+                }
+                L.tmax = t;
+                L.hit_inst = L.inst;
+                L.hit_tri = j;
+                L.hu = bu;
+                L.hv = bv;
+            }
+        }
+    }
+    // Dead end: resume from the stack, dropping what a closer hit has put out of reach; a marker hands the walk
+    // back to the world's tree.
+    for (;;) {
+        while (L.sp > 0 && st_t[L.sp - 1] >= L.tmax) --L.sp;
+        if (L.sp == 0) {
+            L.state = ST_DONE;
+            return;
+        }
+        --L.sp;
+        const int c = st_cnt[L.sp];
+        if (c == MARKER) {
+            L.in_blas = false;
+            continue;
+        }
+        L.ref = st_ref[L.sp];
+        L.count = c;
+        return;
+    }
+}
+
+// The radiance of a hit with these light sums, as trace computes it for a path of one bounce
+// (src/render_core.h:234-236, radiance and throughput starting at 0 and 1).
+__device__ __forceinline__ float3 radiance_of(const DevMaterial &m, float ambient, float3 diffuse, float3 specular) {
+    const float3 direct = m.diffuse_color * (diffuse * m.kd) + specular * m.ks;
+    return mk3(0.0f, 0.0f, 0.0f) + (direct + m.diffuse_color * (ambient * m.kd)) * 1.0f;
+}
+
+// sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283).
+__device__ __forceinline__ void write_rgb(uint8_t *rgb, long long pix, float3 radiance) {
+    float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
+    sum = sum * (1.0f / 1.0f);
+    uint8_t *o = rgb + 3 * static_cast<size_t>(pix);
+    o[0] = to_byte(srgb_channel(sum.x));
+    o[1] = to_byte(srgb_channel(sum.y));
+    o[2] = to_byte(srgb_channel(sum.z));
+}
+
+// A new job from its item number. Items run over views, then 4 x 4 pixel tiles, then the pixels of a tile,
+// then (when both are asked for) the picture ray and the centre ray of a pixel.
+__device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, Lane &L, long long item, int kinds,
+    int tiles_x, int tiles_per_view) {
+    int job = JOB_RGB;
+    if (kinds == 3) {
+        job = (item & 1) ? JOB_AOV : JOB_RGB;
+        item >>= 1;
+    } else if (kinds == 2) {
+        job = JOB_AOV;
+    }
+    const long long per_view = 16LL * tiles_per_view;
+    const int view = static_cast<int>(item / per_view);
+    const int q = static_cast<int>(item % per_view);
+    const int tile = q >> 4, within = q & 15;
+    const int x = (tile % tiles_x) * 4 + (within & 3);
+    const int y = (tile / tiles_x) * 4 + (within >> 2);
+    if (x >= a.width || y >= a.height) {
+        L.state = ST_IDLE;
+        return;
+    }
+    L.job = job;
+    L.pix = (static_cast<long long>(view) * a.height + y) * a.width + x;
+    L.world = view / a.cameras_per_world;
+    const float *m = a.cameras + 12 * static_cast<size_t>(view);
+    float cm[12];
+    for (int k = 0; k < 12; ++k) cm[k] = __ldg(m + k);
+    const float3 right = normalize(mk3(cm[0], cm[4], cm[8]));
+    const float3 up = normalize(mk3(cm[1], cm[5], cm[9]));
+    const float3 fwd = normalize(mk3(-cm[2], -cm[6], -cm[10]));
+    const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
+    float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f;
+    if (job == JOB_RGB) {
+        L.rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
+        const float jx = rand_float(L.rng);
+        const float jy = rand_float(L.rng);
+        px = static_cast<float>(x) + jx;
+        py = static_cast<float>(y) + jy;
+    }
+    L.fwd = fwd;
+    L.o = mk3(cm[3], cm[7], cm[11]);
+    L.d = camera_dir(right, up, fwd, px, py, fw, fh, a.fov_scale, a.aspect);
+    // Spheres and the floor first; the meshes are walked with their closest hit as the limit
+    // (scene_intersect, src/render_core.h:78-112).
+    float best = 1e30f;
+    int best_sphere = -1;
+    for (int i = 0; i < s.sphere_count; ++i) {
+        float t;
+        if (sphere_hit(s.spheres[i], L.o, L.d, t) && t < best) {
+            best = t;
+            best_sphere = i;
+        }
+    }
+    bool hit_floor = false;
+    {
+        float dd;
+        if (floor_hit(s.floor, L.o, L.d, best, dd)) {
+            best = dd;
+            hit_floor = true;
+        }
+    }
+    L.best_sphere = best_sphere;
+    L.hit_floor = hit_floor;
+    L.tmax = best;
+    L.any = false;
+    start_walk(s, L);
+}
+
+// What happens when a lane's walk ends: outputs, and for a lit picture hit, its shadow ray.
+__device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, Lane &L) {
+    if (L.job == JOB_SHADOW) {
+        write_rgb(a.rgb, L.pix, L.blocked ? L.c_shadow : L.c_lit);
+        L.state = ST_IDLE;
+        return;
+    }
+    const bool mesh = L.hit_inst >= 0;
+    const bool found = mesh || L.best_sphere >= 0 || L.hit_floor;
+    float3 normal = mk3(0.0f, 0.0f, 0.0f), point = mk3(0.0f, 0.0f, 0.0f);
+    DevMaterial mat{};
+    int object = OBJECT_NONE;
+    if (found) {  // the surface, as scene_intersect resolves it (src/render_core.h:116-141)
+        point = L.o + L.d * L.tmax;
+        if (mesh) {
+            normal = mesh_surface(s, L.hit_inst, L.hit_tri, L.hu, L.hv, L.d);
+            const int slot = L.hit_inst - L.world * s.per_world;
+            mat = s.slot_material[slot];
+            object = OBJECT_INSTANCE + slot;
+        } else if (L.hit_floor) {
+            object = OBJECT_FLOOR;
+            normal = mk3(0.0f, 1.0f, 0.0f);
+            mat = s.floor.m;
+            const int cx = static_cast<int>(floorf(point.x * s.floor.checker));
+            const int cz = static_cast<int>(floorf(point.z * s.floor.checker));
+            const float3 tint = ((cx + cz) & 1) ? mk3(1.0f, 1.0f, 1.0f) : mk3(1.0f, 0.7f, 0.3f);
+            mat.diffuse_color = tint * 0.3f;
+        } else {
+            normal = normalize(point - s.spheres[L.best_sphere].center);
+            mat = s.spheres[L.best_sphere].m;
+            object = OBJECT_SPHERE + L.best_sphere;
+        }
+    }
+    if (L.job == JOB_AOV) {  // aov_pixel (src/render_core.h:313-327)
+        const size_t p = static_cast<size_t>(L.pix);
+        if (a.depth) a.depth[p] = found ? L.tmax * dot(L.d, L.fwd) : __int_as_float(0x7f800000);
+        if (a.normal) {
+            a.normal[3 * p] = normal.x;
+            a.normal[3 * p + 1] = normal.y;
+            a.normal[3 * p + 2] = normal.z;
+        }
+        if (a.object_id) a.object_id[p] = object;
+        if (a.hit_instance) {
+            a.hit_instance[p] = mesh ? L.hit_inst : -1;
+            a.hit_triangle[p] = mesh ? __ldg(s.tri_index + L.hit_tri) : -1;
+            a.hit_u[p] = mesh ? L.hu : 0.0f;
+            a.hit_v[p] = mesh ? L.hv : 0.0f;
+        }
+        L.state = ST_IDLE;
+        return;
+    }
+    // The picture ray (trace, src/render_core.h:202-245, one bounce).
+    if (!found) {
+        const float t = saturate(dot(L.d, s.env_up) * 0.5f + 0.5f);
+        const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
+        write_rgb(a.rgb, L.pix, mk3(0.0f, 0.0f, 0.0f) + sky * 1.0f);
+        L.state = ST_IDLE;
+        return;
+    }
+    const float3 zero = mk3(0.0f, 0.0f, 0.0f);
+    if (s.light_count == 1) {
+        const DevLight &lt = s.lights[0];
+        const float z = 1.0f - 2.0f * rand_float(L.rng);
+        const float rad = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        const float phi = 6.28318530718f * rand_float(L.rng);
+        const float3 lp = lt.position + mk3(rad * cosf(phi), rad * sinf(phi), z) * lt.radius;
+        const float3 to_light = lp - point;
+        const float light_distance = sqrtf(dot(to_light, to_light));
+        const float3 light_dir = to_light * (1.0f / light_distance);
+        const float strength = lt.intensity * light_factor(lt, light_dir, light_distance);
+        if (strength > 0.0f) {
+            const float3 lit = lt.color * strength;
+            const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
+            const float3 specular = zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), L.d)), mat.exponent);
+            L.c_lit = radiance_of(mat, s.ambient, diffuse, specular);
+            L.c_shadow = radiance_of(mat, s.ambient, zero, zero);
+            // The shadow ray: spheres and the floor first, then any hit in the meshes (scene_occluded,
+            // src/render_core.h:146-161).
+            L.job = JOB_SHADOW;
+            L.o = offset_origin(point, normal, light_dir);
+            L.d = light_dir;
+            L.tmax = light_distance;
+            L.any = true;
+            bool blocked = false;
+            for (int i = 0; i < s.sphere_count && !blocked; ++i) {
+                float t;
+                if (sphere_hit(s.spheres[i], L.o, L.d, t) && t < light_distance) blocked = true;
+            }
+            if (!blocked) {
+                float dd;
+                blocked = floor_hit(s.floor, L.o, L.d, light_distance, dd);
+            }
+            if (blocked) {
+                write_rgb(a.rgb, L.pix, L.c_shadow);
+                L.state = ST_IDLE;
+                return;
+            }
+            start_walk(s, L);
+            return;
+        }
+    }
+    write_rgb(a.rgb, L.pix, radiance_of(mat, s.ambient, zero, zero));
+    L.state = ST_IDLE;
+}
+
+__global__ void __launch_bounds__(256) render_persistent_kernel(const __grid_constant__ SceneParams s, const RenderArgs a,
+    int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill) {
+    int st_ref[STACK], st_cnt[STACK];
+    float st_t[STACK];
+    const int lane = threadIdx.x & 31;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    Lane L;
+    L.state = ST_IDLE;
+    // A correct walk visits each node of its world's tree once and each node of an entered mesh's tree once.
+    const long long cap = 2LL * s.per_world + 2 + static_cast<long long>(s.per_world) * (s.blas_node_count + 2);
+    L.max_steps = cap > INT_MAX ? INT_MAX : static_cast<int>(cap);
+    bool exhausted = false;
+    for (;;) {
+        if (L.state == ST_DONE) complete(s, a, L);
+        const unsigned idle = __ballot_sync(FULL, L.state == ST_IDLE);
+        if (!exhausted && idle != 0 && (__popc(idle) >= refill || idle == FULL)) {
+            const int k = __popc(idle);
+            const int leader = __ffs(idle) - 1;
+            long long base = 0;
+            if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned long long *>(counter), static_cast<unsigned long long>(k));
+            base = __shfl_sync(FULL, base, leader);
+            if (base + k >= total) exhausted = true;
+            if (L.state == ST_IDLE) {
+                const long long item = base + __popc(idle & lanes_below);
+                if (item < total) start_job(s, a, L, item, kinds, tiles_x, tiles_per_view);
+            }
+        }
+        const unsigned busy = __ballot_sync(FULL, L.state != ST_IDLE);
+        if (busy == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        // Walk until enough lanes are free to be worth a refill (or, once the work is all taken, until all are).
+        for (;;) {
+            if (L.state == ST_WALK) walk_step(s, L, st_ref, st_cnt, st_t, a.error_flag);
+            const unsigned walking = __ballot_sync(FULL, L.state == ST_WALK);
+            if (walking == 0) break;
+            if (!exhausted && 32 - __popc(walking) >= refill) break;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
+    cudaStream_t stream) {
+    const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
+    const int tiles_per_view = tiles_x * tiles_y;
+    const int kinds = (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
+    if (kinds == 0) return cudaSuccess;
+    const long long total = 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent_kernel, t.threads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    // Enough resident warps to fill every SM, and no more warps than there are jobs for.
+    long long blocks = static_cast<long long>(sms) * per_sm;
+    const long long needed = (total + t.threads - 1) / t.threads;
+    if (blocks > needed) blocks = needed;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    render_persistent_kernel<<<static_cast<unsigned>(blocks), t.threads, 0, stream>>>(s, a, counter, total, kinds, tiles_x,
+        tiles_per_view, t.refill);
+    return cudaGetLastError();
+}
+
+}  // namespace ngb

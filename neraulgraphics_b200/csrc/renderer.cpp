@@ -103,6 +103,12 @@ struct Renderer {
     DevBuf<float4> inst, tlas;
     DevBuf<unsigned long long> keys;
     DevBuf<int> sorted_ids, roots, parent, arrivals;
+    DevBuf<float4> blas_pairs, tlas_pairs;
+    DevBuf<int2> slot_root;
+    DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
+    bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
+    int kernel_choice = 0;                    // 0: automatic, 1: the per-pixel kernel, 2: the persistent kernel
+    PersistentTuning tuning{256, 16};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -204,6 +210,12 @@ Renderer::Renderer(const ngb_scene &s) {
     }
     params.sphere_count = s.sphere_count;
     params.light_count = s.light_count;
+    // A path bounces when throughput * reflectivity >= 1e-3 (src/render_core.h:238-239); with throughput 1
+    // at the first hit, that is any material hit with reflectivity >= 1e-3.
+    for (int i = 0; i < s.sphere_count; ++i) reflective = reflective || s.spheres[i].material.reflectivity >= 1e-3f;
+    reflective = reflective || (s.floor.half_extent_x > 0.0f && s.floor.material.reflectivity >= 1e-3f);
+    for (int i = 0; i < s.instance_count; ++i) reflective = reflective || s.instances[i].material.reflectivity >= 1e-3f;
+    work_counter.ensure(1);
     params.floor = DevPlane{s.floor.y, s.floor.half_extent_x, s.floor.z_min, s.floor.z_max, s.floor.checker_scale,
         dev_material(s.floor.material)};
     params.env_up = make_float3(0.0f, 1.0f, 0.0f);
@@ -241,6 +253,14 @@ Renderer::Renderer(const ngb_scene &s) {
         material_of_slot[i] = dev_material(s.instances[i].material);
     }
     upload(slot_blas_root, root_of_slot);
+    upload(blas_pairs, built.pairs);
+    std::vector<int2> root_ref_of_slot(per_world);
+    for (int i = 0; i < per_world; ++i) {
+        const int mesh = s.instances[i].mesh;
+        root_ref_of_slot[i] = make_int2(built.root_refs[2 * mesh], built.root_refs[2 * mesh + 1]);
+    }
+    upload(slot_root, root_ref_of_slot);
+    tlas_pairs.ensure(4 * std::max<long long>(n - 1, 1));
     upload(slot_bounds, bounds_of_slot);
     upload(slot_material, material_of_slot);
     matrices.ensure(12 * n);
@@ -262,6 +282,11 @@ Renderer::Renderer(const ngb_scene &s) {
     params.tri_index = tri_index.p;
     params.slot_material = slot_material.p;
     params.blas_node_count = static_cast<int>(built.nodes.size() / 8);
+    params.blas_pairs = blas_pairs.p;
+    params.tlas_pairs = tlas_pairs.p;
+    params.slot_root = slot_root.p;
+    params.slot_bounds = slot_bounds.p;
+    params.tlas_internal = static_cast<int>(n - 1);
 
     // Every world starts with the transforms the instances were given (src/cuda_backend.cu:765-770).
     std::vector<float> initial(12 * n);
@@ -290,6 +315,7 @@ Renderer::~Renderer() {
     slot_bounds.release(), slot_material.release(), matrices.release(), inst.release(), tlas.release();
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
+    blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
     hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
@@ -349,6 +375,7 @@ void Renderer::build(const float *matrices_in, bool compose, const float *poses)
     a.parent = parent.p;
     a.arrivals = arrivals.p;
     a.error_flag = error_flag.p;
+    a.tlas_pairs = tlas_pairs.p;
     CK(launch_build_worlds(a, stream));
 }
 
@@ -465,8 +492,16 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
         a.hit_v = hit_v.ensure(pixels());
     }
     a.error_flag = error_flag.p;
+    // The persistent kernel covers one sample per pixel, at most one light and no bounces; everything else
+    // takes the per-pixel kernel, which runs trace in full.
+    const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
+    const bool persistent = kernel_choice == 2 ? persistent_ok : (kernel_choice == 0 && persistent_ok);
     CK(cudaEventRecord(ev_start, stream));
-    CK(launch_render(params, a, stream));
+    if (persistent) {
+        CK(launch_render_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
+    } else {
+        CK(launch_render(params, a, stream));
+    }
     CK(cudaEventRecord(ev_stop, stream));
     timing_pending = true;
     finish();
@@ -772,6 +807,17 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
         g_create_error = e.what();
         return NGB_CUDA_ERROR;
     }
+}
+
+int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(kernel >= 0 && kernel <= 2, "kernel must be 0 (automatic), 1 (per pixel) or 2 (persistent)");
+        ngb::require(threads_per_block >= 32 && threads_per_block <= 256 && threads_per_block % 32 == 0,
+            "threads_per_block must be a multiple of 32 from 32 to 256");
+        ngb::require(refill_lanes >= 1 && refill_lanes <= 32, "refill_lanes must be 1 to 32");
+        r.kernel_choice = kernel;
+        r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes};
+    });
 }
 
 int ngb_record_hits(ngb_renderer *h, int32_t on) {

@@ -293,6 +293,11 @@ class BatchRenderer:
 
     # ----------------------------------------------------------------------------------------- inspection --
 
+    def set_tuning(self, kernel=0, threads_per_block=256, refill_lanes=16):
+        """kernel: 0 automatic, 1 the per-pixel kernel, 2 the persistent kernel (where it applies: one sample per
+        pixel, at most one light, no reflective material); threads_per_block and refill_lanes tune the latter."""
+        check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes)), self._h)
+
     def record_hits(self, on=True):
         check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
 

@@ -268,3 +268,55 @@ def test_a_thousand_worlds_stay_in_gpu_memory(torch_cuda):
     assert tuple(depth.shape) == (1000, scenes.H, scenes.W) and depth.is_cuda
     assert float(torch.isfinite(depth).float().mean()) > 0.1
     assert r.last_kernel_ms > 0
+
+
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_both_render_kernels_are_the_oracles(torch_cuda, kernel):
+    """The per-pixel kernel and the persistent kernel, forced in turn, on odd image sizes (partial 4 x 4 tiles),
+    two cameras per world, spheres and a checker floor, with hit records."""
+    wl = workloads.icosphere_worlds(worlds=5, width=37, height=29, seed=11)
+    d = wl.desc
+    spheres = [ng.Sphere((0.5, -1.0, -7.0), 0.7), ng.Sphere((-1.5, 0.0, -8.0), 0.5)]
+    floor = ng.Plane(y=-2.0, half_extent_x=12.0, z_min=-30.0, z_max=-2.0, checker_scale=1.0)
+    desc = ng.SceneDesc(d.width, d.height, 5, 2, spheres, d.lights, floor, d.meshes, d.instances)
+    cams = np.repeat(wl.cameras, 2, axis=0)
+    cams[1::2, :, 3] += np.float32([0.3, 0.0, 0.0])
+    r, o = product(desc), O.Oracle(desc)
+    r.set_tuning(kernel=kernel, threads_per_block=128, refill_lanes=8)
+    r.set_instance_transforms(wl.matrices)
+    o.set_instance_transforms(wl.matrices)
+    r.ambient = 0.05
+    o.set_ambient(0.05)
+    r.record_hits(True)
+    got = r.render(cams, 1.0, 1, **ALL, frame=3)
+    want = o.render(cams, 1.0, 1, **ALL, frame=3, hits=True)
+    assert_same_images(got, want)
+    h = r.inspect_hits()
+    for k in ("hit_instance", "hit_triangle"):
+        assert np.array_equal(h[k], want[k]), k
+    for k in ("hit_u", "hit_v"):
+        assert np.array_equal(bits(h[k]), bits(want[k])), k
+
+
+@pytest.mark.parametrize("outputs", [dict(rgb=True), dict(rgb=False, depth=True), dict(rgb=False, object_ids=True)])
+def test_persistent_kernel_with_one_kind_of_output(torch_cuda, outputs):
+    wl = workloads.body_worlds(worlds=64, seed=2)
+    r, o = product(wl.desc), O.Oracle(wl.desc)
+    for x in (r, o):
+        x.bind_bodies(**wl.binding)
+        x.set_body_poses(wl.poses)
+    r.set_tuning(kernel=2)
+    assert_same_images(r.render(wl.cameras, 1.0, 1, **outputs), o.render(wl.cameras, 1.0, 1, **outputs))
+
+
+def test_persistent_kernel_tunings_agree(torch_cuda):
+    wl = workloads.body_worlds(worlds=128, seed=5)
+    r = product(wl.desc)
+    r.bind_bodies(**wl.binding)
+    r.set_body_poses(wl.poses)
+    out = dict(rgb=True, depth=True, object_ids=True)
+    r.set_tuning(kernel=1)
+    want = r.render(wl.cameras, 1.0, 1, **out)
+    for threads, refill in ((256, 16), (128, 4), (64, 32), (32, 1)):
+        r.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill)
+        assert_same_images(r.render(wl.cameras, 1.0, 1, **out), want, rgb_tol=0)
