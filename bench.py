@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
     return p.parse_args()
 
 
@@ -222,6 +223,11 @@ def run_ours(args, rank, world, local_rank, dist):
     cams_dev = torch.from_numpy(wl.cameras).to(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
+    tuned = None
+    r.set_body_poses(poses_dev[0])
+    if not args.no_autotune:
+        from neraulgraphics_b200.autotune import tune
+        tuned = tune(r, cams_dev, wl.fov, rgb=True, depth=True, object_ids=True, use_cache=False)
     for s in range(W):
         r.set_body_poses(poses_dev[s])
         r.render(cams_dev, wl.fov, 1, **kw)
@@ -315,6 +321,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "cpu_baseline": cpu,
         "reference_cuda": ref_cuda,
         "gpu_launches": 3 * K,
+        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("threads", "registers", "refill", "ms")},
         "clocks": clk,
     }
 

@@ -269,9 +269,10 @@ int ngb_set_stream(ngb_renderer *r, void *cuda_stream);
 int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
 /* How renders run. kernel: 0 automatic (the persistent kernel whenever it applies: one sample per pixel, at
  * most one light, no material with reflectivity >= 1e-3), 1 the per-pixel kernel, 2 the persistent kernel
- * where it applies. threads_per_block (32..256, a multiple of 32) and refill_lanes (1..32: a warp takes new
- * pixels once this many of its lanes are free) tune the persistent kernel. Defaults: 0, 256, 16. */
-int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes);
+ * where it applies. The persistent kernel's shape: threads_per_block and registers (the register budget per
+ * thread) as one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64, and refill_lanes (1..32: a warp takes new
+ * pixels once this many of its lanes are free). Defaults: 0, 128, 16, 64. */
+int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers);
 
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
  * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */

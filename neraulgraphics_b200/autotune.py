@@ -1,0 +1,82 @@
+"""Picks the persistent render kernel's launch shape for a workload by timing it.
+
+The shape is the CTA size, the register budget per thread (which sets how many warps an SM holds) and the
+refill threshold (how many of a warp's lanes must be free before it takes new pixels). The best depends on
+the scene (how long rays walk, how much they vary), so it is measured on the caller's own renderer and
+cameras, with CUDA events, and remembered in a JSON cache keyed by the GPU and the workload's shape.
+
+    from neraulgraphics_b200.autotune import tune
+    best = tune(renderer, cameras, fov=1.0, rgb=True, depth=True, object_ids=True)
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import time
+
+CANDIDATES = [(threads, regs, refill) for threads, regs in ((128, 64), (256, 64), (128, 48), (128, 72), (64, 64))
+              for refill in (8, 16, 24, 28)]
+
+
+def cache_path() -> str:
+    return os.environ.get("NGB_TUNING_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "neraulgraphics_b200", "tuning.json"))
+
+
+def _key(renderer, outputs) -> str:
+    import torch
+    name = torch.cuda.get_device_name(renderer._device)
+    return (f"{name}|{renderer.world_count}x{renderer.cameras_per_world}|{renderer.width}x{renderer.height}|"
+            f"{renderer.instances_per_world}|{outputs}")
+
+
+def _load() -> dict:
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, object_ids=False, repeats=3,
+         use_cache=True, budget_s=60.0) -> dict:
+    """Times every candidate shape on this renderer and these cameras (device tensors), sets the fastest and
+    returns {"threads", "registers", "refill", "ms", "timings"}."""
+    import torch
+    outputs = dict(rgb=rgb, depth=depth, normals=normals, object_ids=object_ids)
+    key = _key(renderer, tuple(sorted(k for k, v in outputs.items() if v)))
+    cache = _load() if use_cache else {}
+    if key in cache:
+        best = cache[key]
+        renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
+                            registers=best["registers"])
+        return dict(best, cached=True)
+    timings = []
+    start = time.perf_counter()
+    for threads, regs, refill in CANDIDATES:
+        renderer.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs)
+        renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
+        e1.record()
+        e1.synchronize()
+        timings.append({"threads": threads, "registers": regs, "refill": refill, "ms": e0.elapsed_time(e1) / repeats})
+        if time.perf_counter() - start > budget_s:
+            break
+    best = min(timings, key=lambda t: t["ms"])
+    renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
+                        registers=best["registers"])
+    result = dict(best, timings=timings)
+    if use_cache:
+        cache[key] = {k: best[k] for k in ("threads", "registers", "refill", "ms")}
+        try:
+            os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
+            with open(cache_path(), "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+    return result

@@ -79,8 +79,9 @@ cudaError_t launch_rays(const SceneParams &s, const RayArgs &a, cudaStream_t str
 
 // The persistent render: spp 1, at most one light, no mirror bounces (see persistent.cu).
 struct PersistentTuning {
-    int threads;      // per CTA, a multiple of 32
+    int threads;      // per CTA: 64, 128 or 256
     int refill;       // a warp fetches new pixels once this many of its lanes are idle
+    int registers;    // register budget per thread: 48, 64 or 72 (not every pair with threads is built)
 };
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
     const PersistentTuning &t, cudaStream_t stream);

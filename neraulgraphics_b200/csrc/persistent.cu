@@ -35,26 +35,50 @@ constexpr int ST_IDLE = 0, ST_WALK = 1, ST_DONE = 2;
 constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3;
 constexpr unsigned FULL = 0xffffffffu;
 
+// A lane's hot state, in registers: the current ray (world space, or mesh space inside an instance), the
+// current node, the stack depth and the closest hit so far.
 struct Lane {
     int state, job;
-    long long pix;      // output index (view * H + y) * W + x
     int world;
-    uint32_t rng;
-    float3 fwd;         // camera forward, for depth along the view axis
-    float3 c_lit, c_shadow;
-    int best_sphere;
-    bool hit_floor;
-    // the walk
-    float3 o, d, inv;   // world-space ray
-    float3 lo, ld, linv;  // mesh-space ray, inside an instance
+    float3 o, d, inv;
     float tmax;
     int ref, count;     // current node: (internal, 0), (instance, -1) or (first triangle, count)
     int sp;
     int inst;
     bool in_blas, any, blocked;
     int hit_inst, hit_tri;
-    float hu, hv;
-    int steps, max_steps;
+    int steps;
+};
+
+// A lane's cold state, in shared memory, one column per thread (structure of arrays, conflict-free): what is
+// read only when a walk enters or leaves an instance, records a hit, or ends.
+enum Cold {
+    C_WO, C_WD = C_WO + 3, C_WINV = C_WD + 3,  // the world-space ray while the walk is inside an instance
+    C_HU = C_WINV + 3, C_HV,                   // barycentrics of the closest hit
+    C_PIX_LO, C_PIX_HI, C_RNG,
+    C_FWD, C_LIT = C_FWD + 3, C_SHADOW = C_LIT + 3,
+    C_SPHERE = C_SHADOW + 3, C_FLOOR,
+    C_FIELDS
+};
+
+struct ColdRef {
+    float *base;
+    int stride;
+    __device__ __forceinline__ float &f(int field) const { return base[field * stride]; }
+    __device__ __forceinline__ int &i(int field) const { return reinterpret_cast<int *>(base)[field * stride]; }
+    __device__ __forceinline__ void put3(int field, float3 v) const {
+        f(field) = v.x;
+        f(field + 1) = v.y;
+        f(field + 2) = v.z;
+    }
+    __device__ __forceinline__ float3 get3(int field) const { return mk3(f(field), f(field + 1), f(field + 2)); }
+    __device__ __forceinline__ void put_pix(long long p) const {
+        i(C_PIX_LO) = static_cast<int>(p & 0xffffffffLL);
+        i(C_PIX_HI) = static_cast<int>(p >> 32);
+    }
+    __device__ __forceinline__ long long pix() const {
+        return (static_cast<long long>(i(C_PIX_HI)) << 32) | static_cast<unsigned>(i(C_PIX_LO));
+    }
 };
 
 __device__ __forceinline__ float3 camera_dir(float3 right, float3 up, float3 fwd, float px, float py, float fw, float fh,
@@ -94,8 +118,9 @@ __device__ __forceinline__ void start_walk(const SceneParams &s, Lane &L) {
 }
 
 // One node of the walk: the body of traverse's loop at either level, then its pop.
-__device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st_ref, int *st_cnt, float *st_t, int *err) {
-    if (++L.steps > L.max_steps) {  // only a malformed tree gets here
+__device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
+    float *st_t, int max_steps, int *err) {
+    if (++L.steps > max_steps) {  // only a malformed tree gets here
         *err = 2;
         L.state = ST_DONE;
         return;
@@ -103,10 +128,8 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
     if (L.count == 0) {
         const float4 *rec = (L.in_blas ? s.blas_pairs : s.tlas_pairs) + 4 * static_cast<long long>(L.ref);
         const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
-        const float3 o = L.in_blas ? L.lo : L.o;
-        const float3 inv = L.in_blas ? L.linv : L.inv;
-        const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o, inv, L.tmax);
-        const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), o, inv, L.tmax);
+        const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), L.o, L.inv, L.tmax);
+        const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), L.o, L.inv, L.tmax);
         if (dl < NO_HIT || dr < NO_HIT) {
             const bool left_first = dl <= dr;
             const float far_t = left_first ? dr : dl;
@@ -129,13 +152,13 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
         // An instance: into its mesh's space, and its mesh's root box test (blas_walk's first line).
         const InstanceRec r = load_instance(s.inst, L.ref);
         const int slot = __float_as_int(__ldg(s.inst + 4 * L.ref + 3).y);
-        L.lo = to_local_point(r, L.o);
-        L.ld = to_local_dir(r, L.d);
-        L.linv = safe_inverse(L.ld);
+        const float3 lo = to_local_point(r, L.o);
+        const float3 ld = to_local_dir(r, L.d);
+        const float3 linv = safe_inverse(ld);
         const float *b = s.slot_bounds + 6 * slot;
         const float4 blo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), 0.0f);
         const float4 bhi = make_float4(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5), 0.0f);
-        if (box_entry(blo, bhi, L.lo, L.linv, L.tmax) < NO_HIT) {
+        if (box_entry(blo, bhi, lo, linv, L.tmax) < NO_HIT) {
             if (L.sp >= STACK) {
                 *err = 1;
                 L.state = ST_DONE;
@@ -146,6 +169,13 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
             st_t[L.sp] = -INFINITY;  // never dropped by the tmax test
             ++L.sp;
             const int2 root = __ldg(s.slot_root + slot);
+            // The world-space ray waits in shared memory while the walk is in mesh space.
+            cold.put3(C_WO, L.o);
+            cold.put3(C_WD, L.d);
+            cold.put3(C_WINV, L.inv);
+            L.o = lo;
+            L.d = ld;
+            L.inv = linv;
             L.inst = L.ref;
             L.in_blas = true;
             L.ref = root.x;
@@ -155,7 +185,7 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
     } else {
         for (int j = L.ref; j < L.ref + L.count; ++j) {
             float t, bu, bv;
-            if (triangle_hit(s.tris, j, L.lo, L.ld, L.tmax, t, bu, bv)) {
+            if (triangle_hit(s.tris, j, L.o, L.d, L.tmax, t, bu, bv)) {
                 if (L.any) {
                     L.blocked = true;
                     L.state = ST_DONE;
@@ -164,8 +194,8 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
                 L.tmax = t;
                 L.hit_inst = L.inst;
                 L.hit_tri = j;
-                L.hu = bu;
-                L.hv = bv;
+                cold.f(C_HU) = bu;
+                cold.f(C_HV) = bv;
             }
         }
     }
@@ -174,12 +204,20 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, int *st
     for (;;) {
         while (L.sp > 0 && st_t[L.sp - 1] >= L.tmax) --L.sp;
         if (L.sp == 0) {
+            if (L.in_blas) {  // the world-space ray back, for completion
+                L.o = cold.get3(C_WO);
+                L.d = cold.get3(C_WD);
+                L.in_blas = false;
+            }
             L.state = ST_DONE;
             return;
         }
         --L.sp;
         const int c = st_cnt[L.sp];
         if (c == MARKER) {
+            L.o = cold.get3(C_WO);
+            L.d = cold.get3(C_WD);
+            L.inv = cold.get3(C_WINV);
             L.in_blas = false;
             continue;
         }
@@ -208,8 +246,8 @@ __device__ __forceinline__ void write_rgb(uint8_t *rgb, long long pix, float3 ra
 
 // A new job from its item number. Items run over views, then 4 x 4 pixel tiles, then the pixels of a tile,
 // then (when both are asked for) the picture ray and the centre ray of a pixel.
-__device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, Lane &L, long long item, int kinds,
-    int tiles_x, int tiles_per_view) {
+__device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, Lane &L, const ColdRef &cold,
+    long long item, int kinds, int tiles_x, int tiles_per_view) {
     int job = JOB_RGB;
     if (kinds == 3) {
         job = (item & 1) ? JOB_AOV : JOB_RGB;
@@ -228,7 +266,7 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
         return;
     }
     L.job = job;
-    L.pix = (static_cast<long long>(view) * a.height + y) * a.width + x;
+    cold.put_pix((static_cast<long long>(view) * a.height + y) * a.width + x);
     L.world = view / a.cameras_per_world;
     const float *m = a.cameras + 12 * static_cast<size_t>(view);
     float cm[12];
@@ -239,13 +277,14 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
     float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f;
     if (job == JOB_RGB) {
-        L.rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
-        const float jx = rand_float(L.rng);
-        const float jy = rand_float(L.rng);
+        uint32_t rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
+        const float jx = rand_float(rng);
+        const float jy = rand_float(rng);
+        cold.i(C_RNG) = static_cast<int>(rng);
         px = static_cast<float>(x) + jx;
         py = static_cast<float>(y) + jy;
     }
-    L.fwd = fwd;
+    cold.put3(C_FWD, fwd);
     L.o = mk3(cm[3], cm[7], cm[11]);
     L.d = camera_dir(right, up, fwd, px, py, fw, fh, a.fov_scale, a.aspect);
     // Spheres and the floor first; the meshes are walked with their closest hit as the limit
@@ -267,33 +306,36 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
             hit_floor = true;
         }
     }
-    L.best_sphere = best_sphere;
-    L.hit_floor = hit_floor;
+    cold.i(C_SPHERE) = best_sphere;
+    cold.i(C_FLOOR) = hit_floor ? 1 : 0;
     L.tmax = best;
     L.any = false;
     start_walk(s, L);
 }
 
 // What happens when a lane's walk ends: outputs, and for a lit picture hit, its shadow ray.
-__device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, Lane &L) {
+__device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, Lane &L, const ColdRef &cold) {
+    const long long pix = cold.pix();
     if (L.job == JOB_SHADOW) {
-        write_rgb(a.rgb, L.pix, L.blocked ? L.c_shadow : L.c_lit);
+        write_rgb(a.rgb, pix, cold.get3(L.blocked ? C_SHADOW : C_LIT));
         L.state = ST_IDLE;
         return;
     }
     const bool mesh = L.hit_inst >= 0;
-    const bool found = mesh || L.best_sphere >= 0 || L.hit_floor;
+    const int best_sphere = cold.i(C_SPHERE);
+    const bool hit_floor = cold.i(C_FLOOR) != 0;
+    const bool found = mesh || best_sphere >= 0 || hit_floor;
     float3 normal = mk3(0.0f, 0.0f, 0.0f), point = mk3(0.0f, 0.0f, 0.0f);
     DevMaterial mat{};
     int object = OBJECT_NONE;
     if (found) {  // the surface, as scene_intersect resolves it (src/render_core.h:116-141)
         point = L.o + L.d * L.tmax;
         if (mesh) {
-            normal = mesh_surface(s, L.hit_inst, L.hit_tri, L.hu, L.hv, L.d);
+            normal = mesh_surface(s, L.hit_inst, L.hit_tri, cold.f(C_HU), cold.f(C_HV), L.d);
             const int slot = L.hit_inst - L.world * s.per_world;
             mat = s.slot_material[slot];
             object = OBJECT_INSTANCE + slot;
-        } else if (L.hit_floor) {
+        } else if (hit_floor) {
             object = OBJECT_FLOOR;
             normal = mk3(0.0f, 1.0f, 0.0f);
             mat = s.floor.m;
@@ -302,14 +344,14 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             const float3 tint = ((cx + cz) & 1) ? mk3(1.0f, 1.0f, 1.0f) : mk3(1.0f, 0.7f, 0.3f);
             mat.diffuse_color = tint * 0.3f;
         } else {
-            normal = normalize(point - s.spheres[L.best_sphere].center);
-            mat = s.spheres[L.best_sphere].m;
-            object = OBJECT_SPHERE + L.best_sphere;
+            normal = normalize(point - s.spheres[best_sphere].center);
+            mat = s.spheres[best_sphere].m;
+            object = OBJECT_SPHERE + best_sphere;
         }
     }
     if (L.job == JOB_AOV) {  // aov_pixel (src/render_core.h:313-327)
-        const size_t p = static_cast<size_t>(L.pix);
-        if (a.depth) a.depth[p] = found ? L.tmax * dot(L.d, L.fwd) : __int_as_float(0x7f800000);
+        const size_t p = static_cast<size_t>(pix);
+        if (a.depth) a.depth[p] = found ? L.tmax * dot(L.d, cold.get3(C_FWD)) : __int_as_float(0x7f800000);
         if (a.normal) {
             a.normal[3 * p] = normal.x;
             a.normal[3 * p + 1] = normal.y;
@@ -319,8 +361,8 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
         if (a.hit_instance) {
             a.hit_instance[p] = mesh ? L.hit_inst : -1;
             a.hit_triangle[p] = mesh ? __ldg(s.tri_index + L.hit_tri) : -1;
-            a.hit_u[p] = mesh ? L.hu : 0.0f;
-            a.hit_v[p] = mesh ? L.hv : 0.0f;
+            a.hit_u[p] = mesh ? cold.f(C_HU) : 0.0f;
+            a.hit_v[p] = mesh ? cold.f(C_HV) : 0.0f;
         }
         L.state = ST_IDLE;
         return;
@@ -329,16 +371,17 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
     if (!found) {
         const float t = saturate(dot(L.d, s.env_up) * 0.5f + 0.5f);
         const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
-        write_rgb(a.rgb, L.pix, mk3(0.0f, 0.0f, 0.0f) + sky * 1.0f);
+        write_rgb(a.rgb, pix, mk3(0.0f, 0.0f, 0.0f) + sky * 1.0f);
         L.state = ST_IDLE;
         return;
     }
     const float3 zero = mk3(0.0f, 0.0f, 0.0f);
     if (s.light_count == 1) {
         const DevLight &lt = s.lights[0];
-        const float z = 1.0f - 2.0f * rand_float(L.rng);
+        uint32_t rng = static_cast<uint32_t>(cold.i(C_RNG));
+        const float z = 1.0f - 2.0f * rand_float(rng);
         const float rad = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-        const float phi = 6.28318530718f * rand_float(L.rng);
+        const float phi = 6.28318530718f * rand_float(rng);
         const float3 lp = lt.position + mk3(rad * cosf(phi), rad * sinf(phi), z) * lt.radius;
         const float3 to_light = lp - point;
         const float light_distance = sqrtf(dot(to_light, to_light));
@@ -348,8 +391,9 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             const float3 lit = lt.color * strength;
             const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
             const float3 specular = zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), L.d)), mat.exponent);
-            L.c_lit = radiance_of(mat, s.ambient, diffuse, specular);
-            L.c_shadow = radiance_of(mat, s.ambient, zero, zero);
+            const float3 c_shadow = radiance_of(mat, s.ambient, zero, zero);
+            cold.put3(C_LIT, radiance_of(mat, s.ambient, diffuse, specular));
+            cold.put3(C_SHADOW, c_shadow);
             // The shadow ray: spheres and the floor first, then any hit in the meshes (scene_occluded,
             // src/render_core.h:146-161).
             L.job = JOB_SHADOW;
@@ -367,7 +411,7 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
                 blocked = floor_hit(s.floor, L.o, L.d, light_distance, dd);
             }
             if (blocked) {
-                write_rgb(a.rgb, L.pix, L.c_shadow);
+                write_rgb(a.rgb, pix, c_shadow);
                 L.state = ST_IDLE;
                 return;
             }
@@ -375,24 +419,30 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             return;
         }
     }
-    write_rgb(a.rgb, L.pix, radiance_of(mat, s.ambient, zero, zero));
+    write_rgb(a.rgb, pix, radiance_of(mat, s.ambient, zero, zero));
     L.state = ST_IDLE;
 }
 
-__global__ void __launch_bounds__(256) render_persistent_kernel(const __grid_constant__ SceneParams s, const RenderArgs a,
-    int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill) {
+// THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget (65536 / (THREADS * MIN_BLOCKS)):
+// the walk's temporaries fit 64 registers without spilling, which doubles the warps per scheduler over the
+// compiler's unbounded choice (92).
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(const __grid_constant__ SceneParams s,
+    const RenderArgs a, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill) {
+    extern __shared__ float cold_smem[];
     int st_ref[STACK], st_cnt[STACK];
     float st_t[STACK];
     const int lane = threadIdx.x & 31;
     const unsigned lanes_below = (1u << lane) - 1u;
+    const ColdRef cold{cold_smem + threadIdx.x, THREADS};
     Lane L;
     L.state = ST_IDLE;
     // A correct walk visits each node of its world's tree once and each node of an entered mesh's tree once.
     const long long cap = 2LL * s.per_world + 2 + static_cast<long long>(s.per_world) * (s.blas_node_count + 2);
-    L.max_steps = cap > INT_MAX ? INT_MAX : static_cast<int>(cap);
+    const int max_steps = cap > INT_MAX ? INT_MAX : static_cast<int>(cap);
     bool exhausted = false;
     for (;;) {
-        if (L.state == ST_DONE) complete(s, a, L);
+        if (L.state == ST_DONE) complete(s, a, L, cold);
         const unsigned idle = __ballot_sync(FULL, L.state == ST_IDLE);
         if (!exhausted && idle != 0 && (__popc(idle) >= refill || idle == FULL)) {
             const int k = __popc(idle);
@@ -403,7 +453,7 @@ __global__ void __launch_bounds__(256) render_persistent_kernel(const __grid_con
             if (base + k >= total) exhausted = true;
             if (L.state == ST_IDLE) {
                 const long long item = base + __popc(idle & lanes_below);
-                if (item < total) start_job(s, a, L, item, kinds, tiles_x, tiles_per_view);
+                if (item < total) start_job(s, a, L, cold, item, kinds, tiles_x, tiles_per_view);
             }
         }
         const unsigned busy = __ballot_sync(FULL, L.state != ST_IDLE);
@@ -413,7 +463,7 @@ __global__ void __launch_bounds__(256) render_persistent_kernel(const __grid_con
         }
         // Walk until enough lanes are free to be worth a refill (or, once the work is all taken, until all are).
         for (;;) {
-            if (L.state == ST_WALK) walk_step(s, L, st_ref, st_cnt, st_t, a.error_flag);
+            if (L.state == ST_WALK) walk_step(s, L, cold, st_ref, st_cnt, st_t, max_steps, a.error_flag);
             const unsigned walking = __ballot_sync(FULL, L.state == ST_WALK);
             if (walking == 0) break;
             if (!exhausted && 32 - __popc(walking) >= refill) break;
@@ -421,31 +471,44 @@ __global__ void __launch_bounds__(256) render_persistent_kernel(const __grid_con
     }
 }
 
-}  // namespace
-
-cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
-    cudaStream_t stream) {
+template <int THREADS, int MIN_BLOCKS>
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, cudaStream_t stream) {
     const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
     const int tiles_per_view = tiles_x * tiles_y;
     const int kinds = (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
     if (kinds == 0) return cudaSuccess;
     const long long total = 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
+    auto kernel = render_persistent_kernel<THREADS, MIN_BLOCKS>;
+    const size_t smem = static_cast<size_t>(C_FIELDS) * THREADS * sizeof(float);
     int device = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_persistent_kernel, t.threads, 0);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // Enough resident warps to fill every SM, and no more warps than there are jobs for.
     long long blocks = static_cast<long long>(sms) * per_sm;
-    const long long needed = (total + t.threads - 1) / t.threads;
+    const long long needed = (total + THREADS - 1) / THREADS;
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    render_persistent_kernel<<<static_cast<unsigned>(blocks), t.threads, 0, stream>>>(s, a, counter, total, kinds, tiles_x,
-        tiles_per_view, t.refill);
+    kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, counter, total, kinds, tiles_x, tiles_per_view,
+        refill);
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
+    cudaStream_t stream) {
+    // (threads per CTA, register budget) -> the instantiation with that budget.
+    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, t.refill, stream);
+    if (t.threads == 128 && t.registers == 72) return launch_variant<128, 7>(s, a, counter, t.refill, stream);
+    if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10>(s, a, counter, t.refill, stream);
+    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, t.refill, stream);
+    if (t.threads == 256 && t.registers == 48) return launch_variant<256, 5>(s, a, counter, t.refill, stream);
+    if (t.threads == 64 && t.registers == 64) return launch_variant<64, 16>(s, a, counter, t.refill, stream);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace ngb

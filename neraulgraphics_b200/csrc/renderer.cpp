@@ -108,7 +108,7 @@ struct Renderer {
     DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: the per-pixel kernel, 2: the persistent kernel
-    PersistentTuning tuning{256, 16};
+    PersistentTuning tuning{128, 16, 64};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -809,14 +809,16 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
     }
 }
 
-int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes) {
+int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes,
+    int32_t registers) {
     return guarded(h, [&](ngb::Renderer &r) {
         ngb::require(kernel >= 0 && kernel <= 2, "kernel must be 0 (automatic), 1 (per pixel) or 2 (persistent)");
-        ngb::require(threads_per_block >= 32 && threads_per_block <= 256 && threads_per_block % 32 == 0,
-            "threads_per_block must be a multiple of 32 from 32 to 256");
+        const bool built = (threads_per_block == 128 && (registers == 48 || registers == 64 || registers == 72)) ||
+            (threads_per_block == 256 && (registers == 48 || registers == 64)) || (threads_per_block == 64 && registers == 64);
+        ngb::require(built, "threads_per_block and registers must be one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64");
         ngb::require(refill_lanes >= 1 && refill_lanes <= 32, "refill_lanes must be 1 to 32");
         r.kernel_choice = kernel;
-        r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes};
+        r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers};
     });
 }
 

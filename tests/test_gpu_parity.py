@@ -282,7 +282,7 @@ def test_both_render_kernels_are_the_oracles(torch_cuda, kernel):
     cams = np.repeat(wl.cameras, 2, axis=0)
     cams[1::2, :, 3] += np.float32([0.3, 0.0, 0.0])
     r, o = product(desc), O.Oracle(desc)
-    r.set_tuning(kernel=kernel, threads_per_block=128, refill_lanes=8)
+    r.set_tuning(kernel=kernel, threads_per_block=128, refill_lanes=8, registers=48)
     r.set_instance_transforms(wl.matrices)
     o.set_instance_transforms(wl.matrices)
     r.ambient = 0.05
@@ -317,6 +317,6 @@ def test_persistent_kernel_tunings_agree(torch_cuda):
     out = dict(rgb=True, depth=True, object_ids=True)
     r.set_tuning(kernel=1)
     want = r.render(wl.cameras, 1.0, 1, **out)
-    for threads, refill in ((256, 16), (128, 4), (64, 32), (32, 1)):
-        r.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill)
+    for threads, refill, regs in ((256, 16, 64), (128, 4, 72), (64, 32, 64), (128, 1, 48), (256, 24, 48)):
+        r.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs)
         assert_same_images(r.render(wl.cameras, 1.0, 1, **out), want, rgb_tol=0)
