@@ -271,7 +271,7 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
  * most one light, no material with reflectivity >= 1e-3), 1 the per-pixel kernel, 2 the persistent kernel
  * where it applies. The persistent kernel's shape: threads_per_block and registers (the register budget per
  * thread) as one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64, and refill_lanes (1..32: a warp takes new
- * pixels once this many of its lanes are free). Defaults: 0, 128, 16, 64. */
+ * pixels once this many of its lanes are free). Defaults: 0, 128, 28, 72. */
 int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers);
 
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
@@ -307,6 +307,11 @@ int ngb_record_hits(ngb_renderer *r, int32_t on);
  * Host arrays of view_count * height * width; any may be NULL. Filled by renders made with
  * ngb_record_hits on that asked for NGB_OUTPUT_DEPTH, NGB_OUTPUT_NORMAL or NGB_OUTPUT_OBJECT_ID. */
 int ngb_inspect_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *u, float *v);
+
+/* The 256 sRGB byte thresholds the renderer uses (host only): thresholds[k] is the smallest float whose sRGB
+ * byte, (uint8)(saturate(srgb(saturate(v))) * 255 + 0.5) with the host's powf (src/geom_dev.h:169-182), is k
+ * or more; thresholds[0] = 0. */
+int ngb_srgb_thresholds(float *thresholds);
 
 /* The meshes' bottom-level trees exactly as ngb_create builds them, on the host only (no GPU needed): call
  * with NULL arrays for the counts, then with arrays of node_count x 8 words (bvh::Node: lo xyz, a,

@@ -102,6 +102,7 @@ struct SceneParams {
     const int2 *slot_root;     // per slot: its mesh root's reference (node, 0) or (first triangle, count)
     const float *slot_bounds;  // per slot: its mesh's box in mesh space, 6 floats
     int tlas_internal;         // n - 1: nodes below this index are internal
+    const float *srgb_table;   // 256 sRGB byte thresholds made on the host (see host.h: srgb_thresholds)
 };
 
 // ---------------------------------------------------------------------------------------------- math --
@@ -116,7 +117,9 @@ __device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.
 __device__ __forceinline__ float3 cross(float3 a, float3 b) {
     return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-__device__ __forceinline__ float3 normalize(float3 v) { return v * (1.0f / sqrtf(dot(v, v))); }
+// 1 / x correctly rounded: the same float as 1.0f / x, by the reciprocal's own rounding sequence.
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float3 normalize(float3 v) { return v * recip(sqrtf(dot(v, v))); }
 __device__ __forceinline__ float saturate(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
 __device__ __forceinline__ float3 reflect(float3 i, float3 n) { return i - n * (2.0f * dot(i, n)); }
 __device__ __forceinline__ float3 xyz(float4 v) { return mk3(v.x, v.y, v.z); }

@@ -394,4 +394,27 @@ BuiltMeshes build_meshes(const ngb_scene &s) {
     return out;
 }
 
+uint8_t srgb_byte(float v) {
+    const float x = std::fmin(std::fmax(v, 0.0f), 1.0f);
+    const float c = x <= 0.0031308f ? 12.92f * x : 1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f;
+    return static_cast<uint8_t>(std::fmin(std::fmax(c, 0.0f), 1.0f) * 255.0f + 0.5f);
+}
+
+void srgb_thresholds(float t[256]) {
+    t[0] = 0.0f;
+    // Floats in [0, 1] are ordered like their bit patterns, so bisect on the bits.
+    const uint32_t one = 0x3f800000u;
+    for (int k = 1; k < 256; ++k) {
+        uint32_t lo = 0, hi = one;  // byte(lo) < k <= byte(hi)
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            float m;
+            std::memcpy(&m, &mid, 4);
+            if (srgb_byte(m) >= k) hi = mid;
+            else lo = mid;
+        }
+        std::memcpy(&t[k], &hi, 4);
+    }
+}
+
 }  // namespace ngb

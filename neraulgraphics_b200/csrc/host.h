@@ -60,4 +60,11 @@ struct BuiltMeshes {
 
 BuiltMeshes build_meshes(const ngb_scene &s);
 
+// The sRGB byte of a linear value, (uint8)(saturate(srgb(saturate(v))) * 255 + 0.5) with srgb's 1/2.4 power
+// taken by the host's powf (src/geom_dev.h:169-182, render_core.h:280-282), as 255 thresholds: t[k] (k = 1..255)
+// is the smallest float whose byte is k or more, t[0] = 0. The byte of v is the number of k >= 1 with
+// t[k] <= v. Found by bisection over the floats of [0, 1] (the mapping is monotonic there).
+void srgb_thresholds(float t[256]);
+uint8_t srgb_byte(float v);  // the mapping itself, on the host
+
 }  // namespace ngb

@@ -60,6 +60,7 @@ struct RenderArgs {
     float *hit_u;
     float *hit_v;
     int *error_flag;               // set nonzero if a traversal stack would overflow
+    float4 *camera_basis;          // views x 3: scratch for the persistent kernel's per-view camera
 };
 cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream);
 

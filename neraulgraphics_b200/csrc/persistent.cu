@@ -183,20 +183,26 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, const C
             return;
         }
     } else {
-        for (int j = L.ref; j < L.ref + L.count; ++j) {
-            float t, bu, bv;
-            if (triangle_hit(s.tris, j, L.o, L.d, L.tmax, t, bu, bv)) {
-                if (L.any) {
-                    L.blocked = true;
-                    L.state = ST_DONE;
-                    return;
-                }
-                L.tmax = t;
-                L.hit_inst = L.inst;
-                L.hit_tri = j;
-                cold.f(C_HU) = bu;
-                cold.f(C_HV) = bv;
+        // One triangle of the leaf per step, in the leaf's order, so a step costs about the same whether it
+        // tests boxes or a triangle.
+        const int j = L.ref;
+        float t, bu, bv;
+        if (triangle_hit(s.tris, j, L.o, L.d, L.tmax, t, bu, bv)) {
+            if (L.any) {
+                L.blocked = true;
+                L.state = ST_DONE;
+                return;
             }
+            L.tmax = t;
+            L.hit_inst = L.inst;
+            L.hit_tri = j;
+            cold.f(C_HU) = bu;
+            cold.f(C_HV) = bv;
+        }
+        if (L.count > 1) {
+            ++L.ref;
+            --L.count;
+            return;
         }
     }
     // Dead end: resume from the stack, dropping what a closer hit has put out of reach; a marker hands the walk
@@ -235,13 +241,13 @@ __device__ __forceinline__ float3 radiance_of(const DevMaterial &m, float ambien
 }
 
 // sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283).
-__device__ __forceinline__ void write_rgb(uint8_t *rgb, long long pix, float3 radiance) {
+__device__ __forceinline__ void write_rgb(const float *table, uint8_t *rgb, long long pix, float3 radiance) {
     float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
     sum = sum * (1.0f / 1.0f);
     uint8_t *o = rgb + 3 * static_cast<size_t>(pix);
-    o[0] = to_byte(srgb_channel(sum.x));
-    o[1] = to_byte(srgb_channel(sum.y));
-    o[2] = to_byte(srgb_channel(sum.z));
+    o[0] = srgb_byte(table, sum.x);
+    o[1] = srgb_byte(table, sum.y);
+    o[2] = srgb_byte(table, sum.z);
 }
 
 // A new job from its item number. Items run over views, then 4 x 4 pixel tiles, then the pixels of a tile,
@@ -268,12 +274,13 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
     L.job = job;
     cold.put_pix((static_cast<long long>(view) * a.height + y) * a.width + x);
     L.world = view / a.cameras_per_world;
-    const float *m = a.cameras + 12 * static_cast<size_t>(view);
-    float cm[12];
-    for (int k = 0; k < 12; ++k) cm[k] = __ldg(m + k);
-    const float3 right = normalize(mk3(cm[0], cm[4], cm[8]));
-    const float3 up = normalize(mk3(cm[1], cm[5], cm[9]));
-    const float3 fwd = normalize(mk3(-cm[2], -cm[6], -cm[10]));
+    // The view's camera (camera_from_matrix, src/render_core.h:264-273), made once per view by
+    // prepare_cameras: (position.xyz, right.x) (right.yz, up.xy) (up.z, forward.xyz).
+    const float4 c0 = __ldcg(a.camera_basis + 3 * view), c1 = __ldcg(a.camera_basis + 3 * view + 1);
+    const float4 c2 = __ldcg(a.camera_basis + 3 * view + 2);
+    const float3 right = mk3(c0.w, c1.x, c1.y);
+    const float3 up = mk3(c1.z, c1.w, c2.x);
+    const float3 fwd = mk3(c2.y, c2.z, c2.w);
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
     float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f;
     if (job == JOB_RGB) {
@@ -285,7 +292,7 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
         py = static_cast<float>(y) + jy;
     }
     cold.put3(C_FWD, fwd);
-    L.o = mk3(cm[3], cm[7], cm[11]);
+    L.o = mk3(c0.x, c0.y, c0.z);
     L.d = camera_dir(right, up, fwd, px, py, fw, fh, a.fov_scale, a.aspect);
     // Spheres and the floor first; the meshes are walked with their closest hit as the limit
     // (scene_intersect, src/render_core.h:78-112).
@@ -317,7 +324,7 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
 __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, Lane &L, const ColdRef &cold) {
     const long long pix = cold.pix();
     if (L.job == JOB_SHADOW) {
-        write_rgb(a.rgb, pix, cold.get3(L.blocked ? C_SHADOW : C_LIT));
+        write_rgb(s.srgb_table, a.rgb, pix, cold.get3(L.blocked ? C_SHADOW : C_LIT));
         L.state = ST_IDLE;
         return;
     }
@@ -371,7 +378,7 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
     if (!found) {
         const float t = saturate(dot(L.d, s.env_up) * 0.5f + 0.5f);
         const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
-        write_rgb(a.rgb, pix, mk3(0.0f, 0.0f, 0.0f) + sky * 1.0f);
+        write_rgb(s.srgb_table, a.rgb, pix, mk3(0.0f, 0.0f, 0.0f) + sky * 1.0f);
         L.state = ST_IDLE;
         return;
     }
@@ -411,7 +418,7 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
                 blocked = floor_hit(s.floor, L.o, L.d, light_distance, dd);
             }
             if (blocked) {
-                write_rgb(a.rgb, pix, c_shadow);
+                write_rgb(s.srgb_table, a.rgb, pix, c_shadow);
                 L.state = ST_IDLE;
                 return;
             }
@@ -419,7 +426,7 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             return;
         }
     }
-    write_rgb(a.rgb, pix, radiance_of(mat, s.ambient, zero, zero));
+    write_rgb(s.srgb_table, a.rgb, pix, radiance_of(mat, s.ambient, zero, zero));
     L.state = ST_IDLE;
 }
 
@@ -471,6 +478,20 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
     }
 }
 
+// One thread per view: the camera basis of camera_from_matrix (src/render_core.h:264-273), renormalised.
+__global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *cameras, int views, float4 *basis) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= views) return;
+    float m[12];
+    for (int k = 0; k < 12; ++k) m[k] = __ldg(cameras + 12 * static_cast<size_t>(v) + k);
+    const float3 right = normalize(mk3(m[0], m[4], m[8]));
+    const float3 up = normalize(mk3(m[1], m[5], m[9]));
+    const float3 fwd = normalize(mk3(-m[2], -m[6], -m[10]));
+    basis[3 * v] = make_float4(m[3], m[7], m[11], right.x);
+    basis[3 * v + 1] = make_float4(right.y, right.z, up.x, up.y);
+    basis[3 * v + 2] = make_float4(up.z, fwd.x, fwd.y, fwd.z);
+}
+
 template <int THREADS, int MIN_BLOCKS>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, cudaStream_t stream) {
     const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
@@ -492,6 +513,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
+    prepare_cameras_kernel<<<(a.views + 127) / 128, 128, 0, stream>>>(a.cameras, a.views, a.camera_basis);
     kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, counter, total, kinds, tiles_x, tiles_per_view,
         refill);
     return cudaGetLastError();

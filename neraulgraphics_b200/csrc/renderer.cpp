@@ -106,9 +106,11 @@ struct Renderer {
     DevBuf<float4> blas_pairs, tlas_pairs;
     DevBuf<int2> slot_root;
     DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
+    DevBuf<float4> camera_basis;              // the persistent render's per-view cameras
+    DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: the per-pixel kernel, 2: the persistent kernel
-    PersistentTuning tuning{128, 16, 64};
+    PersistentTuning tuning{128, 28, 72};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -216,6 +218,13 @@ Renderer::Renderer(const ngb_scene &s) {
     reflective = reflective || (s.floor.half_extent_x > 0.0f && s.floor.material.reflectivity >= 1e-3f);
     for (int i = 0; i < s.instance_count; ++i) reflective = reflective || s.instances[i].material.reflectivity >= 1e-3f;
     work_counter.ensure(1);
+    {
+        float table[256];
+        srgb_thresholds(table);
+        srgb_table.ensure(256);
+        CK(cudaMemcpy(srgb_table.p, table, sizeof(table), cudaMemcpyHostToDevice));
+        params.srgb_table = srgb_table.p;
+    }
     params.floor = DevPlane{s.floor.y, s.floor.half_extent_x, s.floor.z_min, s.floor.z_max, s.floor.checker_scale,
         dev_material(s.floor.material)};
     params.env_up = make_float3(0.0f, 1.0f, 0.0f);
@@ -316,6 +325,7 @@ Renderer::~Renderer() {
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
+    camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
     hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
@@ -498,6 +508,7 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     const bool persistent = kernel_choice == 2 ? persistent_ok : (kernel_choice == 0 && persistent_ok);
     CK(cudaEventRecord(ev_start, stream));
     if (persistent) {
+        a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
         CK(launch_render_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
     } else {
         CK(launch_render(params, a, stream));
@@ -820,6 +831,12 @@ int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, i
         r.kernel_choice = kernel;
         r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers};
     });
+}
+
+int ngb_srgb_thresholds(float *thresholds) {
+    if (!thresholds) return NGB_INVALID_ARGUMENT;
+    ngb::srgb_thresholds(thresholds);
+    return NGB_OK;
 }
 
 int ngb_record_hits(ngb_renderer *h, int32_t on) {

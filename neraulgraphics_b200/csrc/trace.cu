@@ -56,9 +56,9 @@ __global__ void __launch_bounds__(128) render_kernel(const __grid_constant__ Sce
         }
         sum = sum * (1.0f / static_cast<float>(a.spp));
         uint8_t *o = a.rgb + 3 * pix;
-        o[0] = to_byte(srgb_channel(sum.x));
-        o[1] = to_byte(srgb_channel(sum.y));
-        o[2] = to_byte(srgb_channel(sum.z));
+        o[0] = srgb_byte(s.srgb_table, sum.x);
+        o[1] = srgb_byte(s.srgb_table, sum.y);
+        o[2] = srgb_byte(s.srgb_table, sum.z);
     }
     if (a.depth || a.normal || a.object_id || a.hit_instance) {  // aov_pixel (src/render_core.h:313-327)
         const float3 dir = camera_ray(static_cast<float>(x) + 0.5f, static_cast<float>(y) + 0.5f);

@@ -14,7 +14,7 @@ __device__ __forceinline__ float3 safe_inverse(float3 d) {
     const float x = fabsf(d.x) < 1e-12f ? copysignf(1e-12f, d.x) : d.x;
     const float y = fabsf(d.y) < 1e-12f ? copysignf(1e-12f, d.y) : d.y;
     const float z = fabsf(d.z) < 1e-12f ? copysignf(1e-12f, d.z) : d.z;
-    return mk3(1.0f / x, 1.0f / y, 1.0f / z);
+    return mk3(recip(x), recip(y), recip(z));
 }
 
 // Slab test (src/mesh_dev.h:66-74): where the ray enters the box, or NO_HIT.
@@ -36,7 +36,7 @@ __device__ __forceinline__ bool triangle_hit(const float4 *tris, int i, float3 o
     const float3 p = cross(d, e2);
     const float det = dot(e1, p);
     if (fabsf(det) < 1e-14f) return false;
-    const float inv_det = 1.0f / det;
+    const float inv_det = recip(det);
     const float3 s = o - v0;
     const float u = dot(s, p) * inv_det;
     if (u < 0.0f || u > 1.0f) return false;
@@ -360,7 +360,7 @@ __device__ __forceinline__ float3 trace(const SceneParams &s, int world, float3 
             const float3 lp = L.position + mk3(rad * cosf(phi), rad * sinf(phi), z) * L.radius;
             const float3 to_light = lp - hit.point;
             const float light_distance = sqrtf(dot(to_light, to_light));
-            const float3 light_dir = to_light * (1.0f / light_distance);
+            const float3 light_dir = to_light * recip(light_distance);
             const float strength = L.intensity * light_factor(L, light_dir, light_distance);
             if (strength <= 0.0f) continue;
             if (scene_occluded(s, world, offset_origin(hit.point, hit.normal, light_dir), light_dir, light_distance, err))
@@ -385,6 +385,20 @@ __device__ __forceinline__ float srgb_channel(float v) {
 }
 
 __device__ __forceinline__ uint8_t to_byte(float c) { return static_cast<uint8_t>(saturate(c) * 255.0f + 0.5f); }
+
+// The sRGB byte of a linear value, exactly as the host's powf makes it (src/geom_dev.h:169-176,
+// render_core.h:280): a guess from the fast approximate power, then moved to the k with
+// table[k] <= v < table[k + 1] (the table holds each byte's first float, made on the host and checked
+// against every float of [0, 1]). A NaN stays at 0, as saturate makes it.
+__device__ __forceinline__ uint8_t srgb_byte(const float *table, float v) {
+    const float x = saturate(v);
+    const float c = x <= 0.0031308f ? 12.92f * x : 1.055f * __powf(x, 1.0f / 2.4f) - 0.055f;
+    int k = static_cast<int>(saturate(c) * 255.0f + 0.5f);
+    while (k < 255 && v >= __ldg(table + k + 1)) ++k;
+    while (k > 0 && v < __ldg(table + k)) --k;
+    return static_cast<uint8_t>(k);
+}
+
 
 }  // namespace
 }  // namespace tr

@@ -293,7 +293,7 @@ class BatchRenderer:
 
     # ----------------------------------------------------------------------------------------- inspection --
 
-    def set_tuning(self, kernel=0, threads_per_block=128, refill_lanes=16, registers=64):
+    def set_tuning(self, kernel=0, threads_per_block=128, refill_lanes=28, registers=72):
         """kernel: 0 automatic, 1 the per-pixel kernel, 2 the persistent kernel (where it applies: one sample per
         pixel, at most one light, no reflective material); threads_per_block, registers and refill_lanes tune
         the latter (see ngb_set_tuning)."""

@@ -1417,6 +1417,25 @@ void orc_blas(const orc_scene *s, int *node_count, int *triangle_count, int32_t 
     if (triangle_index) memcpy(triangle_index, s->tri_index, sizeof(int32_t) * s->tri_count);
 }
 
+/* The sRGB byte of every float in [0, 1], scanned in order: returns the number of places where the byte goes
+ * down (0 when the mapping is monotonic) and fills first[k], the first float whose byte is k or more. */
+long long orc_srgb_scan(float *first) {
+    long long drops = 0;
+    int prev = 0;
+    for (int k = 0; k < 256; ++k) first[k] = 2.0f;
+    first[0] = 0.0f;
+    for (uint32_t bitsv = 0; bitsv <= 0x3f800000u; ++bitsv) {
+        float v;
+        memcpy(&v, &bitsv, 4);
+        const float c = srgb_channel(v);
+        const int b = (uint8_t)(saturate(c) * 255.0f + 0.5f);
+        if (b < prev) ++drops;
+        for (int k = prev + 1; k <= b; ++k) first[k] = v;
+        if (b > prev) prev = b;
+    }
+    return drops;
+}
+
 void orc_traversal_bytes(const orc_scene *s, double *bytes, double *rays) {
     *bytes = s->trav_bytes;
     *rays = s->trav_rays;

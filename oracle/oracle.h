@@ -66,6 +66,10 @@ void orc_blas(const orc_scene *s, int *node_count, int *triangle_count, int32_t 
  * 64 per pair of child boxes tested, 48 per instance entered, 48 per triangle tested. rays: the rays traced. */
 void orc_traversal_bytes(const orc_scene *s, double *bytes, double *rays);
 
+/* Scans the sRGB byte (src/geom_dev.h:169-176, render_core.h:280) of every float in [0, 1]: the number of
+ * decreases, and the first float reaching each byte. */
+long long orc_srgb_scan(float *first);
+
 /* Single-precision compose alone (src/cuda_backend.cu:165-202), for pinning the GPU compose kernel. */
 void orc_compose(int worlds, int per_world, int bodies_per_world, const int32_t *body_of_instance,
     const float *local_pose, const float *scale, const float *poses, float *matrices);

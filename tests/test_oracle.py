@@ -227,3 +227,20 @@ def test_workloads_are_deterministic():
     s2 = workloads.random_walk(b.poses, 3, seed=1)
     assert np.array_equal(s1, s2) and s1.shape == (3, 4, 20, 7)
     assert np.allclose(np.linalg.norm(s1[..., 3:], axis=-1), 1.0, atol=1e-6)
+
+
+def test_srgb_threshold_table_reproduces_the_host_mapping_for_every_float():
+    """The renderer turns linear light into sRGB bytes with a threshold table made on the host by bisection;
+    an exhaustive scan of every float in [0, 1] (the oracle's srgb_channel, the reference's formula) shows the
+    mapping never decreases and that the table's thresholds are exactly the first floats of each byte."""
+    import ctypes
+    from neraulgraphics_b200._lib import lib
+    first = np.zeros(256, np.float32)
+    L = O.oracle_lib()
+    L.orc_srgb_scan.restype = ctypes.c_longlong
+    L.orc_srgb_scan.argtypes = [ctypes.c_void_p]
+    drops = L.orc_srgb_scan(first.ctypes.data_as(ctypes.c_void_p))
+    assert drops == 0
+    table = np.zeros(256, np.float32)
+    assert lib().ngb_srgb_thresholds(table.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert np.array_equal(bits(table), bits(first))
