@@ -228,6 +228,8 @@ def run_ours(args, rank, world, local_rank, dist):
     if not args.no_autotune:
         from neraulgraphics_b200.autotune import tune
         tuned = tune(r, cams_dev, wl.fov, rgb=True, depth=True, object_ids=True, use_cache=False)
+        for t in sorted(tuned["timings"], key=lambda t: t["ms"])[:12]:
+            print("autotune", t, file=sys.stderr)
     for s in range(W):
         r.set_body_poses(poses_dev[s])
         r.render(cams_dev, wl.fov, 1, **kw)
@@ -321,7 +323,8 @@ def run_ours(args, rank, world, local_rank, dist):
         "cpu_baseline": cpu,
         "reference_cuda": ref_cuda,
         "gpu_launches": 3 * K,
-        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("threads", "registers", "refill", "ms")},
+        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("threads", "registers", "refill", "leaf_batch",
+                                                                            "ms")},
         "clocks": clk,
     }
 

@@ -270,9 +270,11 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
 /* How renders run. kernel: 0 automatic (the persistent kernel whenever it applies: one sample per pixel, at
  * most one light, no material with reflectivity >= 1e-3), 1 the per-pixel kernel, 2 the persistent kernel
  * where it applies. The persistent kernel's shape: threads_per_block and registers (the register budget per
- * thread) as one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64, and refill_lanes (1..32: a warp takes new
- * pixels once this many of its lanes are free). Defaults: 0, 128, 28, 72. */
-int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers);
+ * thread) as one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64, refill_lanes (1..32: a warp takes new
+ * pixels once this many of its lanes are free) and leaf_batch (1..32: lanes at a leaf wait until this many do,
+ * or none is at an internal node, before the warp takes a leaf step). Defaults: 0, 128, 28, 72, 16. */
+int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers,
+    int32_t leaf_batch);
 
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
  * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */

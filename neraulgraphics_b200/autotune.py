@@ -15,8 +15,8 @@ import json
 import os
 import time
 
-CANDIDATES = [(threads, regs, refill) for threads, regs in ((128, 64), (256, 64), (128, 48), (128, 72), (64, 64))
-              for refill in (8, 16, 24, 28)]
+CANDIDATES = [(threads, regs, refill, batch) for threads, regs in ((128, 64), (256, 64), (128, 48), (64, 64))
+              for refill in (16, 24, 28) for batch in (1, 8, 16, 24)]
 
 
 def cache_path() -> str:
@@ -42,7 +42,7 @@ def _load() -> dict:
 def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, object_ids=False, repeats=3,
          use_cache=True, budget_s=60.0) -> dict:
     """Times every candidate shape on this renderer and these cameras (device tensors), sets the fastest and
-    returns {"threads", "registers", "refill", "ms", "timings"}."""
+    returns {"threads", "registers", "refill", "leaf_batch", "ms", "timings"}."""
     import torch
     outputs = dict(rgb=rgb, depth=depth, normals=normals, object_ids=object_ids)
     key = _key(renderer, tuple(sorted(k for k, v in outputs.items() if v)))
@@ -50,12 +50,12 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
     if key in cache:
         best = cache[key]
         renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
-                            registers=best["registers"])
+                            registers=best["registers"], leaf_batch=best["leaf_batch"])
         return dict(best, cached=True)
     timings = []
     start = time.perf_counter()
-    for threads, regs, refill in CANDIDATES:
-        renderer.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs)
+    for threads, regs, refill, batch in CANDIDATES:
+        renderer.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs, leaf_batch=batch)
         renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -64,15 +64,16 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
             renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         e1.record()
         e1.synchronize()
-        timings.append({"threads": threads, "registers": regs, "refill": refill, "ms": e0.elapsed_time(e1) / repeats})
+        timings.append({"threads": threads, "registers": regs, "refill": refill, "leaf_batch": batch,
+                        "ms": e0.elapsed_time(e1) / repeats})
         if time.perf_counter() - start > budget_s:
             break
     best = min(timings, key=lambda t: t["ms"])
     renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
-                        registers=best["registers"])
+                        registers=best["registers"], leaf_batch=best["leaf_batch"])
     result = dict(best, timings=timings)
     if use_cache:
-        cache[key] = {k: best[k] for k in ("threads", "registers", "refill", "ms")}
+        cache[key] = {k: best[k] for k in ("threads", "registers", "refill", "leaf_batch", "ms")}
         try:
             os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
             with open(cache_path(), "w") as f:

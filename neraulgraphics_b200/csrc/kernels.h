@@ -83,6 +83,7 @@ struct PersistentTuning {
     int threads;      // per CTA: 64, 128 or 256
     int refill;       // a warp fetches new pixels once this many of its lanes are idle
     int registers;    // register budget per thread: 48, 64 or 72 (not every pair with threads is built)
+    int leaf_batch;   // a warp takes a leaf step once this many lanes wait at leaves (or none is at an inner node)
 };
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
     const PersistentTuning &t, cudaStream_t stream);

@@ -117,39 +117,66 @@ __device__ __forceinline__ void start_walk(const SceneParams &s, Lane &L) {
     L.state = ST_WALK;
 }
 
-// One node of the walk: the body of traverse's loop at either level, then its pop.
-__device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
-    float *st_t, int max_steps, int *err) {
-    if (++L.steps > max_steps) {  // only a malformed tree gets here
-        *err = 2;
-        L.state = ST_DONE;
-        return;
-    }
-    if (L.count == 0) {
-        const float4 *rec = (L.in_blas ? s.blas_pairs : s.tlas_pairs) + 4 * static_cast<long long>(L.ref);
-        const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
-        const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), L.o, L.inv, L.tmax);
-        const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), L.o, L.inv, L.tmax);
-        if (dl < NO_HIT || dr < NO_HIT) {
-            const bool left_first = dl <= dr;
-            const float far_t = left_first ? dr : dl;
-            if (far_t < NO_HIT) {
-                if (L.sp >= STACK) {
-                    *err = 1;
-                    L.state = ST_DONE;
-                    return;
-                }
-                st_ref[L.sp] = __float_as_int(left_first ? q3.z : q3.x);
-                st_cnt[L.sp] = __float_as_int(left_first ? q3.w : q3.y);
-                st_t[L.sp] = far_t;
-                ++L.sp;
-            }
-            L.ref = __float_as_int(left_first ? q3.x : q3.z);
-            L.count = __float_as_int(left_first ? q3.y : q3.w);
+// The walk's pop (traverse's dead end, src/mesh_dev.h:154-157): resume from the stack, dropping what a closer
+// hit has put out of reach; a marker hands the walk back to the world's tree.
+__device__ __forceinline__ void walk_pop(Lane &L, const ColdRef &cold, const int *st_ref, const int *st_cnt,
+    const float *st_t) {
+    for (;;) {
+        while (L.sp > 0 && st_t[L.sp - 1] >= L.tmax) --L.sp;
+        if (L.sp == 0) {
+            L.state = ST_DONE;
             return;
         }
-    } else if (L.count < 0) {
-        // An instance: into its mesh's space, and its mesh's root box test (blas_walk's first line).
+        --L.sp;
+        const int c = st_cnt[L.sp];
+        if (c == MARKER) {
+            L.o = cold.get3(C_WO);
+            L.d = cold.get3(C_WD);
+            L.inv = cold.get3(C_WINV);
+            L.in_blas = false;
+            continue;
+        }
+        L.ref = st_ref[L.sp];
+        L.count = c;
+        return;
+    }
+}
+
+// A walk step at an internal node of either tree: both children's boxes, the nearer one next, the farther one
+// pushed with its entry distance (traverse, src/mesh_dev.h:133-151).
+__device__ __forceinline__ void walk_inner(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
+    float *st_t, int *err) {
+    const float4 *rec = (L.in_blas ? s.blas_pairs : s.tlas_pairs) + 4 * static_cast<long long>(L.ref);
+    const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
+    const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), L.o, L.inv, L.tmax);
+    const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), L.o, L.inv, L.tmax);
+    if (dl < NO_HIT || dr < NO_HIT) {
+        const bool left_first = dl <= dr;
+        const float far_t = left_first ? dr : dl;
+        if (far_t < NO_HIT) {
+            if (L.sp >= STACK) {
+                *err = 1;
+                L.state = ST_DONE;
+                return;
+            }
+            st_ref[L.sp] = __float_as_int(left_first ? q3.z : q3.x);
+            st_cnt[L.sp] = __float_as_int(left_first ? q3.w : q3.y);
+            st_t[L.sp] = far_t;
+            ++L.sp;
+        }
+        L.ref = __float_as_int(left_first ? q3.x : q3.z);
+        L.count = __float_as_int(left_first ? q3.y : q3.w);
+        return;
+    }
+    walk_pop(L, cold, st_ref, st_cnt, st_t);
+}
+
+// A walk step at a leaf: an instance (into its mesh's space, and its mesh root's box test: blas_walk's first
+// line) or one triangle of a mesh leaf, in the leaf's order (mesh_intersect / mesh_occluded's leaves,
+// src/mesh_dev.h:180-226).
+__device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
+    float *st_t, int *err) {
+    if (L.count < 0) {
         const InstanceRec r = load_instance(s.inst, L.ref);
         const int slot = __float_as_int(__ldg(s.inst + 4 * L.ref + 3).y);
         const float3 lo = to_local_point(r, L.o);
@@ -183,8 +210,6 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, const C
             return;
         }
     } else {
-        // One triangle of the leaf per step, in the leaf's order, so a step costs about the same whether it
-        // tests boxes or a triangle.
         const int j = L.ref;
         float t, bu, bv;
         if (triangle_hit(s.tris, j, L.o, L.d, L.tmax, t, bu, bv)) {
@@ -205,32 +230,7 @@ __device__ __forceinline__ void walk_step(const SceneParams &s, Lane &L, const C
             return;
         }
     }
-    // Dead end: resume from the stack, dropping what a closer hit has put out of reach; a marker hands the walk
-    // back to the world's tree.
-    for (;;) {
-        while (L.sp > 0 && st_t[L.sp - 1] >= L.tmax) --L.sp;
-        if (L.sp == 0) {
-            if (L.in_blas) {  // the world-space ray back, for completion
-                L.o = cold.get3(C_WO);
-                L.d = cold.get3(C_WD);
-                L.in_blas = false;
-            }
-            L.state = ST_DONE;
-            return;
-        }
-        --L.sp;
-        const int c = st_cnt[L.sp];
-        if (c == MARKER) {
-            L.o = cold.get3(C_WO);
-            L.d = cold.get3(C_WD);
-            L.inv = cold.get3(C_WINV);
-            L.in_blas = false;
-            continue;
-        }
-        L.ref = st_ref[L.sp];
-        L.count = c;
-        return;
-    }
+    walk_pop(L, cold, st_ref, st_cnt, st_t);
 }
 
 // The radiance of a hit with these light sums, as trace computes it for a path of one bounce
@@ -435,7 +435,8 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
 // compiler's unbounded choice (92).
 template <int THREADS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(const __grid_constant__ SceneParams s,
-    const RenderArgs a, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill) {
+    const RenderArgs a, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill,
+    int leaf_batch) {
     extern __shared__ float cold_smem[];
     int st_ref[STACK], st_cnt[STACK];
     float st_t[STACK];
@@ -469,11 +470,28 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
             continue;
         }
         // Walk until enough lanes are free to be worth a refill (or, once the work is all taken, until all are).
+        // Lanes at a leaf (an instance to enter, a triangle to test) wait while the others take internal-node
+        // steps, and the warp takes a leaf step only once leaf_batch of them wait or no lane is at an internal
+        // node: each kind of step then runs with many lanes instead of every kind running in every step. A
+        // lane's own walk is unchanged, step for step.
         for (;;) {
-            if (L.state == ST_WALK) walk_step(s, L, cold, st_ref, st_cnt, st_t, max_steps, a.error_flag);
-            const unsigned walking = __ballot_sync(FULL, L.state == ST_WALK);
-            if (walking == 0) break;
-            if (!exhausted && 32 - __popc(walking) >= refill) break;
+            const bool walking = L.state == ST_WALK;
+            const unsigned at_leaf = __ballot_sync(FULL, walking && L.count != 0);
+            const unsigned at_inner = __ballot_sync(FULL, walking && L.count == 0);
+            const unsigned busy_walk = at_leaf | at_inner;
+            if (busy_walk == 0) break;
+            if (!exhausted && 32 - __popc(busy_walk) >= refill) break;
+            const bool leaf_phase = __popc(at_leaf) >= leaf_batch || at_inner == 0;
+            if (walking && (L.count != 0) == leaf_phase) {
+                if (++L.steps > max_steps) {  // a lane's own steps; only a malformed tree gets past the cap
+                    *a.error_flag = 2;
+                    L.state = ST_DONE;
+                } else if (leaf_phase) {
+                    walk_leaf(s, L, cold, st_ref, st_cnt, st_t, a.error_flag);
+                } else {
+                    walk_inner(s, L, cold, st_ref, st_cnt, st_t, a.error_flag);
+                }
+            }
         }
     }
 }
@@ -493,7 +511,8 @@ __global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *camer
 }
 
 template <int THREADS, int MIN_BLOCKS>
-cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, cudaStream_t stream) {
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, int leaf_batch,
+    cudaStream_t stream) {
     const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
     const int tiles_per_view = tiles_x * tiles_y;
     const int kinds = (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
@@ -515,7 +534,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (e != cudaSuccess) return e;
     prepare_cameras_kernel<<<(a.views + 127) / 128, 128, 0, stream>>>(a.cameras, a.views, a.camera_basis);
     kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, counter, total, kinds, tiles_x, tiles_per_view,
-        refill);
+        refill, leaf_batch);
     return cudaGetLastError();
 }
 
@@ -524,12 +543,12 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream) {
     // (threads per CTA, register budget) -> the instantiation with that budget.
-    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, t.refill, stream);
-    if (t.threads == 128 && t.registers == 72) return launch_variant<128, 7>(s, a, counter, t.refill, stream);
-    if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10>(s, a, counter, t.refill, stream);
-    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, t.refill, stream);
-    if (t.threads == 256 && t.registers == 48) return launch_variant<256, 5>(s, a, counter, t.refill, stream);
-    if (t.threads == 64 && t.registers == 64) return launch_variant<64, 16>(s, a, counter, t.refill, stream);
+    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 128 && t.registers == 72) return launch_variant<128, 7>(s, a, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10>(s, a, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 256 && t.registers == 48) return launch_variant<256, 5>(s, a, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 64 && t.registers == 64) return launch_variant<64, 16>(s, a, counter, t.refill, t.leaf_batch, stream);
     return cudaErrorInvalidValue;
 }
 

@@ -110,7 +110,7 @@ struct Renderer {
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: the per-pixel kernel, 2: the persistent kernel
-    PersistentTuning tuning{128, 28, 72};
+    PersistentTuning tuning{128, 28, 72, 16};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -821,15 +821,16 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
 }
 
 int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes,
-    int32_t registers) {
+    int32_t registers, int32_t leaf_batch) {
     return guarded(h, [&](ngb::Renderer &r) {
         ngb::require(kernel >= 0 && kernel <= 2, "kernel must be 0 (automatic), 1 (per pixel) or 2 (persistent)");
         const bool built = (threads_per_block == 128 && (registers == 48 || registers == 64 || registers == 72)) ||
             (threads_per_block == 256 && (registers == 48 || registers == 64)) || (threads_per_block == 64 && registers == 64);
         ngb::require(built, "threads_per_block and registers must be one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64");
         ngb::require(refill_lanes >= 1 && refill_lanes <= 32, "refill_lanes must be 1 to 32");
+        ngb::require(leaf_batch >= 1 && leaf_batch <= 32, "leaf_batch must be 1 to 32");
         r.kernel_choice = kernel;
-        r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers};
+        r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers, leaf_batch};
     });
 }
 

@@ -293,12 +293,12 @@ class BatchRenderer:
 
     # ----------------------------------------------------------------------------------------- inspection --
 
-    def set_tuning(self, kernel=0, threads_per_block=128, refill_lanes=28, registers=72):
+    def set_tuning(self, kernel=0, threads_per_block=128, refill_lanes=28, registers=72, leaf_batch=16):
         """kernel: 0 automatic, 1 the per-pixel kernel, 2 the persistent kernel (where it applies: one sample per
-        pixel, at most one light, no reflective material); threads_per_block, registers and refill_lanes tune
-        the latter (see ngb_set_tuning)."""
-        check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes), int(registers)),
-              self._h)
+        pixel, at most one light, no reflective material); threads_per_block, registers, refill_lanes and
+        leaf_batch tune the latter (see ngb_set_tuning)."""
+        check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes), int(registers),
+                                       int(leaf_batch)), self._h)
 
     def record_hits(self, on=True):
         check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)

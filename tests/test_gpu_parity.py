@@ -317,6 +317,7 @@ def test_persistent_kernel_tunings_agree(torch_cuda):
     out = dict(rgb=True, depth=True, object_ids=True)
     r.set_tuning(kernel=1)
     want = r.render(wl.cameras, 1.0, 1, **out)
-    for threads, refill, regs in ((256, 16, 64), (128, 4, 72), (64, 32, 64), (128, 1, 48), (256, 24, 48)):
-        r.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs)
+    for threads, refill, regs, batch in ((256, 16, 64, 1), (128, 4, 72, 32), (64, 32, 64, 8), (128, 1, 48, 16),
+                                         (256, 24, 48, 24)):
+        r.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs, leaf_batch=batch)
         assert_same_images(r.render(wl.cameras, 1.0, 1, **out), want, rgb_tol=0)
