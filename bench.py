@@ -323,8 +323,8 @@ def run_ours(args, rank, world, local_rank, dist):
         "cpu_baseline": cpu,
         "reference_cuda": ref_cuda,
         "gpu_launches": 3 * K,
-        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("threads", "registers", "refill", "leaf_batch",
-                                                                            "ms")},
+        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
+                                                                            "leaf_batch", "ms")},
         "clocks": clk,
     }
 

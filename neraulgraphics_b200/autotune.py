@@ -1,9 +1,11 @@
-"""Picks the persistent render kernel's launch shape for a workload by timing it.
+"""Picks the render kernel's launch shape for a workload by timing it.
 
-The shape is the CTA size, the register budget per thread (which sets how many warps an SM holds) and the
-refill threshold (how many of a warp's lanes must be free before it takes new pixels). The best depends on
-the scene (how long rays walk, how much they vary), so it is measured on the caller's own renderer and
-cameras, with CUDA events, and remembered in a JSON cache keyed by the GPU and the workload's shape.
+For worlds of at most 32 instances the tile kernel runs, and its shape is the CTA size and the register
+budget per thread (which sets how many warps an SM holds). Otherwise the persistent kernel runs, and its
+shape adds the refill threshold (how many of a warp's lanes must be free before it takes new pixels) and the
+leaf batch. The best depends on the scene (how long rays walk, how much they vary), so it is measured on the
+caller's own renderer and cameras, with CUDA events, and remembered in a JSON cache keyed by the GPU and the
+workload's shape.
 
     from neraulgraphics_b200.autotune import tune
     best = tune(renderer, cameras, fov=1.0, rgb=True, depth=True, object_ids=True)
@@ -17,6 +19,8 @@ import time
 
 CANDIDATES = [(threads, regs, refill, batch) for threads, regs in ((128, 64), (256, 64), (128, 48), (64, 64))
               for refill in (16, 24, 28) for batch in (1, 8, 16, 24)]
+TILE_CANDIDATES = [(128, 64, 0, 0), (128, 80, 0, 0), (128, 96, 0, 0), (256, 64, 0, 0), (256, 80, 0, 0)]
+TILE_MAX_INSTANCES = 32
 
 
 def cache_path() -> str:
@@ -31,6 +35,14 @@ def _key(renderer, outputs) -> str:
             f"{renderer.instances_per_world}|{outputs}")
 
 
+def _apply(renderer, shape: dict) -> None:
+    if shape["kernel"] == 3:
+        renderer.set_tuning(kernel=3, threads_per_block=shape["threads"], registers=shape["registers"])
+    else:
+        renderer.set_tuning(kernel=shape["kernel"], threads_per_block=shape["threads"], refill_lanes=shape["refill"],
+                            registers=shape["registers"], leaf_batch=shape["leaf_batch"])
+
+
 def _load() -> dict:
     try:
         with open(cache_path()) as f:
@@ -42,20 +54,21 @@ def _load() -> dict:
 def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, object_ids=False, repeats=3,
          use_cache=True, budget_s=60.0) -> dict:
     """Times every candidate shape on this renderer and these cameras (device tensors), sets the fastest and
-    returns {"threads", "registers", "refill", "leaf_batch", "ms", "timings"}."""
+    returns {"kernel", "threads", "registers", "refill", "leaf_batch", "ms", "timings"}."""
     import torch
     outputs = dict(rgb=rgb, depth=depth, normals=normals, object_ids=object_ids)
-    key = _key(renderer, tuple(sorted(k for k, v in outputs.items() if v)))
+    kernel = 3 if renderer.instances_per_world <= TILE_MAX_INSTANCES else 2
+    key = _key(renderer, tuple(sorted(k for k, v in outputs.items() if v))) + f"|kernel{kernel}"
     cache = _load() if use_cache else {}
     if key in cache:
         best = cache[key]
-        renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
-                            registers=best["registers"], leaf_batch=best["leaf_batch"])
+        _apply(renderer, best)
         return dict(best, cached=True)
     timings = []
     start = time.perf_counter()
-    for threads, regs, refill, batch in CANDIDATES:
-        renderer.set_tuning(kernel=2, threads_per_block=threads, refill_lanes=refill, registers=regs, leaf_batch=batch)
+    for threads, regs, refill, batch in (TILE_CANDIDATES if kernel == 3 else CANDIDATES):
+        _apply(renderer, {"kernel": kernel, "threads": threads, "refill": refill, "registers": regs,
+                          "leaf_batch": batch})
         renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -64,16 +77,15 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
             renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         e1.record()
         e1.synchronize()
-        timings.append({"threads": threads, "registers": regs, "refill": refill, "leaf_batch": batch,
-                        "ms": e0.elapsed_time(e1) / repeats})
+        timings.append({"kernel": kernel, "threads": threads, "registers": regs, "refill": refill,
+                        "leaf_batch": batch, "ms": e0.elapsed_time(e1) / repeats})
         if time.perf_counter() - start > budget_s:
             break
     best = min(timings, key=lambda t: t["ms"])
-    renderer.set_tuning(kernel=0, threads_per_block=best["threads"], refill_lanes=best["refill"],
-                        registers=best["registers"], leaf_batch=best["leaf_batch"])
+    _apply(renderer, best)
     result = dict(best, timings=timings)
     if use_cache:
-        cache[key] = {k: best[k] for k in ("threads", "registers", "refill", "leaf_batch", "ms")}
+        cache[key] = {k: best[k] for k in ("kernel", "threads", "registers", "refill", "leaf_batch", "ms")}
         try:
             os.makedirs(os.path.dirname(cache_path()), exist_ok=True)
             with open(cache_path(), "w") as f:

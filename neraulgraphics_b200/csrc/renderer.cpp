@@ -109,8 +109,9 @@ struct Renderer {
     DevBuf<float4> camera_basis;              // the persistent render's per-view cameras
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
-    int kernel_choice = 0;                    // 0: automatic, 1: the per-pixel kernel, 2: the persistent kernel
+    int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
     PersistentTuning tuning{128, 28, 72, 16};
+    PersistentTuning tile_tuning{128, 0, 64, 0};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -502,12 +503,17 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
         a.hit_v = hit_v.ensure(pixels());
     }
     a.error_flag = error_flag.p;
-    // The persistent kernel covers one sample per pixel, at most one light and no bounces; everything else
-    // takes the per-pixel kernel, which runs trace in full.
+    // The persistent and tile kernels cover one sample per pixel, at most one light and no bounces, the tile
+    // kernel for worlds of at most TILE_MAX_INSTANCES instances; everything else takes the per-pixel kernel,
+    // which runs trace in full.
     const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
-    const bool persistent = kernel_choice == 2 ? persistent_ok : (kernel_choice == 0 && persistent_ok);
+    const bool tiles_ok = persistent_ok && (params.instance_count == 0 || params.per_world <= TILE_MAX_INSTANCES);
+    const bool tiles = tiles_ok && (kernel_choice == 0 || kernel_choice == 3);
+    const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
     CK(cudaEventRecord(ev_start, stream));
-    if (persistent) {
+    if (tiles) {
+        CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream));
+    } else if (persistent) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
         CK(launch_render_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
     } else {
@@ -823,7 +829,17 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
 int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes,
     int32_t registers, int32_t leaf_batch) {
     return guarded(h, [&](ngb::Renderer &r) {
-        ngb::require(kernel >= 0 && kernel <= 2, "kernel must be 0 (automatic), 1 (per pixel) or 2 (persistent)");
+        ngb::require(kernel >= 0 && kernel <= 3,
+            "kernel must be 0 (automatic), 1 (per pixel), 2 (persistent) or 3 (tiles)");
+        if (kernel == 3) {
+            const bool built = (threads_per_block == 128 && (registers == 64 || registers == 80 || registers == 96)) ||
+                (threads_per_block == 256 && (registers == 64 || registers == 80));
+            ngb::require(built, "for the tile kernel, threads_per_block and registers must be one of 128/64, 128/80, "
+                "128/96, 256/64, 256/80");
+            r.kernel_choice = kernel;
+            r.tile_tuning = ngb::PersistentTuning{threads_per_block, 0, registers, 0};
+            return;
+        }
         const bool built = (threads_per_block == 128 && (registers == 48 || registers == 64 || registers == 72)) ||
             (threads_per_block == 256 && (registers == 48 || registers == 64)) || (threads_per_block == 64 && registers == 64);
         ngb::require(built, "threads_per_block and registers must be one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64");

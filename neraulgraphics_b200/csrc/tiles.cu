@@ -1,0 +1,518 @@
+// The tile render kernel: the batched path's common case (one sample per pixel, at most one light, no mirror
+// bounces) for worlds of at most 32 instances, which is what a batch of small simulator worlds holds.
+//
+// One warp renders an 8 x 4 pixel tile of one view. All 32 rays of a tile start at the same eye and point into
+// the same narrow pyramid, and a small world has at most one instance per lane, so the warp replaces the world
+// tree's walk by one conservative test per instance:
+//   - lane j tests instance j's world box against the tile's pyramid (four planes through the eye, widened by
+//     a margin far above rounding) and against the eye's distance; the ballot is the tile's candidate list,
+//     sorted by the distance below which no ray of the tile can enter the box;
+//   - every lane then visits the candidates in that order, the same instance at the same time across the warp,
+//     so the mesh walks of neighbouring rays run together over the same nodes; a lane enters a candidate only
+//     if its own ray passes the slab test of the instance's box (the test the world tree applies to that leaf),
+//     with its closest hit so far as the limit, exactly as the world tree's walk does;
+//   - the shadow rays of the tile go from the lit points to the light's sphere; the candidates for them are
+//     the instances whose boxes meet the convex hull of those segments, tested on the coordinate axes and on
+//     four axes tilted towards the light (separating axes of the hull).
+// Why the hits are the reference's: a ray's slab test on a box inside a parent box never passes where the
+// parent's fails (the subtraction, the product and min/max are monotone in correctly rounded arithmetic), so
+// the world tree reaches an instance's leaf exactly when the ray passes the leaf's own box test; the walk
+// inside a mesh is the reference's, order and all (src/mesh_dev.h:113-159). What can change is only the order
+// in which instances are visited, and with it which of two hits within rounding of each other is kept, the
+// near-ties the parity tests name. A shadow ray's any-hit answer does not depend on the order at all.
+#include <climits>
+
+#include "kernels.h"
+#include "trace_common.cuh"
+
+namespace ngb {
+namespace {
+
+using namespace tr;
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int TILE_W = 8, TILE_H = 4;
+constexpr int WALK_STACK = 64;      // a mesh's tree is at most 60 deep
+constexpr int TILES_PER_FETCH = 4;  // tiles a warp takes with one atomic
+
+// A world instance as a warp holds it while it renders a tile: its world box, the instance, and the distance
+// below which no camera ray of the tile can enter the box.
+struct TileBox {
+    float4 lo;  // xyz, w: instance (int bits)
+    float4 hi;  // xyz, w: entry bound
+};
+
+struct WarpSmem {
+    TileBox box[TILE_MAX_INSTANCES];
+    int order[TILE_MAX_INSTANCES];  // the camera rays' candidates, smallest entry bound first
+};
+
+// An instance's leaf as the world tree's walk handles it once the ray has passed the leaf's box: the ray
+// moved to mesh space and the mesh root's box test (blas_walk, src/mesh_dev.h:164-175), then the mesh's tree
+// from its child-pair records: the nearer child first (dl <= dr), the farther one pushed with its entry
+// distance and dropped at pop time once a hit is closer (traverse, src/mesh_dev.h:113-159), and a leaf's
+// triangles in order (mesh_intersect / mesh_occluded, src/mesh_dev.h:180-226).
+// any: true at the first hit closer than tmax. Otherwise: lowers tmax to each closer hit and records it, true
+// if there was one. Not inlined, so that the picture, centre and shadow rays share one copy of the walk (the
+// instruction cache holds it once) and its stack lives in this function's own frame.
+__device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, const float *__restrict__ slot_bounds,
+    const int2 *__restrict__ slot_root, const float4 *__restrict__ pairs, const float4 *__restrict__ tris, int id,
+    float3 o, float3 d, float &tmax, bool any, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
+    const float4 *rec = inst + 4 * static_cast<long long>(id);
+    InstanceRec r;
+    r.r0 = __ldg(rec);
+    r.r1 = __ldg(rec + 1);
+    r.r2 = __ldg(rec + 2);
+    const int slot = __float_as_int(__ldg(rec + 3).y);
+    o = to_local_point(r, o);
+    d = to_local_dir(r, d);
+    const float3 inv = safe_inverse(d);
+    const float *b = slot_bounds + 6 * slot;
+    const float4 blo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), 0.0f);
+    const float4 bhi = make_float4(__ldg(b + 3), __ldg(b + 4), __ldg(b + 5), 0.0f);
+    if (box_entry(blo, bhi, o, inv, tmax) >= NO_HIT) return false;
+    const int2 root = __ldg(slot_root + slot);
+    int ref = root.x, count = root.y;
+    int st_ref[WALK_STACK], st_cnt[WALK_STACK];
+    float st_t[WALK_STACK];
+    bool found = false;
+    int sp = 0;
+    for (int steps = 0;; ++steps) {
+        if (steps > max_steps) {  // a correct walk visits each node once; only a malformed tree gets here
+            *err = 2;
+            return found;
+        }
+        if (count == 0) {
+            const float4 *q = pairs + 4 * static_cast<long long>(ref);
+            const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+            const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o, inv,
+                tmax);
+            const float dr = box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), o, inv,
+                tmax);
+            if (dl < NO_HIT || dr < NO_HIT) {
+                const bool left_first = dl <= dr;
+                const float far_t = left_first ? dr : dl;
+                if (far_t < NO_HIT) {
+                    if (sp >= WALK_STACK) {
+                        *err = 1;
+                        return found;
+                    }
+                    st_ref[sp] = __float_as_int(left_first ? q3.z : q3.x);
+                    st_cnt[sp] = __float_as_int(left_first ? q3.w : q3.y);
+                    st_t[sp] = far_t;
+                    ++sp;
+                }
+                ref = __float_as_int(left_first ? q3.x : q3.z);
+                count = __float_as_int(left_first ? q3.y : q3.w);
+                continue;
+            }
+        } else {
+            for (int j = ref; j < ref + count; ++j) {
+                float t, bu, bv;
+                if (triangle_hit(tris, j, o, d, tmax, t, bu, bv)) {
+                    if (any) return true;
+                    tmax = t;
+                    hit_tri = j;
+                    hu = bu;
+                    hv = bv;
+                    found = true;
+                }
+            }
+        }
+        while (sp > 0 && st_t[sp - 1] >= tmax) --sp;
+        if (sp == 0) return found;
+        --sp;
+        ref = st_ref[sp];
+        count = st_cnt[sp];
+    }
+}
+
+// A camera ray's closest mesh hit over the tile's candidates, visited by the whole warp in the same order.
+// The warp stops once no lane's closest hit lies beyond the next candidate's entry bound.
+__device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpSmem &sm, int ncand, bool active,
+    float3 o, float3 d, float &tmax, int &hit_inst, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
+    const float3 inv = safe_inverse(d);
+    for (int c = 0; c < ncand; ++c) {
+        const TileBox b = sm.box[sm.order[c]];
+        const bool reach = active && b.hi.w < tmax;
+        if (!__any_sync(FULL, reach)) break;
+        if (reach && box_entry(b.lo, b.hi, o, inv, tmax) < NO_HIT) {
+            const int id = __float_as_int(b.lo.w);
+            if (instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, false, hit_tri,
+                    hu, hv, max_steps, err))
+                hit_inst = id;
+        }
+    }
+}
+
+// Spheres and the floor before the meshes, the meshes with the closest of those as their limit
+// (scene_intersect, src/render_core.h:78-112).
+__device__ __forceinline__ float spheres_and_floor(const SceneParams &s, float3 o, float3 d, int &best_sphere,
+    bool &hit_floor) {
+    float best = 1e30f;
+    best_sphere = -1;
+    for (int i = 0; i < s.sphere_count; ++i) {
+        float t;
+        if (sphere_hit(s.spheres[i], o, d, t) && t < best) {
+            best = t;
+            best_sphere = i;
+        }
+    }
+    hit_floor = false;
+    float dd;
+    if (floor_hit(s.floor, o, d, best, dd)) {
+        best = dd;
+        hit_floor = true;
+    }
+    return best;
+}
+
+// The surface of a closest hit, as scene_intersect resolves it (src/render_core.h:116-141).
+__device__ __forceinline__ void resolve(const SceneParams &s, int world, float3 point, float3 d, int hit_inst,
+    int hit_tri, float hu, float hv, int best_sphere, bool hit_floor, float3 &normal, DevMaterial &mat, int &object) {
+    if (hit_inst >= 0) {
+        normal = mesh_surface(s, hit_inst, hit_tri, hu, hv, d);
+        const int slot = hit_inst - world * s.per_world;
+        mat = s.slot_material[slot];
+        object = OBJECT_INSTANCE + slot;
+    } else if (hit_floor) {
+        object = OBJECT_FLOOR;
+        normal = mk3(0.0f, 1.0f, 0.0f);
+        mat = s.floor.m;
+        const int cx = static_cast<int>(floorf(point.x * s.floor.checker));
+        const int cz = static_cast<int>(floorf(point.z * s.floor.checker));
+        const float3 tint = ((cx + cz) & 1) ? mk3(1.0f, 1.0f, 1.0f) : mk3(1.0f, 0.7f, 0.3f);
+        mat.diffuse_color = tint * 0.3f;
+    } else {
+        normal = normalize(point - s.spheres[best_sphere].center);
+        mat = s.spheres[best_sphere].m;
+        object = OBJECT_SPHERE + best_sphere;
+    }
+}
+
+// sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283), packed r | g << 8 | b << 16.
+// Not inlined: one copy serves every colour the kernel writes.
+__device__ __noinline__ int rgb_bytes(const float *table, float3 radiance) {
+    float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
+    sum = sum * (1.0f / 1.0f);
+    return srgb_byte(table, sum.x) | (srgb_byte(table, sum.y) << 8) | (srgb_byte(table, sum.z) << 16);
+}
+
+__device__ __forceinline__ void put_rgb(uint8_t *rgb, long long pix, int bytes) {
+    uint8_t *o = rgb + 3 * static_cast<size_t>(pix);
+    o[0] = static_cast<uint8_t>(bytes);
+    o[1] = static_cast<uint8_t>(bytes >> 8);
+    o[2] = static_cast<uint8_t>(bytes >> 16);
+}
+
+__device__ __forceinline__ float warp_max(float v) { return from_ordered(__reduce_max_sync(FULL, to_ordered(v))); }
+__device__ __forceinline__ float warp_min(float v) { return from_ordered(__reduce_min_sync(FULL, to_ordered(v))); }
+__device__ __forceinline__ float abs_dot(float3 n, float3 h) { return fabsf(n.x) * h.x + fabsf(n.y) * h.y + fabsf(n.z) * h.z; }
+
+// THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget, as for the persistent kernel.
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const __grid_constant__ SceneParams s,
+    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
+    __shared__ WarpSmem warp_smem[THREADS / 32];
+    WarpSmem &sm = warp_smem[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int P = s.instance_count > 0 ? s.per_world : 0;
+    const long long first_leaf = s.tlas_internal;  // leaf k of the sorted leaves is node n - 1 + k
+    const int max_steps = s.blas_node_count + 2;
+    const bool want_aov = a.depth || a.normal || a.object_id || a.hit_instance;
+    const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
+    const float fs = a.fov_scale, asp = a.aspect;
+    for (;;) {
+        long long first = 0;
+        if (lane == 0)
+            first = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long *>(counter),
+                static_cast<unsigned long long>(TILES_PER_FETCH)));
+        first = __shfl_sync(FULL, first, 0);
+        if (first >= tiles) break;
+        const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
+        for (long long tile = first; tile < last; ++tile) {
+            const int view = static_cast<int>(tile / tiles_per_view);
+            const int q = static_cast<int>(tile % tiles_per_view);
+            const int x0 = (q % tiles_x) * TILE_W, y0 = (q / tiles_x) * TILE_H;
+            const int x = x0 + (lane % TILE_W), y = y0 + lane / TILE_W;
+            const bool pixel = x < a.width && y < a.height;
+            const int world = view / a.cameras_per_world;
+            const long long pix = (static_cast<long long>(view) * a.height + y) * a.width + x;
+
+            // The view's camera (camera_from_matrix, src/render_core.h:264-273).
+            const float *cm = a.cameras + 12LL * view;
+            const float3 eye = mk3(__ldg(cm + 3), __ldg(cm + 7), __ldg(cm + 11));
+            const float3 right = normalize(mk3(__ldg(cm), __ldg(cm + 4), __ldg(cm + 8)));
+            const float3 up = normalize(mk3(__ldg(cm + 1), __ldg(cm + 5), __ldg(cm + 9)));
+            const float3 fwd = normalize(mk3(-__ldg(cm + 2), -__ldg(cm + 6), -__ldg(cm + 10)));
+
+            // The tile's pyramid: the tangent-plane offsets of its pixel edges (every jittered and centre ray of
+            // the tile lies inside), widened by 1e-3, and the four side planes through the eye, facing inwards.
+            float sxa = (2.0f * static_cast<float>(x0) / fw - 1.0f) * fs * asp;
+            float sxb = (2.0f * static_cast<float>(x0 + TILE_W) / fw - 1.0f) * fs * asp;
+            float sya = -(2.0f * static_cast<float>(y0) / fh - 1.0f) * fs;
+            float syb = -(2.0f * static_cast<float>(y0 + TILE_H) / fh - 1.0f) * fs;
+            const float sx_lo = fminf(sxa, sxb) - 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
+            const float sx_hi = fmaxf(sxa, sxb) + 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
+            const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
+            const float sy_hi = fmaxf(sya, syb) + 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
+
+            __syncwarp();
+            bool cand = false;
+            float bound = 0.0f;
+            if (lane < P) {
+                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(world) * P + lane);
+                const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
+                const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+                const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
+                const float3 rel = c - eye;
+                const float pad = 1e-4f * (fabsf(rel.x) + fabsf(rel.y) + fabsf(rel.z) + h.x + h.y + h.z) + 1e-4f;
+                const float3 k00 = right * sx_lo + up * sy_lo + fwd, k10 = right * sx_hi + up * sy_lo + fwd;
+                const float3 k11 = right * sx_hi + up * sy_hi + fwd, k01 = right * sx_lo + up * sy_hi + fwd;
+                const float3 mid = k00 + k11;
+                const float3 edges[4][2] = {{k00, k10}, {k10, k11}, {k11, k01}, {k01, k00}};
+                cand = true;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    float3 n = cross(edges[e][0], edges[e][1]);
+                    if (dot(n, mid) < 0.0f) n = -n;
+                    const float reach = dot(n, rel) + abs_dot(n, h) + pad * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
+                    if (reach < 0.0f) cand = false;
+                }
+                // No ray of the tile can enter the box closer than the eye's distance to it (the rays are unit
+                // length); the bound sits 1e-5 below that, far beyond the slab test's rounding.
+                const float dx = fmaxf(fmaxf(lo.x - eye.x, eye.x - hi.x), 0.0f);
+                const float dy = fmaxf(fmaxf(lo.y - eye.y, eye.y - hi.y), 0.0f);
+                const float dz = fmaxf(fmaxf(lo.z - eye.z, eye.z - hi.z), 0.0f);
+                bound = sqrtf(dx * dx + dy * dy + dz * dz) * 0.99999f;
+                sm.box[lane].lo = make_float4(lo.x, lo.y, lo.z, __int_as_float(~__float_as_int(lo.w)));
+                sm.box[lane].hi = make_float4(hi.x, hi.y, hi.z, bound);
+            }
+            const unsigned cmask = __ballot_sync(FULL, cand);
+            int rank = 0;
+            for (unsigned m = cmask; m != 0; m &= m - 1) {
+                const int k = __ffs(m) - 1;
+                const float bk = __shfl_sync(FULL, bound, k);
+                rank += (bk < bound) || (bk == bound && k < lane);
+            }
+            if (cand) sm.order[rank] = lane;
+            const int ncand = __popc(cmask);
+            __syncwarp();
+
+            // The camera rays, each pass through the same code: the centre ray for depth, normals and IDs
+            // (aov_pixel, src/render_core.h:313-327), then the jittered picture ray, one bounce, one light
+            // (trace, src/render_core.h:202-245), whose lit hits leave a shadow ray for the pass after.
+            bool pending = false;
+            float3 so = mk3(0.0f, 0.0f, 0.0f), sd = mk3(0.0f, 0.0f, 1.0f);
+            float sdist = 0.0f;
+            int lit_bytes = 0, shadow_bytes = 0;
+            const int last_pass = a.rgb ? 1 : 0;
+            for (int pass = want_aov ? 0 : 1; pass <= last_pass; ++pass) {
+                float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f;
+                uint32_t rng = 0;
+                if (pass == 1) {
+                    rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
+                    const float jx = rand_float(rng);
+                    const float jy = rand_float(rng);
+                    px = static_cast<float>(x) + jx;
+                    py = static_cast<float>(y) + jy;
+                }
+                const float3 d = camera_dir(right, up, fwd, px, py, fw, fh, fs, asp);
+                int best_sphere;
+                bool hit_floor;
+                float tmax = spheres_and_floor(s, eye, d, best_sphere, hit_floor);
+                int hit_inst = -1, hit_tri = -1;
+                float hu = 0.0f, hv = 0.0f;
+                closest_meshes(s, sm, ncand, pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps, a.error_flag);
+                if (!pixel) continue;
+                const bool mesh = hit_inst >= 0;
+                const bool found = mesh || best_sphere >= 0 || hit_floor;
+                float3 normal = mk3(0.0f, 0.0f, 0.0f);
+                DevMaterial mat{};
+                int object = OBJECT_NONE;
+                const float3 point = eye + d * tmax;
+                if (found) resolve(s, world, point, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal, mat, object);
+                const size_t p = static_cast<size_t>(pix);
+                if (pass == 0) {
+                    if (a.depth) a.depth[p] = found ? tmax * dot(d, fwd) : __int_as_float(0x7f800000);
+                    if (a.normal) {
+                        a.normal[3 * p] = normal.x;
+                        a.normal[3 * p + 1] = normal.y;
+                        a.normal[3 * p + 2] = normal.z;
+                    }
+                    if (a.object_id) a.object_id[p] = object;
+                    if (a.hit_instance) {
+                        a.hit_instance[p] = mesh ? hit_inst : -1;
+                        a.hit_triangle[p] = mesh ? __ldg(s.tri_index + hit_tri) : -1;
+                        a.hit_u[p] = mesh ? hu : 0.0f;
+                        a.hit_v[p] = mesh ? hv : 0.0f;
+                    }
+                    continue;
+                }
+                const float3 zero = mk3(0.0f, 0.0f, 0.0f);
+                float3 radiance;
+                if (!found) {
+                    const float t = saturate(dot(d, s.env_up) * 0.5f + 0.5f);
+                    const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
+                    radiance = zero + sky * 1.0f;
+                } else {
+                    radiance = radiance_of(mat, s.ambient, zero, zero);
+                    if (s.light_count == 1) {
+                        const DevLight &lt = s.lights[0];
+                        const float z = 1.0f - 2.0f * rand_float(rng);
+                        const float rad = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+                        const float phi = 6.28318530718f * rand_float(rng);
+                        float sin_phi, cos_phi;
+                        sincosf(phi, &sin_phi, &cos_phi);
+                        const float3 lp = lt.position + mk3(rad * cos_phi, rad * sin_phi, z) * lt.radius;
+                        const float3 to_light = lp - point;
+                        const float light_distance = sqrtf(dot(to_light, to_light));
+                        const float3 light_dir = to_light * (1.0f / light_distance);
+                        const float strength = lt.intensity * light_factor(lt, light_dir, light_distance);
+                        if (strength > 0.0f) {
+                            // The shadow ray: spheres and the floor first (scene_occluded, src/render_core.h:146-161).
+                            so = offset_origin(point, normal, light_dir);
+                            sd = light_dir;
+                            sdist = light_distance;
+                            bool blocked = false;
+                            for (int i = 0; i < s.sphere_count && !blocked; ++i) {
+                                float t;
+                                if (sphere_hit(s.spheres[i], so, sd, t) && t < sdist) blocked = true;
+                            }
+                            if (!blocked) {
+                                float dd;
+                                blocked = floor_hit(s.floor, so, sd, sdist, dd);
+                            }
+                            if (!blocked) {
+                                const float3 lit = lt.color * strength;
+                                const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
+                                const float3 specular =
+                                    zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), d)), mat.exponent);
+                                shadow_bytes = rgb_bytes(s.srgb_table, radiance);
+                                radiance = radiance_of(mat, s.ambient, diffuse, specular);
+                                pending = true;
+                            }
+                        }
+                    }
+                }
+                const int bytes = rgb_bytes(s.srgb_table, radiance);
+                if (pending) lit_bytes = bytes;
+                else put_rgb(a.rgb, pix, bytes);
+            }
+            if (!a.rgb) continue;
+
+            // The tile's shadow rays: the candidates are the instances whose boxes meet the convex hull of the
+            // segments from the shadow origins to their ends at the light. Separating axes: x, y and z, the
+            // direction away from the light, and four axes tilted from the sideways directions towards the
+            // light by the light sphere's angular radius, which hug the hull's sides. Each support is taken over
+            // the segments' own end points, so any axis is a valid test; these make it a tight one.
+            const unsigned shadow_lanes = __ballot_sync(FULL, pending);
+            if (shadow_lanes == 0) continue;
+            const DevLight &lt = s.lights[0];
+            const float3 se = so + sd * sdist;
+            const float INF = __int_as_float(0x7f800000);
+            const float mnx = warp_min(pending ? fminf(so.x, se.x) : INF);
+            const float mny = warp_min(pending ? fminf(so.y, se.y) : INF);
+            const float mnz = warp_min(pending ? fminf(so.z, se.z) : INF);
+            const float mxx = warp_max(pending ? fmaxf(so.x, se.x) : -INF);
+            const float mxy = warp_max(pending ? fmaxf(so.y, se.y) : -INF);
+            const float mxz = warp_max(pending ? fmaxf(so.z, se.z) : -INF);
+            const int leader = __ffs(shadow_lanes) - 1;
+            const float3 pl = mk3(__shfl_sync(FULL, so.x, leader), __shfl_sync(FULL, so.y, leader),
+                __shfl_sync(FULL, so.z, leader));
+            float3 ell = lt.position - pl;
+            const float ell_len = sqrtf(dot(ell, ell));
+            constexpr int AXES = 5;
+            float3 axis[AXES];
+            float support[AXES];
+            int axes = 0;
+            if (ell_len > 1e-3f) {
+                ell = ell * (1.0f / ell_len);
+                const float kappa = lt.radius / ell_len;
+                const float3 side = fabsf(ell.x) < 0.9f ? mk3(1.0f, 0.0f, 0.0f) : mk3(0.0f, 1.0f, 0.0f);
+                const float3 u = normalize(cross(ell, side));
+                const float3 v = cross(ell, u);
+                axis[0] = u - ell * kappa;
+                axis[1] = -u - ell * kappa;
+                axis[2] = v - ell * kappa;
+                axis[3] = -v - ell * kappa;
+                axis[4] = -ell;
+                axes = AXES;
+#pragma unroll
+                for (int k = 0; k < AXES; ++k)
+                    support[k] = warp_max(pending ? fmaxf(dot(axis[k], so), dot(axis[k], se)) : -INF);
+            }
+            bool scand = false;
+            if (lane < P) {
+                const TileBox b = sm.box[lane];
+                const float3 c = mk3(0.5f * (b.lo.x + b.hi.x), 0.5f * (b.lo.y + b.hi.y), 0.5f * (b.lo.z + b.hi.z));
+                const float3 h = mk3(0.5f * (b.hi.x - b.lo.x), 0.5f * (b.hi.y - b.lo.y), 0.5f * (b.hi.z - b.lo.z));
+                const float scale = fabsf(lt.position.x) + fabsf(lt.position.y) + fabsf(lt.position.z) + lt.radius +
+                    fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + h.x + h.y + h.z + 1.0f;
+                const float pad = 1e-4f * scale;
+                scand = b.hi.x >= mnx - pad && b.lo.x <= mxx + pad && b.hi.y >= mny - pad && b.lo.y <= mxy + pad &&
+                    b.hi.z >= mnz - pad && b.lo.z <= mxz + pad;
+#pragma unroll
+                for (int k = 0; k < AXES; ++k) {
+                    if (k < axes && dot(axis[k], c) - abs_dot(axis[k], h) >
+                            support[k] + pad * (fabsf(axis[k].x) + fabsf(axis[k].y) + fabsf(axis[k].z)))
+                        scand = false;
+                }
+            }
+            bool blocked = false;
+            const float3 sinv = safe_inverse(sd);
+            for (unsigned m = __ballot_sync(FULL, scand); m != 0; m &= m - 1) {
+                const bool open = pending && !blocked;
+                if (!__any_sync(FULL, open)) break;
+                const TileBox b = sm.box[__ffs(m) - 1];
+                if (open && box_entry(b.lo, b.hi, so, sinv, sdist) < NO_HIT) {
+                    float tm = sdist, hu, hv;
+                    int ht;
+                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris,
+                        __float_as_int(b.lo.w), so, sd, tm, true, ht, hu, hv, max_steps, a.error_flag);
+                }
+            }
+            if (pending) put_rgb(a.rgb, pix, blocked ? shadow_bytes : lit_bytes);
+        }
+    }
+}
+
+template <int THREADS, int MIN_BLOCKS>
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream) {
+    const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
+    const int tiles_per_view = tiles_x * tiles_y;
+    const long long tiles = static_cast<long long>(tiles_per_view) * a.views;
+    const bool aov = a.depth || a.normal || a.object_id || a.hit_instance;
+    if (tiles == 0 || (!a.rgb && !aov)) return cudaSuccess;
+    auto kernel = render_tiles_kernel<THREADS, MIN_BLOCKS>;
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    // Every SM full of resident warps, and no more warps than there are fetches of tiles.
+    long long blocks = static_cast<long long>(sms) * per_sm;
+    const long long needed = (tiles + TILES_PER_FETCH * (THREADS / 32) - 1) / (TILES_PER_FETCH * (THREADS / 32));
+    if (blocks > needed) blocks = needed;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    kernel<<<static_cast<unsigned>(blocks), THREADS, 0, stream>>>(s, a, counter, tiles, tiles_x, tiles_per_view);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
+    cudaStream_t stream) {
+    if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) return cudaErrorInvalidValue;
+    // (threads per CTA, register budget) -> the instantiation with that budget.
+    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, stream);
+    if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6>(s, a, counter, stream);
+    if (t.threads == 128 && t.registers == 96) return launch_variant<128, 5>(s, a, counter, stream);
+    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, stream);
+    if (t.threads == 256 && t.registers == 80) return launch_variant<256, 3>(s, a, counter, stream);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace ngb

@@ -400,6 +400,32 @@ __device__ __forceinline__ uint8_t srgb_byte(const float *table, float v) {
 }
 
 
+// The camera ray through image point (px, py) (camera_ray, src/device_scene.h:114-119): the tangent-plane offsets, then the
+// direction normalised.
+__device__ __forceinline__ float3 camera_dir(float3 right, float3 up, float3 fwd, float px, float py, float fw, float fh,
+    float fov_scale, float aspect) {
+    const float sx = (2.0f * px / fw - 1.0f) * fov_scale * aspect;
+    const float sy = -(2.0f * py / fh - 1.0f) * fov_scale;
+    return normalize(right * sx + up * sy + fwd);
+}
+
+// The radiance of a hit with these light sums, as trace computes it for a path of one bounce
+// (src/render_core.h:234-236, radiance and throughput starting at 0 and 1).
+__device__ __forceinline__ float3 radiance_of(const DevMaterial &m, float ambient, float3 diffuse, float3 specular) {
+    const float3 direct = m.diffuse_color * (diffuse * m.kd) + specular * m.ks;
+    return mk3(0.0f, 0.0f, 0.0f) + (direct + m.diffuse_color * (ambient * m.kd)) * 1.0f;
+}
+
+// sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283).
+__device__ __forceinline__ void write_rgb(const float *table, uint8_t *rgb, long long pix, float3 radiance) {
+    float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
+    sum = sum * (1.0f / 1.0f);
+    uint8_t *o = rgb + 3 * static_cast<size_t>(pix);
+    o[0] = srgb_byte(table, sum.x);
+    o[1] = srgb_byte(table, sum.y);
+    o[2] = srgb_byte(table, sum.z);
+}
+
 }  // namespace
 }  // namespace tr
 }  // namespace ngb
