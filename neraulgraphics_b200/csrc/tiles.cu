@@ -76,13 +76,16 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
     int st_ref[WALK_STACK], st_cnt[WALK_STACK];
     float st_t[WALK_STACK];
     bool found = false;
-    int sp = 0;
-    for (int steps = 0;; ++steps) {
-        if (steps > max_steps) {  // a correct walk visits each node once; only a malformed tree gets here
-            *err = 2;
-            return found;
-        }
-        if (count == 0) {
+    int sp = 0, steps = 0;
+    // While-while: a lane walks internal nodes until it stands at a leaf (or its walk ends), and the leaf's
+    // triangles are tested once the warp's lanes have all come out of the inner loop, so the two kinds of
+    // step run with their own lanes together instead of every iteration paying for both.
+    for (;;) {
+        while (count == 0) {
+            if (++steps > max_steps) {  // a correct walk visits each node once; only a malformed tree gets here
+                *err = 2;
+                return found;
+            }
             const float4 *q = pairs + 4 * static_cast<long long>(ref);
             const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
             const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o, inv,
@@ -104,19 +107,27 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
                 }
                 ref = __float_as_int(left_first ? q3.x : q3.z);
                 count = __float_as_int(left_first ? q3.y : q3.w);
-                continue;
+            } else {
+                while (sp > 0 && st_t[sp - 1] >= tmax) --sp;
+                if (sp == 0) return found;
+                --sp;
+                ref = st_ref[sp];
+                count = st_cnt[sp];
             }
-        } else {
-            for (int j = ref; j < ref + count; ++j) {
-                float t, bu, bv;
-                if (triangle_hit(tris, j, o, d, tmax, t, bu, bv)) {
-                    if (any) return true;
-                    tmax = t;
-                    hit_tri = j;
-                    hu = bu;
-                    hv = bv;
-                    found = true;
-                }
+        }
+        if (++steps > max_steps) {
+            *err = 2;
+            return found;
+        }
+        for (int j = ref; j < ref + count; ++j) {
+            float t, bu, bv;
+            if (triangle_hit(tris, j, o, d, tmax, t, bu, bv)) {
+                if (any) return true;
+                tmax = t;
+                hit_tri = j;
+                hu = bu;
+                hv = bv;
+                found = true;
             }
         }
         while (sp > 0 && st_t[sp - 1] >= tmax) --sp;
