@@ -60,8 +60,17 @@ struct RenderArgs {
     float *hit_u;
     float *hit_v;
     int *error_flag;               // set nonzero if a traversal stack would overflow
-    float4 *camera_basis;          // views x 3: scratch for the persistent kernel's per-view camera
+    float4 *camera_basis;          // views x 3: scratch for the persistent and tile kernels' per-view camera
+    // Per-pixel scratch of the tile kernels, between the camera, shade and shadow kernels (see tiles.cu).
+    float4 *pic_hit;               // the picture ray's closest hit: t, u, v, triangle
+    int *pic_code;                 // its object code, then the shadowed pixel's bytes
+    float4 *shadow_o;              // the shadow ray's origin and length (0: no shadow ray)
+    float4 *shadow_d;              // its direction and the lit pixel's bytes
 };
+
+// The per-view camera basis of camera_from_matrix (src/render_core.h:264-273): (position.xyz, right.x)
+// (right.yz, up.xy) (up.z, forward.xyz) for each view.
+cudaError_t launch_prepare_cameras(const float *cameras, int views, float4 *basis, cudaStream_t stream);
 cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream);
 
 // Ray queries over the worlds of a batch: ray i belongs to world i / rays_per_world.

@@ -472,20 +472,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
     }
 }
 
-// One thread per view: the camera basis of camera_from_matrix (src/render_core.h:264-273), renormalised.
-__global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *cameras, int views, float4 *basis) {
-    const int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= views) return;
-    float m[12];
-    for (int k = 0; k < 12; ++k) m[k] = __ldg(cameras + 12 * static_cast<size_t>(v) + k);
-    const float3 right = normalize(mk3(m[0], m[4], m[8]));
-    const float3 up = normalize(mk3(m[1], m[5], m[9]));
-    const float3 fwd = normalize(mk3(-m[2], -m[6], -m[10]));
-    basis[3 * v] = make_float4(m[3], m[7], m[11], right.x);
-    basis[3 * v + 1] = make_float4(right.y, right.z, up.x, up.y);
-    basis[3 * v + 2] = make_float4(up.z, fwd.x, fwd.y, fwd.z);
-}
-
 template <int THREADS, int MIN_BLOCKS>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, int leaf_batch,
     cudaStream_t stream) {
@@ -508,7 +494,8 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    prepare_cameras_kernel<<<(a.views + 127) / 128, 128, 0, stream>>>(a.cameras, a.views, a.camera_basis);
+    e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+    if (e != cudaSuccess) return e;
     kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, counter, total, kinds, tiles_x, tiles_per_view,
         refill, leaf_batch);
     return cudaGetLastError();

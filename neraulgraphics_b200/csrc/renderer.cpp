@@ -106,7 +106,9 @@ struct Renderer {
     DevBuf<float4> blas_pairs, tlas_pairs;
     DevBuf<int2> slot_root;
     DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
-    DevBuf<float4> camera_basis;              // the persistent render's per-view cameras
+    DevBuf<float4> camera_basis;              // the persistent and tile renders' per-view cameras
+    DevBuf<float4> pic_hit, shadow_o, shadow_d;  // the tile render's per-pixel hand-over between its kernels
+    DevBuf<int> pic_code;
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
@@ -326,6 +328,7 @@ Renderer::~Renderer() {
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
+    pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release();
     camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
@@ -512,6 +515,13 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
     CK(cudaEventRecord(ev_start, stream));
     if (tiles) {
+        a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
+        if (a.rgb) {
+            a.pic_hit = pic_hit.ensure(pixels());
+            a.pic_code = pic_code.ensure(pixels());
+            a.shadow_o = shadow_o.ensure(pixels());
+            a.shadow_d = shadow_d.ensure(pixels());
+        }
         CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream));
     } else if (persistent) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));

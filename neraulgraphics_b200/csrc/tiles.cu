@@ -220,9 +220,56 @@ __device__ __forceinline__ float warp_max(float v) { return from_ordered(__reduc
 __device__ __forceinline__ float warp_min(float v) { return from_ordered(__reduce_min_sync(FULL, to_ordered(v))); }
 __device__ __forceinline__ float abs_dot(float3 n, float3 h) { return fabsf(n.x) * h.x + fabsf(n.y) * h.y + fabsf(n.z) * h.z; }
 
-// THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget, as for the persistent kernel.
+// The tile kernels' common start: which tile of which view, and the pixel of this lane.
+struct TileAt {
+    int view, world, x0, y0, x, y;
+    bool pixel;
+    long long pix;
+};
+
+__device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view, int lane) {
+    TileAt t;
+    t.view = static_cast<int>(tile / tiles_per_view);
+    const int q = static_cast<int>(tile % tiles_per_view);
+    t.x0 = (q % tiles_x) * TILE_W;
+    t.y0 = (q / tiles_x) * TILE_H;
+    t.x = t.x0 + (lane % TILE_W);
+    t.y = t.y0 + lane / TILE_W;
+    t.pixel = t.x < a.width && t.y < a.height;
+    t.world = t.view / a.cameras_per_world;
+    t.pix = (static_cast<long long>(t.view) * a.height + t.y) * a.width + t.x;
+    return t;
+}
+
+// A warp's next run of tiles, TILES_PER_FETCH of them from one atomic; first >= tiles when none are left.
+__device__ __forceinline__ long long fetch_tiles(int *counter, int lane) {
+    long long first = 0;
+    if (lane == 0)
+        first = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long *>(counter),
+            static_cast<unsigned long long>(TILES_PER_FETCH)));
+    return __shfl_sync(FULL, first, 0);
+}
+
+// The picture ray of pixel (x, y): its jitter draws from the pixel's random stream, which is left where the
+// light sample continues it (sample_pixel, src/render_core.h:248-258).
+__device__ __forceinline__ float3 picture_ray(const RenderArgs &a, int x, int y, float3 right, float3 up, float3 fwd,
+    uint32_t &rng) {
+    rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
+    const float jx = rand_float(rng);
+    const float jy = rand_float(rng);
+    return camera_dir(right, up, fwd, static_cast<float>(x) + jx, static_cast<float>(y) + jy,
+        static_cast<float>(a.width), static_cast<float>(a.height), a.fov_scale, a.aspect);
+}
+
+// The picture ray's closest hit as the camera kernel hands it to the shade kernel: the object code
+// (instance >= 0, else -1 nothing, -2 the floor, -3 - i sphere i).
+constexpr int CODE_NONE = -1, CODE_FLOOR = -2, CODE_SPHERE = -3;
+
+// Camera kernel. THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget. Per tile: the
+// candidates, then the centre rays (depth, normals, IDs written here) and the picture rays (their closest
+// hits written for the shade kernel).
 template <int THREADS, int MIN_BLOCKS>
-__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const __grid_constant__ SceneParams s,
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
     __shared__ WarpSmem warp_smem[THREADS / 32];
     WarpSmem &sm = warp_smem[threadIdx.x >> 5];
@@ -234,35 +281,23 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
     const float fs = a.fov_scale, asp = a.aspect;
     for (;;) {
-        long long first = 0;
-        if (lane == 0)
-            first = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long *>(counter),
-                static_cast<unsigned long long>(TILES_PER_FETCH)));
-        first = __shfl_sync(FULL, first, 0);
+        const long long first = fetch_tiles(counter, lane);
         if (first >= tiles) break;
         const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
         for (long long tile = first; tile < last; ++tile) {
-            const int view = static_cast<int>(tile / tiles_per_view);
-            const int q = static_cast<int>(tile % tiles_per_view);
-            const int x0 = (q % tiles_x) * TILE_W, y0 = (q / tiles_x) * TILE_H;
-            const int x = x0 + (lane % TILE_W), y = y0 + lane / TILE_W;
-            const bool pixel = x < a.width && y < a.height;
-            const int world = view / a.cameras_per_world;
-            const long long pix = (static_cast<long long>(view) * a.height + y) * a.width + x;
-
+            const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
             // The view's camera (camera_from_matrix, src/render_core.h:264-273).
-            const float *cm = a.cameras + 12LL * view;
-            const float3 eye = mk3(__ldg(cm + 3), __ldg(cm + 7), __ldg(cm + 11));
-            const float3 right = normalize(mk3(__ldg(cm), __ldg(cm + 4), __ldg(cm + 8)));
-            const float3 up = normalize(mk3(__ldg(cm + 1), __ldg(cm + 5), __ldg(cm + 9)));
-            const float3 fwd = normalize(mk3(-__ldg(cm + 2), -__ldg(cm + 6), -__ldg(cm + 10)));
+            const float4 c0 = __ldg(a.camera_basis + 3 * T.view), c1 = __ldg(a.camera_basis + 3 * T.view + 1);
+            const float4 c2 = __ldg(a.camera_basis + 3 * T.view + 2);
+            const float3 eye = mk3(c0.x, c0.y, c0.z), right = mk3(c0.w, c1.x, c1.y);
+            const float3 up = mk3(c1.z, c1.w, c2.x), fwd = mk3(c2.y, c2.z, c2.w);
 
             // The tile's pyramid: the tangent-plane offsets of its pixel edges (every jittered and centre ray of
             // the tile lies inside), widened by 1e-3, and the four side planes through the eye, facing inwards.
-            float sxa = (2.0f * static_cast<float>(x0) / fw - 1.0f) * fs * asp;
-            float sxb = (2.0f * static_cast<float>(x0 + TILE_W) / fw - 1.0f) * fs * asp;
-            float sya = -(2.0f * static_cast<float>(y0) / fh - 1.0f) * fs;
-            float syb = -(2.0f * static_cast<float>(y0 + TILE_H) / fh - 1.0f) * fs;
+            const float sxa = (2.0f * static_cast<float>(T.x0) / fw - 1.0f) * fs * asp;
+            const float sxb = (2.0f * static_cast<float>(T.x0 + TILE_W) / fw - 1.0f) * fs * asp;
+            const float sya = -(2.0f * static_cast<float>(T.y0) / fh - 1.0f) * fs;
+            const float syb = -(2.0f * static_cast<float>(T.y0 + TILE_H) / fh - 1.0f) * fs;
             const float sx_lo = fminf(sxa, sxb) - 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sx_hi = fmaxf(sxa, sxb) + 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
@@ -272,7 +307,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
             bool cand = false;
             float bound = 0.0f;
             if (lane < P) {
-                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(world) * P + lane);
+                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(T.world) * P + lane);
                 const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
                 const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
                 const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
@@ -310,118 +345,184 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
             const int ncand = __popc(cmask);
             __syncwarp();
 
-            // The camera rays, each pass through the same code: the centre ray for depth, normals and IDs
-            // (aov_pixel, src/render_core.h:313-327), then the jittered picture ray, one bounce, one light
-            // (trace, src/render_core.h:202-245), whose lit hits leave a shadow ray for the pass after.
-            bool pending = false;
-            float3 so = mk3(0.0f, 0.0f, 0.0f), sd = mk3(0.0f, 0.0f, 1.0f);
-            float sdist = 0.0f;
-            int lit_bytes = 0, shadow_bytes = 0;
+            // The centre ray for depth, normals and IDs (aov_pixel, src/render_core.h:313-327), then the picture
+            // ray (trace, src/render_core.h:202-245) up to its closest hit. Spheres and the floor first.
             const int last_pass = a.rgb ? 1 : 0;
             for (int pass = want_aov ? 0 : 1; pass <= last_pass; ++pass) {
-                float px = static_cast<float>(x) + 0.5f, py = static_cast<float>(y) + 0.5f;
-                uint32_t rng = 0;
-                if (pass == 1) {
-                    rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
-                    const float jx = rand_float(rng);
-                    const float jy = rand_float(rng);
-                    px = static_cast<float>(x) + jx;
-                    py = static_cast<float>(y) + jy;
+                float3 d;
+                if (pass == 0) {
+                    d = camera_dir(right, up, fwd, static_cast<float>(T.x) + 0.5f, static_cast<float>(T.y) + 0.5f, fw, fh,
+                        fs, asp);
+                } else {
+                    uint32_t rng;
+                    d = picture_ray(a, T.x, T.y, right, up, fwd, rng);
                 }
-                const float3 d = camera_dir(right, up, fwd, px, py, fw, fh, fs, asp);
                 int best_sphere;
                 bool hit_floor;
                 float tmax = spheres_and_floor(s, eye, d, best_sphere, hit_floor);
                 int hit_inst = -1, hit_tri = -1;
                 float hu = 0.0f, hv = 0.0f;
-                closest_meshes(s, sm, ncand, pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps, a.error_flag);
-                if (!pixel) continue;
+                closest_meshes(s, sm, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps, a.error_flag);
+                if (!T.pixel) continue;
+                const size_t p = static_cast<size_t>(T.pix);
+                if (pass == 1) {
+                    a.pic_hit[p] = make_float4(tmax, hu, hv, __int_as_float(hit_tri));
+                    a.pic_code[p] = hit_inst >= 0 ? hit_inst
+                        : hit_floor           ? CODE_FLOOR
+                        : best_sphere >= 0    ? CODE_SPHERE - best_sphere
+                                              : CODE_NONE;
+                    continue;
+                }
                 const bool mesh = hit_inst >= 0;
                 const bool found = mesh || best_sphere >= 0 || hit_floor;
                 float3 normal = mk3(0.0f, 0.0f, 0.0f);
                 DevMaterial mat{};
                 int object = OBJECT_NONE;
-                const float3 point = eye + d * tmax;
-                if (found) resolve(s, world, point, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal, mat, object);
-                const size_t p = static_cast<size_t>(pix);
-                if (pass == 0) {
-                    if (a.depth) a.depth[p] = found ? tmax * dot(d, fwd) : __int_as_float(0x7f800000);
-                    if (a.normal) {
-                        a.normal[3 * p] = normal.x;
-                        a.normal[3 * p + 1] = normal.y;
-                        a.normal[3 * p + 2] = normal.z;
-                    }
-                    if (a.object_id) a.object_id[p] = object;
-                    if (a.hit_instance) {
-                        a.hit_instance[p] = mesh ? hit_inst : -1;
-                        a.hit_triangle[p] = mesh ? __ldg(s.tri_index + hit_tri) : -1;
-                        a.hit_u[p] = mesh ? hu : 0.0f;
-                        a.hit_v[p] = mesh ? hv : 0.0f;
-                    }
-                    continue;
+                if (found) resolve(s, T.world, eye + d * tmax, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal,
+                    mat, object);
+                if (a.depth) a.depth[p] = found ? tmax * dot(d, fwd) : __int_as_float(0x7f800000);
+                if (a.normal) {
+                    a.normal[3 * p] = normal.x;
+                    a.normal[3 * p + 1] = normal.y;
+                    a.normal[3 * p + 2] = normal.z;
                 }
-                const float3 zero = mk3(0.0f, 0.0f, 0.0f);
-                float3 radiance;
-                if (!found) {
-                    const float t = saturate(dot(d, s.env_up) * 0.5f + 0.5f);
-                    const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
-                    radiance = zero + sky * 1.0f;
-                } else {
-                    radiance = radiance_of(mat, s.ambient, zero, zero);
-                    if (s.light_count == 1) {
-                        const DevLight &lt = s.lights[0];
-                        const float z = 1.0f - 2.0f * rand_float(rng);
-                        const float rad = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-                        const float phi = 6.28318530718f * rand_float(rng);
-                        float sin_phi, cos_phi;
-                        sincosf(phi, &sin_phi, &cos_phi);
-                        const float3 lp = lt.position + mk3(rad * cos_phi, rad * sin_phi, z) * lt.radius;
-                        const float3 to_light = lp - point;
-                        const float light_distance = sqrtf(dot(to_light, to_light));
-                        const float3 light_dir = to_light * (1.0f / light_distance);
-                        const float strength = lt.intensity * light_factor(lt, light_dir, light_distance);
-                        if (strength > 0.0f) {
-                            // The shadow ray: spheres and the floor first (scene_occluded, src/render_core.h:146-161).
-                            so = offset_origin(point, normal, light_dir);
-                            sd = light_dir;
-                            sdist = light_distance;
-                            bool blocked = false;
-                            for (int i = 0; i < s.sphere_count && !blocked; ++i) {
-                                float t;
-                                if (sphere_hit(s.spheres[i], so, sd, t) && t < sdist) blocked = true;
-                            }
-                            if (!blocked) {
-                                float dd;
-                                blocked = floor_hit(s.floor, so, sd, sdist, dd);
-                            }
-                            if (!blocked) {
-                                const float3 lit = lt.color * strength;
-                                const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
-                                const float3 specular =
-                                    zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), d)), mat.exponent);
-                                shadow_bytes = rgb_bytes(s.srgb_table, radiance);
-                                radiance = radiance_of(mat, s.ambient, diffuse, specular);
-                                pending = true;
-                            }
-                        }
-                    }
+                if (a.object_id) a.object_id[p] = object;
+                if (a.hit_instance) {
+                    a.hit_instance[p] = mesh ? hit_inst : -1;
+                    a.hit_triangle[p] = mesh ? __ldg(s.tri_index + hit_tri) : -1;
+                    a.hit_u[p] = mesh ? hu : 0.0f;
+                    a.hit_v[p] = mesh ? hv : 0.0f;
                 }
-                const int bytes = rgb_bytes(s.srgb_table, radiance);
-                if (pending) lit_bytes = bytes;
-                else put_rgb(a.rgb, pix, bytes);
             }
-            if (!a.rgb) continue;
+        }
+    }
+}
 
-            // The tile's shadow rays: the candidates are the instances whose boxes meet the convex hull of the
-            // segments from the shadow origins to their ends at the light. Separating axes: x, y and z, the
-            // direction away from the light, and four axes tilted from the sideways directions towards the
-            // light by the light sphere's angular radius, which hug the hull's sides. Each support is taken over
-            // the segments' own end points, so any axis is a valid test; these make it a tight one.
+// Shade kernel: one thread per pixel, straight-line code. The picture ray's hit resolved and lit (trace's
+// first bounce, src/render_core.h:202-245): a pixel with nothing left to trace gets its bytes here; a lit
+// surface leaves its shadow ray (origin, light distance) (direction, lit bytes) and its shadowed bytes (over
+// the hit's code) for the shadow kernel. shadow_o.w = 0 marks a pixel without a shadow ray.
+__global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ SceneParams s, const RenderArgs a,
+    long long pixels) {
+    const long long per_view = static_cast<long long>(a.width) * a.height;
+    const float3 zero = mk3(0.0f, 0.0f, 0.0f);
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < pixels;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int view = static_cast<int>(p / per_view);
+        const int rem = static_cast<int>(p % per_view);
+        const int y = rem / a.width, x = rem % a.width;
+        const int world = view / a.cameras_per_world;
+        const float4 c0 = __ldg(a.camera_basis + 3 * view), c1 = __ldg(a.camera_basis + 3 * view + 1);
+        const float4 c2 = __ldg(a.camera_basis + 3 * view + 2);
+        const float3 eye = mk3(c0.x, c0.y, c0.z), right = mk3(c0.w, c1.x, c1.y);
+        const float3 up = mk3(c1.z, c1.w, c2.x), fwd = mk3(c2.y, c2.z, c2.w);
+        uint32_t rng;
+        const float3 d = picture_ray(a, x, y, right, up, fwd, rng);
+        const int code = a.pic_code[p];
+        const float4 h = a.pic_hit[p];
+        float3 radiance;
+        bool pending = false;
+        float3 so = zero, sd = zero;
+        float sdist = 0.0f;
+        int lit_bytes = 0, shadow_bytes = 0;
+        if (code == CODE_NONE) {
+            const float t = saturate(dot(d, s.env_up) * 0.5f + 0.5f);
+            const float3 sky = (s.env_color_down + (s.env_color_up - s.env_color_down) * t) * s.env_intensity;
+            radiance = zero + sky * 1.0f;
+        } else {
+            const float tmax = h.x;
+            const int hit_inst = code >= 0 ? code : -1;
+            const bool hit_floor = code == CODE_FLOOR;
+            const int best_sphere = code <= CODE_SPHERE ? CODE_SPHERE - code : -1;
+            const float3 point = eye + d * tmax;
+            float3 normal;
+            DevMaterial mat;
+            int object;
+            resolve(s, world, point, d, hit_inst, __float_as_int(h.w), h.y, h.z, best_sphere, hit_floor, normal, mat, object);
+            radiance = radiance_of(mat, s.ambient, zero, zero);
+            if (s.light_count == 1) {
+                const DevLight &lt = s.lights[0];
+                const float z = 1.0f - 2.0f * rand_float(rng);
+                const float rad = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+                const float phi = 6.28318530718f * rand_float(rng);
+                float sin_phi, cos_phi;
+                sincosf(phi, &sin_phi, &cos_phi);
+                const float3 lp = lt.position + mk3(rad * cos_phi, rad * sin_phi, z) * lt.radius;
+                const float3 to_light = lp - point;
+                const float light_distance = sqrtf(dot(to_light, to_light));
+                const float3 light_dir = to_light * (1.0f / light_distance);
+                const float strength = lt.intensity * light_factor(lt, light_dir, light_distance);
+                if (strength > 0.0f) {
+                    // The shadow ray: spheres and the floor here (scene_occluded, src/render_core.h:146-161).
+                    so = offset_origin(point, normal, light_dir);
+                    sd = light_dir;
+                    sdist = light_distance;
+                    bool blocked = false;
+                    for (int i = 0; i < s.sphere_count && !blocked; ++i) {
+                        float t;
+                        if (sphere_hit(s.spheres[i], so, sd, t) && t < sdist) blocked = true;
+                    }
+                    if (!blocked) {
+                        float dd;
+                        blocked = floor_hit(s.floor, so, sd, sdist, dd);
+                    }
+                    if (!blocked) {
+                        const float3 lit = lt.color * strength;
+                        const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
+                        const float3 specular =
+                            zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), d)), mat.exponent);
+                        shadow_bytes = rgb_bytes(s.srgb_table, radiance);
+                        radiance = radiance_of(mat, s.ambient, diffuse, specular);
+                        pending = true;
+                    }
+                }
+            }
+        }
+        const int bytes = rgb_bytes(s.srgb_table, radiance);
+        if (pending) {
+            lit_bytes = bytes;
+            a.shadow_o[p] = make_float4(so.x, so.y, so.z, sdist);
+            a.shadow_d[p] = make_float4(sd.x, sd.y, sd.z, __int_as_float(lit_bytes));
+            a.pic_code[p] = shadow_bytes;
+        } else {
+            put_rgb(a.rgb, p, bytes);
+            a.shadow_o[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+}
+
+// Shadow kernel: per tile, the shadow rays the shade kernel left. The candidates are the instances whose
+// boxes meet the convex hull of the tile's segments from the shadow origins to their ends at the light.
+// Separating axes: x, y and z, the direction away from the light, and four axes tilted from the sideways
+// directions towards the light by the light sphere's angular radius, which hug the hull's sides. Each support
+// is taken over the segments' own end points, so any axis is a valid test; these make it a tight one.
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const __grid_constant__ SceneParams s,
+    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
+    __shared__ TileBox warp_box[THREADS / 32][TILE_MAX_INSTANCES];
+    TileBox *box = warp_box[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int P = s.instance_count > 0 ? s.per_world : 0;
+    const long long first_leaf = s.tlas_internal;
+    const int max_steps = s.blas_node_count + 2;
+    const DevLight &lt = s.lights[0];
+    const float INF = __int_as_float(0x7f800000);
+    for (;;) {
+        const long long first = fetch_tiles(counter, lane);
+        if (first >= tiles) break;
+        const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
+        for (long long tile = first; tile < last; ++tile) {
+            const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
+            float4 o4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (T.pixel) o4 = a.shadow_o[T.pix];
+            const bool pending = o4.w > 0.0f;
             const unsigned shadow_lanes = __ballot_sync(FULL, pending);
             if (shadow_lanes == 0) continue;
-            const DevLight &lt = s.lights[0];
+            float4 d4 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+            if (pending) d4 = a.shadow_d[T.pix];
+            const float3 so = mk3(o4.x, o4.y, o4.z), sd = mk3(d4.x, d4.y, d4.z);
+            const float sdist = o4.w;
             const float3 se = so + sd * sdist;
-            const float INF = __int_as_float(0x7f800000);
             const float mnx = warp_min(pending ? fminf(so.x, se.x) : INF);
             const float mny = warp_min(pending ? fminf(so.y, se.y) : INF);
             const float mnz = warp_min(pending ? fminf(so.z, se.z) : INF);
@@ -453,16 +554,20 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
                 for (int k = 0; k < AXES; ++k)
                     support[k] = warp_max(pending ? fmaxf(dot(axis[k], so), dot(axis[k], se)) : -INF);
             }
+            __syncwarp();
             bool scand = false;
             if (lane < P) {
-                const TileBox b = sm.box[lane];
-                const float3 c = mk3(0.5f * (b.lo.x + b.hi.x), 0.5f * (b.lo.y + b.hi.y), 0.5f * (b.lo.z + b.hi.z));
-                const float3 h = mk3(0.5f * (b.hi.x - b.lo.x), 0.5f * (b.hi.y - b.lo.y), 0.5f * (b.hi.z - b.lo.z));
+                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(T.world) * P + lane);
+                const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
+                box[lane].lo = make_float4(lo.x, lo.y, lo.z, __int_as_float(~__float_as_int(lo.w)));
+                box[lane].hi = hi;
+                const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+                const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
                 const float scale = fabsf(lt.position.x) + fabsf(lt.position.y) + fabsf(lt.position.z) + lt.radius +
                     fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + h.x + h.y + h.z + 1.0f;
                 const float pad = 1e-4f * scale;
-                scand = b.hi.x >= mnx - pad && b.lo.x <= mxx + pad && b.hi.y >= mny - pad && b.lo.y <= mxy + pad &&
-                    b.hi.z >= mnz - pad && b.lo.z <= mxz + pad;
+                scand = hi.x >= mnx - pad && lo.x <= mxx + pad && hi.y >= mny - pad && lo.y <= mxy + pad &&
+                    hi.z >= mnz - pad && lo.z <= mxz + pad;
 #pragma unroll
                 for (int k = 0; k < AXES; ++k) {
                     if (k < axes && dot(axis[k], c) - abs_dot(axis[k], h) >
@@ -470,12 +575,13 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
                         scand = false;
                 }
             }
+            __syncwarp();
             bool blocked = false;
             const float3 sinv = safe_inverse(sd);
             for (unsigned m = __ballot_sync(FULL, scand); m != 0; m &= m - 1) {
                 const bool open = pending && !blocked;
                 if (!__any_sync(FULL, open)) break;
-                const TileBox b = sm.box[__ffs(m) - 1];
+                const TileBox b = box[__ffs(m) - 1];
                 if (open && box_entry(b.lo, b.hi, so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
@@ -483,9 +589,28 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_tiles_kernel(const
                         __float_as_int(b.lo.w), so, sd, tm, true, ht, hu, hv, max_steps, a.error_flag);
                 }
             }
-            if (pending) put_rgb(a.rgb, pix, blocked ? shadow_bytes : lit_bytes);
+            if (pending) put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));
         }
     }
+}
+
+template <class Kernel>
+cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const RenderArgs &a, int *counter,
+    long long tiles, int tiles_x, int tiles_per_view, cudaStream_t stream) {
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    // Every SM full of resident warps, and no more warps than there are fetches of tiles.
+    long long blocks = static_cast<long long>(sms) * per_sm;
+    const long long needed = (tiles + TILES_PER_FETCH * (threads / 32) - 1) / (TILES_PER_FETCH * (threads / 32));
+    if (blocks > needed) blocks = needed;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    kernel<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(s, a, counter, tiles, tiles_x, tiles_per_view);
+    return cudaGetLastError();
 }
 
 template <int THREADS, int MIN_BLOCKS>
@@ -495,21 +620,23 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     const long long tiles = static_cast<long long>(tiles_per_view) * a.views;
     const bool aov = a.depth || a.normal || a.object_id || a.hit_instance;
     if (tiles == 0 || (!a.rgb && !aov)) return cudaSuccess;
-    auto kernel = render_tiles_kernel<THREADS, MIN_BLOCKS>;
-    int device = 0, sms = 0, per_sm = 0;
-    cudaError_t e = cudaGetDevice(&device);
+    cudaError_t e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+    if (e == cudaSuccess)
+        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
+            stream);
+    if (e != cudaSuccess || !a.rgb) return e;
+    const long long pixels = static_cast<long long>(a.views) * a.width * a.height;
+    int device = 0, sms = 0;
+    e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, 0);
     if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    // Every SM full of resident warps, and no more warps than there are fetches of tiles.
-    long long blocks = static_cast<long long>(sms) * per_sm;
-    const long long needed = (tiles + TILES_PER_FETCH * (THREADS / 32) - 1) / (TILES_PER_FETCH * (THREADS / 32));
-    if (blocks > needed) blocks = needed;
-    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return e;
-    kernel<<<static_cast<unsigned>(blocks), THREADS, 0, stream>>>(s, a, counter, tiles, tiles_x, tiles_per_view);
-    return cudaGetLastError();
+    long long blocks = (pixels + 255) / 256;
+    if (blocks > 32LL * sms) blocks = 32LL * sms;
+    shade_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(s, a, pixels);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || s.light_count != 1) return e;
+    return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
+        stream);
 }
 
 }  // namespace

@@ -103,6 +103,20 @@ __global__ void __launch_bounds__(128) ray_kernel(const __grid_constant__ SceneP
     a.object_id[i] = found ? hit.object : OBJECT_NONE;
 }
 
+// One thread per view: the camera basis of camera_from_matrix (src/render_core.h:264-273), renormalised.
+__global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *cameras, int views, float4 *basis) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= views) return;
+    float m[12];
+    for (int k = 0; k < 12; ++k) m[k] = __ldg(cameras + 12 * static_cast<size_t>(v) + k);
+    const float3 right = normalize(mk3(m[0], m[4], m[8]));
+    const float3 up = normalize(mk3(m[1], m[5], m[9]));
+    const float3 fwd = normalize(mk3(-m[2], -m[6], -m[10]));
+    basis[3 * v] = make_float4(m[3], m[7], m[11], right.x);
+    basis[3 * v + 1] = make_float4(right.y, right.z, up.x, up.y);
+    basis[3 * v + 2] = make_float4(up.z, fwd.x, fwd.y, fwd.z);
+}
+
 }  // namespace
 
 cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream) {
@@ -111,6 +125,12 @@ cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_
     if (blocks <= 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
     render_kernel<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(s, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prepare_cameras(const float *cameras, int views, float4 *basis, cudaStream_t stream) {
+    if (views <= 0) return cudaSuccess;
+    prepare_cameras_kernel<<<(views + 127) / 128, 128, 0, stream>>>(cameras, views, basis);
     return cudaGetLastError();
 }
 
