@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
+    p.add_argument("--profile", action="store_true",
+                   help="device-resident steps only (no autotune, e2e, CPU or reference arms): for ncu captures")
     return p.parse_args()
 
 
@@ -74,7 +76,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -123,11 +125,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
+PROFILE = os.path.join(ROOT, "profiles", "camera_tiles_kernel_body_worlds.md")
+
+
 def traffic_per_image():
-    """DRAM bytes per image of the render kernel, from the committed ncu summary (or None)."""
-    path = os.path.join(ROOT, "profiles", "render_kernel_body_worlds.md")
+    """DRAM bytes per image of the camera kernel, from the committed ncu summary (or None)."""
     try:
-        for line in open(path):
+        for line in open(PROFILE):
             if line.startswith("dram_bytes_per_image:"):
                 return float(line.split(":", 1)[1].split()[0])
     except OSError:
@@ -135,15 +139,31 @@ def traffic_per_image():
     return None
 
 
-def render_algorithmic_bytes(wl, per_world, blas_bytes):
-    """Compulsory bytes of one render launch: outputs, cameras, each world's tree and instance records, and the
-    shared meshes once."""
+def camera_kernel_algorithmic_bytes(wl, per_world, blas_bytes):
+    """Compulsory bytes of one camera-kernel launch: its outputs (depth 4 and ID 4 per pixel, and the picture
+    ray's hit handed to the shade kernel, 16 + 4), the cameras (48 per view), each world's leaf boxes (32 per
+    instance) and instance records (64), and the shared meshes once."""
     d = wl.desc
     views = d.view_count
-    out = views * d.height * d.width * (3 + 4 + 4)
+    out = views * d.height * d.width * (4 + 4 + 16 + 4)
     cams = views * 48
-    trees = d.world_count * ((2 * per_world - 1) * 32 + per_world * 64)
+    trees = d.world_count * per_world * (32 + 64)
     return out + cams + trees + blas_bytes
+
+
+def rays_per_image(wl, sample=16):
+    """Rays the path traces per image (a centre ray and a picture ray per pixel, and a shadow ray per lit
+    picture hit), counted by the oracle on the first sample worlds."""
+    import oracle as O
+    from neraulgraphics_b200.scene import SceneDesc
+    d = wl.desc
+    desc = SceneDesc(d.width, d.height, sample, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    o = O.Oracle(desc)
+    o.bind_bodies(**wl.binding)
+    o.set_body_poses(wl.poses[:sample])
+    o.render(wl.cameras[:sample], wl.fov, 1, rgb=True, depth=True, object_ids=True)
+    _, rays = o.traversal_bytes()
+    return rays / sample
 
 
 def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64):
@@ -225,7 +245,7 @@ def run_ours(args, rank, world, local_rank, dist):
     kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
     tuned = None
     r.set_body_poses(poses_dev[0])
-    if not args.no_autotune:
+    if not args.no_autotune and not args.profile:
         from neraulgraphics_b200.autotune import tune
         tuned = tune(r, cams_dev, wl.fov, rgb=True, depth=True, object_ids=True, use_cache=False)
         for t in sorted(tuned["timings"], key=lambda t: t["ms"])[:12]:
@@ -258,6 +278,18 @@ def run_ours(args, rank, world, local_rank, dist):
         dist.barrier()
     views = d.view_count
     value = world * views * K / (total_ms / 1000.0)
+    # Per-kernel GPU times of the render, from the library's events between its launches (untimed renders).
+    stage = []
+    for s in range(5):
+        r.render(cams_dev, wl.fov, 1, **kw)
+        stage.append(r.last_stage_ms)
+    stage_ms = [statistics.median(x[i] for x in stage) for i in range(len(stage[0]))]
+    if args.profile:
+        if rank == 0:
+            return {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,
+                    "warmup": W, "ms_per_step": round(total_ms / K, 4), "profile_run": True,
+                    "stage_ms": [round(x, 4) for x in stage_ms]}
+        return None
 
     # End to end through the public API with host buffers.
     pinned_poses = torch.from_numpy(steps_np).pin_memory().numpy()
@@ -300,9 +332,11 @@ def run_ours(args, rank, world, local_rank, dist):
     peak, peak_kind = peaks()
     built = ng.build_meshes(d.meshes)
     blas_bytes = built["nodes"].nbytes + built["triangles"].nbytes
-    alg = render_algorithmic_bytes(wl, d.per_world, blas_bytes)
+    alg = camera_kernel_algorithmic_bytes(wl, d.per_world, blas_bytes)
     rmed = statistics.median(render_ms)
-    achieved = alg / (rmed / 1000.0) / 1e9
+    cam_ms = stage_ms[0]
+    achieved = alg / (cam_ms / 1000.0) / 1e9
+    rpi = rays_per_image(wl)
     tr = traffic_per_image()
     clk = clocks.summary()
     return {
@@ -312,17 +346,23 @@ def run_ours(args, rank, world, local_rank, dist):
         "config": workload_config(args.worlds, {"parallelism": f"worlds sharded, {args.worlds} per GPU, no collective",
                                                 "l2": "flushed between timed steps (256 MiB write)"}),
         "stages_ms": {"set_body_poses": round(statistics.median(build_ms), 4),
-                      "render": round(rmed, 4)},
-        "rays_per_s_estimate": None,
+                      "render": round(rmed, 4),
+                      **({"camera_rays": round(stage_ms[0], 4), "shading": round(stage_ms[1], 4),
+                          "shadow_rays": round(stage_ms[2], 4)} if len(stage_ms) == 3 else {})},
+        "rays_per_s": round(value * rpi, 1),
+        "rays_per_image": round(rpi, 1),
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": KE, "path": "BatchRenderer.set_body_poses(pinned host poses) + render(host cameras, out=pinned)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": None if tr is None else int(tr * views),
-                     "kernel": "render_kernel", "algorithmic_bytes_per_launch": int(alg)},
+                     "kernel": "camera_tiles_kernel", "kernel_ms": round(cam_ms, 4),
+                     "algorithmic_bytes_per_launch": int(alg)},
         "cpu_baseline": cpu,
         "reference_cuda": ref_cuda,
-        "gpu_launches": 3 * K,
+        # Per step: the tree build (compose + per-world build, inter-world links) and the render: the camera-basis
+        # kernel and the camera, shade and shadow kernels (tile path), or the camera-basis and one render kernel.
+        "gpu_launches": (2 + (4 if len(stage_ms) == 3 else 2)) * K,
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
                                                                             "leaf_batch", "ms")},
         "clocks": clk,

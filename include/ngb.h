@@ -294,6 +294,10 @@ int32_t ngb_view_count(const ngb_renderer *r);
 int32_t ngb_instances_per_world(const ngb_renderer *r);
 /* GPU time of the last render or ray query, from CUDA events around its launch (cuda_backend.cu:537-543). */
 float ngb_last_kernel_ms(const ngb_renderer *r);
+/* The last render's GPU time by kernel, from CUDA events between its launches: *count = 3 for the tile
+ * kernels (camera rays, shading, shadow rays), 1 for the others (the whole launch). Up to capacity entries are
+ * written. No counterpart in the reference, which times the render as one launch. */
+int ngb_last_stage_ms(ngb_renderer *r, float *ms, int32_t capacity, int32_t *count);
 
 /* ---- inspection, for parity checks ------------------------------------------------------------------ */
 

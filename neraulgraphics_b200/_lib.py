@@ -56,6 +56,7 @@ def lib():
     L.ngb_set_stream.argtypes = [_vp, _vp]
     L.ngb_set_sync.argtypes = [_vp, C.c_int32, C.c_double]
     L.ngb_synchronize.argtypes = [_vp, C.c_double]
+    L.ngb_last_stage_ms.argtypes = [_vp, _f32p, C.c_int32, _i32p]
     for name in ("ngb_width", "ngb_height", "ngb_world_count", "ngb_cameras_per_world", "ngb_view_count",
                  "ngb_instances_per_world"):
         getattr(L, name).argtypes = [_vp]

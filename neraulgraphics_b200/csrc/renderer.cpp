@@ -134,6 +134,9 @@ struct Renderer {
 
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr};  // between the tile render's camera, shade and shadow kernels
+    int stages = 0;                                // kernels timed apart in the last render: 1 or 3
+    float stage_ms[3] = {0.0f, 0.0f, 0.0f};
     bool synchronous = true;
     double timeout = 120.0;
     float kernel_ms = 0.0f;
@@ -144,6 +147,7 @@ struct Renderer {
 
     void build(const float *matrices_in, bool compose, const float *poses);
     void finish();
+    void read_timing();
     void wait(cudaEvent_t ev, double seconds);
     void set_instance_transforms(const float *m, int memory);
     void bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc);
@@ -184,6 +188,8 @@ Renderer::Renderer(const ngb_scene &s) {
     stream = own_stream;
     CK(cudaEventCreate(&ev_start));
     CK(cudaEventCreate(&ev_stop));
+    CK(cudaEventCreate(&ev_stage[0]));
+    CK(cudaEventCreate(&ev_stage[1]));
     CK(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
     CK(cudaHostAlloc(&host_error, sizeof(int), cudaHostAllocDefault));
     *host_error = 0;
@@ -319,6 +325,8 @@ Renderer::~Renderer() {
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
+    for (cudaEvent_t e : ev_stage)
+        if (e) cudaEventDestroy(e);
     if (ev_done) cudaEventDestroy(ev_done);
     if (host_error) cudaFreeHost(host_error);
     if (own_stream) cudaStreamDestroy(own_stream);
@@ -352,15 +360,26 @@ void Renderer::wait(cudaEvent_t ev, double seconds) {
 
 // Called after every launch: brings the device's error flag back with the work and, when synchronous,
 // waits for both.
+// The last launch's GPU times, once its events have completed.
+void Renderer::read_timing() {
+    if (!timing_pending) return;
+    CK(cudaEventElapsedTime(&kernel_ms, ev_start, ev_stop));
+    if (stages == 3) {
+        CK(cudaEventElapsedTime(&stage_ms[0], ev_start, ev_stage[0]));
+        CK(cudaEventElapsedTime(&stage_ms[1], ev_stage[0], ev_stage[1]));
+        CK(cudaEventElapsedTime(&stage_ms[2], ev_stage[1], ev_stop));
+    } else {
+        stage_ms[0] = kernel_ms;
+    }
+    timing_pending = false;
+}
+
 void Renderer::finish() {
     CK(cudaMemcpyAsync(host_error, error_flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CK(cudaEventRecord(ev_done, stream));
     if (!synchronous) return;
     wait(ev_done, timeout);
-    if (timing_pending) {
-        CK(cudaEventElapsedTime(&kernel_ms, ev_start, ev_stop));
-        timing_pending = false;
-    }
+    read_timing();
     if (*host_error) throw CudaFailure(-1, device_error_message(*host_error));
 }
 
@@ -522,12 +541,16 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
             a.shadow_o = shadow_o.ensure(pixels());
             a.shadow_d = shadow_d.ensure(pixels());
         }
-        CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream));
+        CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream, ev_stage[0],
+            ev_stage[1]));
+        stages = 3;
     } else if (persistent) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
         CK(launch_render_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
+        stages = 1;
     } else {
         CK(launch_render(params, a, stream));
+        stages = 1;
     }
     CK(cudaEventRecord(ev_stop, stream));
     timing_pending = true;
@@ -567,6 +590,7 @@ void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, flo
     a.error_flag = error_flag.p;
     CK(cudaEventRecord(ev_start, stream));
     CK(launch_rays(params, a, stream));
+    stages = 1;
     CK(cudaEventRecord(ev_stop, stream));
     timing_pending = true;
     finish();
@@ -778,10 +802,7 @@ int ngb_synchronize(ngb_renderer *h, double timeout_seconds) {
     return guarded(h, [&](ngb::Renderer &r) {
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, timeout_seconds > 0.0 ? timeout_seconds : r.timeout);
-        if (r.timing_pending) {
-            CK(cudaEventElapsedTime(&r.kernel_ms, r.ev_start, r.ev_stop));
-            r.timing_pending = false;
-        }
+        r.read_timing();
         if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
     });
 }
@@ -798,14 +819,21 @@ float ngb_last_kernel_ms(const ngb_renderer *ch) {
     if (!h) return 0.0f;
     float ms = 0.0f;
     guarded(h, [&](ngb::Renderer &r) {
-        if (r.timing_pending) {
-            r.wait(r.ev_stop, r.timeout);
-            CK(cudaEventElapsedTime(&r.kernel_ms, r.ev_start, r.ev_stop));
-            r.timing_pending = false;
-        }
+        if (r.timing_pending) r.wait(r.ev_stop, r.timeout);
+        r.read_timing();
         ms = r.kernel_ms;
     });
     return ms;
+}
+
+int ngb_last_stage_ms(ngb_renderer *h, float *ms, int32_t capacity, int32_t *count) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(ms != nullptr && count != nullptr && capacity >= 0, "ms and count must not be null");
+        if (r.timing_pending) r.wait(r.ev_stop, r.timeout);
+        r.read_timing();
+        *count = r.stages;
+        for (int i = 0; i < r.stages && i < capacity; ++i) ms[i] = r.stage_ms[i];
+    });
 }
 
 int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_count, int32_t *triangle_count,

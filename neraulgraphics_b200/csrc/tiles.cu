@@ -614,17 +614,30 @@ cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const
 }
 
 template <int THREADS, int MIN_BLOCKS>
-cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream) {
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream,
+    cudaEvent_t after_camera, cudaEvent_t after_shade) {
     const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
     const int tiles_per_view = tiles_x * tiles_y;
     const long long tiles = static_cast<long long>(tiles_per_view) * a.views;
     const bool aov = a.depth || a.normal || a.object_id || a.hit_instance;
-    if (tiles == 0 || (!a.rgb && !aov)) return cudaSuccess;
-    cudaError_t e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+    cudaError_t e = cudaSuccess;
+    auto mark = [&](cudaEvent_t ev) {
+        if (e == cudaSuccess && ev) e = cudaEventRecord(ev, stream);
+    };
+    if (tiles == 0 || (!a.rgb && !aov)) {
+        mark(after_camera);
+        mark(after_shade);
+        return e;
+    }
+    e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
     if (e == cudaSuccess)
         e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
             stream);
-    if (e != cudaSuccess || !a.rgb) return e;
+    mark(after_camera);
+    if (e != cudaSuccess || !a.rgb) {
+        mark(after_shade);
+        return e;
+    }
     const long long pixels = static_cast<long long>(a.views) * a.width * a.height;
     int device = 0, sms = 0;
     e = cudaGetDevice(&device);
@@ -634,6 +647,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (blocks > 32LL * sms) blocks = 32LL * sms;
     shade_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(s, a, pixels);
     e = cudaGetLastError();
+    mark(after_shade);
     if (e != cudaSuccess || s.light_count != 1) return e;
     return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
         stream);
@@ -642,14 +656,14 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
 }  // namespace
 
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
-    cudaStream_t stream) {
+    cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade) {
     if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) return cudaErrorInvalidValue;
     // (threads per CTA, register budget) -> the instantiation with that budget.
-    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, stream);
-    if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6>(s, a, counter, stream);
-    if (t.threads == 128 && t.registers == 96) return launch_variant<128, 5>(s, a, counter, stream);
-    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, stream);
-    if (t.threads == 256 && t.registers == 80) return launch_variant<256, 3>(s, a, counter, stream);
+    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 128 && t.registers == 96) return launch_variant<128, 5>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 256 && t.registers == 80) return launch_variant<256, 3>(s, a, counter, stream, after_camera, after_shade);
     return cudaErrorInvalidValue;
 }
 

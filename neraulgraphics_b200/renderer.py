@@ -287,6 +287,15 @@ class BatchRenderer:
     def last_kernel_ms(self) -> float:
         return float(self._lib.ngb_last_kernel_ms(self._h))
 
+    @property
+    def last_stage_ms(self) -> list:
+        """The last render's GPU ms by kernel: [camera rays, shading, shadow rays] for the tile kernels, else
+        [whole launch]."""
+        ms = (C.c_float * 4)()
+        n = C.c_int32(0)
+        check(self._lib.ngb_last_stage_ms(self._h, ms, 4, C.byref(n)), self._h)
+        return [float(ms[i]) for i in range(n.value)]
+
     def synchronize(self, timeout=_TIMEOUT_S):
         """Waits for the queued work (at most timeout seconds) and raises CudaError if a kernel reported an error."""
         check(self._lib.ngb_synchronize(self._h, float(timeout)), self._h)
