@@ -280,6 +280,13 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
 int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers,
     int32_t leaf_batch);
 
+/* How the instance trees are built. mode 0 (default): one fused launch of per-world groups when a world
+ * holds at most 1024 instances, else the global build; 1: always the per-world build (at most 1024 instances
+ * per world); 2: always the global build (global radix sort, Karras nodes, bottom-up refit over global
+ * memory, the reference's steps in cuda_tlas.cuh:215-306). Both make the same tree. No counterpart in the
+ * reference, which always runs its global build. */
+int ngb_set_build(ngb_renderer *r, int32_t mode);
+
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
  * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */
 int ngb_synchronize(ngb_renderer *r, double timeout_seconds);

@@ -22,8 +22,8 @@ constexpr int OBJECT_INSTANCE = OBJECT_FLOOR + 1;
 
 constexpr float NO_HIT = 1e30f;
 // Stack depths. A mesh's tree is at most 60 deep (the host builder's limit), so 64 entries hold any
-// traversal stack over it. A world's LBVH is at most 30 (Morton bits) + ceil(log2(instances)) + 1 deep,
-// under 64 for any instance count below 2^32.
+// traversal stack over it. A world's LBVH is at most 30 (Morton bits) + ceil(log2(instances)) + 1 deep
+// (equal keys split on their positions), 53 for the largest world allowed (2^22 instances).
 constexpr int BLAS_STACK = 64;
 constexpr int TLAS_STACK = 64;
 

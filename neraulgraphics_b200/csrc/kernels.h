@@ -36,9 +36,24 @@ struct BuildArgs {
 
 // Group size (threads per world) of the per-world build: a power of two, at least 32.
 int build_group_size(int per_world);
-// Largest instance count per world the per-world build handles.
+// Largest instance count per world the per-world build handles; above it the global build runs.
 constexpr int MAX_PER_WORLD = 1024;
+// Largest instance count per world at all: a world's tree is then at most 30 + 22 + 1 deep, which the
+// traversal stacks hold (see device.cuh).
+constexpr int MAX_INSTANCES_PER_WORLD = 1 << 22;
 cudaError_t launch_build_worlds(const BuildArgs &a, cudaStream_t stream);
+
+// The global build: the same tree for any instance count per world, over global memory (see lbvh.cu).
+struct LargeBuildScratch {
+    float4 *aabb;                   // n x 2: each instance's world box
+    int *bounds;                    // worlds x 6: ordered-int centre bounds
+    unsigned long long *keys_a;     // n: the radix sort's keys, ping
+    unsigned long long *keys_b;     // n: pong
+    int *ids_a, *ids_b;             // n each: the ids sorted with them
+    unsigned *counts;               // 256 x large_sort_blocks(n)
+};
+int large_sort_blocks(long long n);
+cudaError_t launch_build_large(const BuildArgs &a, const LargeBuildScratch &t, cudaStream_t stream);
 
 // Rendering every view of a batch.
 struct RenderArgs {

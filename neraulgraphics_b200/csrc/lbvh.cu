@@ -341,6 +341,242 @@ __global__ void __launch_bounds__(128) fit_world_links_kernel(const int *roots, 
     }
 }
 
+// ------------------------------------------------------------------------------------------------------
+// The global build, for worlds of more than MAX_PER_WORLD instances (one large world of 100,000 instances,
+// say): the same tree node for node, built over global memory in the reference's steps (cuda_tlas.cuh:69-211)
+// with a stable LSD radix sort of its own in place of CUB's.
+
+// Each world's centre bounds start empty.
+__global__ void __launch_bounds__(128) init_bounds_kernel(int *bounds, int worlds) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= worlds) return;
+    for (int k = 0; k < 3; ++k) {
+        bounds[6 * w + k] = to_ordered(1e30f);
+        bounds[6 * w + 3 + k] = to_ordered(-1e30f);
+    }
+}
+
+// Matrix, inverse, record and world box of each instance, and its world's centre bounds (place_instances,
+// cuda_tlas.cuh:69-96): the per-world kernel's first step, one thread per instance.
+__global__ void __launch_bounds__(128) place_kernel(const BuildArgs a, float4 *aabb, int *bounds) {
+    const long long g = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (g >= a.n) return;
+    const long long w = g / a.per_world;
+    const int i = static_cast<int>(g % a.per_world);
+    float m[12];
+    if (a.compose) {
+        compose(a, w, i, m);
+        float *mo = a.matrices_out + 12 * g;
+        for (int k = 0; k < 12; ++k) mo[k] = m[k];
+    } else {
+        const float *mi = a.matrices_in + 12 * g;
+        for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+    }
+    float inv[12];
+    invert_affine(m, inv);
+    float4 *rec = a.inst + 4 * g;
+    rec[0] = make_float4(inv[0], inv[1], inv[2], inv[3]);
+    rec[1] = make_float4(inv[4], inv[5], inv[6], inv[7]);
+    rec[2] = make_float4(inv[8], inv[9], inv[10], inv[11]);
+    rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + i)), __int_as_float(i), 0.0f, 0.0f);
+    const float *lb = a.slot_bounds + 6 * i;
+    float b[6], lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
+    for (int k = 0; k < 6; ++k) b[k] = __ldg(lb + k);
+    for (int corner = 0; corner < 8; ++corner) {
+        const float p[3] = {(corner & 1) ? b[3] : b[0], (corner & 2) ? b[4] : b[1], (corner & 4) ? b[5] : b[2]};
+        for (int ax = 0; ax < 3; ++ax) {
+            const float v = m[4 * ax] * p[0] + m[4 * ax + 1] * p[1] + m[4 * ax + 2] * p[2] + m[4 * ax + 3];
+            lo[ax] = fminf(lo[ax], v);
+            hi[ax] = fmaxf(hi[ax], v);
+        }
+    }
+    aabb[2 * g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+    aabb[2 * g + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    for (int ax = 0; ax < 3; ++ax) {
+        const int c = to_ordered(0.5f * (lo[ax] + hi[ax]));
+        atomicMin(&bounds[6 * w + ax], c);
+        atomicMax(&bounds[6 * w + 3 + ax], c);
+    }
+}
+
+// Keys (make_keys, cuda_tlas.cuh:99-115): world << 32 | Morton code, and the ids to sort with them.
+__global__ void __launch_bounds__(128) keys_kernel(const BuildArgs a, const float4 *aabb, const int *bounds,
+    unsigned long long *keys_sort, int *ids_sort) {
+    const long long g = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (g >= a.n) return;
+    const long long w = g / a.per_world;
+    const float4 lo = aabb[2 * g], hi = aabb[2 * g + 1];
+    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    uint32_t q[3];
+    for (int ax = 0; ax < 3; ++ax) {
+        const float blo = from_ordered(bounds[6 * w + ax]), bhi = from_ordered(bounds[6 * w + 3 + ax]);
+        const float centre = 0.5f * (l[ax] + h[ax]);
+        const float extent = bhi - blo;
+        const float t = extent > 1e-20f ? (centre - blo) / extent : 0.0f;
+        q[ax] = static_cast<uint32_t>(fminf(fmaxf(t, 0.0f), 1.0f) * 1023.0f);
+    }
+    const uint32_t morton = (spread_bits(q[0]) << 2) | (spread_bits(q[1]) << 1) | spread_bits(q[2]);
+    const unsigned long long key = (static_cast<unsigned long long>(w) << 32) | morton;
+    a.keys[g] = key;
+    keys_sort[g] = key;
+    ids_sort[g] = static_cast<int>(g);
+}
+
+constexpr int SORT_BLOCK = 1024;  // keys per block of a radix pass, one per thread
+constexpr int RADIX = 256;        // 8-bit digits
+
+// Radix pass, step 1: each block's count of each digit, stored digit-major (counts[digit * blocks + block]),
+// so that one exclusive scan gives every (digit, block) its first output position.
+__global__ void __launch_bounds__(SORT_BLOCK) radix_count_kernel(const unsigned long long *keys, long long n, int shift,
+    unsigned *counts, int blocks) {
+    __shared__ unsigned hist[RADIX];
+    if (threadIdx.x < RADIX) hist[threadIdx.x] = 0;
+    __syncthreads();
+    const long long i = blockIdx.x * static_cast<long long>(SORT_BLOCK) + threadIdx.x;
+    if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (RADIX - 1)], 1u);
+    __syncthreads();
+    if (threadIdx.x < RADIX) counts[static_cast<long long>(threadIdx.x) * blocks + blockIdx.x] = hist[threadIdx.x];
+}
+
+// Radix pass, step 2: exclusive prefix sum of the counts in place, one block.
+__global__ void __launch_bounds__(1024) radix_scan_kernel(unsigned *counts, long long total) {
+    __shared__ unsigned partial[1024];
+    const long long per = (total + 1023) / 1024;
+    const long long begin = threadIdx.x * per, end = begin + per < total ? begin + per : total;
+    unsigned sum = 0;
+    for (long long k = begin; k < end; ++k) sum += counts[k];
+    partial[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan of the partial sums
+        const unsigned v = threadIdx.x >= off ? partial[threadIdx.x - off] : 0u;
+        __syncthreads();
+        partial[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned run = threadIdx.x > 0 ? partial[threadIdx.x - 1] : 0u;
+    for (long long k = begin; k < end; ++k) {
+        const unsigned c = counts[k];
+        counts[k] = run;
+        run += c;
+    }
+}
+
+// Radix pass, step 3: every key to its position, stable: its block's first position for its digit, plus the
+// keys of that digit before it in the block (in earlier warps, counted in shared memory, and earlier lanes of
+// its own warp, from the lanes holding the same digit).
+__global__ void __launch_bounds__(SORT_BLOCK) radix_scatter_kernel(const unsigned long long *keys_in, const int *ids_in,
+    unsigned long long *keys_out, int *ids_out, long long n, int shift, const unsigned *offsets, int blocks) {
+    __shared__ unsigned warp_count[SORT_BLOCK / 32][RADIX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < (SORT_BLOCK / 32) * RADIX; k += SORT_BLOCK) (&warp_count[0][0])[k] = 0;
+    __syncthreads();
+    const long long i = blockIdx.x * static_cast<long long>(SORT_BLOCK) + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned long long key = valid ? keys_in[i] : 0ull;
+    const int digit = valid ? static_cast<int>((key >> shift) & (RADIX - 1)) : RADIX;
+    const unsigned peers = __match_any_sync(0xffffffffu, digit);
+    const unsigned rank_in_warp = __popc(peers & ((1u << lane) - 1u));
+    if (valid && rank_in_warp == 0) warp_count[warp][digit] = __popc(peers);
+    __syncthreads();
+    if (!valid) return;
+    unsigned pos = offsets[static_cast<long long>(digit) * blocks + blockIdx.x] + rank_in_warp;
+    for (int w = 0; w < warp; ++w) pos += warp_count[w][digit];
+    keys_out[pos] = key;
+    ids_out[pos] = ids_in[i];
+}
+
+// The leaves in sorted order (make_leaves, cuda_tlas.cuh:162-175), the sorted ids, and each world of one
+// instance's root (its leaf).
+__global__ void __launch_bounds__(128) leaves_kernel(const BuildArgs a, const int *ids_sorted, const float4 *aabb) {
+    const long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (k >= a.n) return;
+    const int g = ids_sorted[k];
+    a.sorted_ids[k] = g;
+    const float4 lo = aabb[2 * static_cast<long long>(g)], hi = aabb[2 * static_cast<long long>(g) + 1];
+    float4 *leaf = a.tlas + 2 * (a.n - 1 + k);
+    leaf[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(~g));
+    leaf[1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(-1));
+    if (k == 0) a.parent[0] = -1;
+    if (a.per_world == 1) a.roots[k] = static_cast<int>(a.n - 1 + k);
+}
+
+// The Karras node at sorted position p (build_radix_tree + common_prefix, cuda_tlas.cuh:119-159) over the
+// sorted 64-bit keys, equal keys told apart by position; and the root of the world whose run it spans.
+__global__ void __launch_bounds__(128) karras_kernel(const BuildArgs a, const unsigned long long *skeys) {
+    const long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    const long long n = a.n;
+    if (p >= n - 1) return;
+    const unsigned long long kp = skeys[p];
+    auto dlt = [&](long long x) -> int {
+        if (x < 0 || x >= n) return -1;
+        const unsigned long long kx = skeys[x];
+        if (kx == kp) return 64 + __clz(static_cast<int>(static_cast<uint32_t>(p) ^ static_cast<uint32_t>(x)));
+        return __clzll(static_cast<long long>(kp ^ kx));
+    };
+    const int d = dlt(p + 1) > dlt(p - 1) ? 1 : -1;
+    const int min_prefix = dlt(p - d);
+    long long max_length = 2;
+    while (dlt(p + max_length * d) > min_prefix) max_length *= 2;
+    long long length = 0;
+    for (long long t = max_length / 2; t >= 1; t /= 2)
+        if (dlt(p + (length + t) * d) > min_prefix) length += t;
+    const long long j = p + length * d;
+    const int node_prefix = dlt(j);
+    long long s = 0;
+    for (long long t = (length + 1) / 2;; t = (t + 1) / 2) {
+        if (dlt(p + (s + t) * d) > node_prefix) s += t;
+        if (t == 1) break;
+    }
+    const long long gamma = p + s * d + (d < 0 ? d : 0);
+    const long long rlo = p < j ? p : j, rhi = p < j ? j : p;
+    const int left = static_cast<int>((rlo == gamma) ? n - 1 + gamma : gamma);
+    const int right = static_cast<int>((rhi == gamma + 1) ? n - 1 + gamma + 1 : gamma + 1);
+    a.parent[left] = static_cast<int>(p);
+    a.parent[right] = static_cast<int>(p);
+    float4 *nd = a.tlas + 2 * p;
+    reinterpret_cast<float *>(nd)[3] = __int_as_float(left);
+    reinterpret_cast<float *>(nd + 1)[3] = __int_as_float(right);
+    const long long P = a.per_world;
+    if (rlo % P == 0 && rhi == rlo + P - 1) a.roots[rlo / P] = static_cast<int>(p);
+}
+
+// Boxes from the leaves up (fit_boxes, cuda_tlas.cuh:179-196): the second arrival at a node knows both
+// children are done and climbs on; it also writes the node's child-pair record. Counters are left at zero.
+__global__ void __launch_bounds__(128) refit_kernel(const BuildArgs a) {
+    const long long k = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    const long long n = a.n;
+    if (k >= n) return;
+    int node = static_cast<int>(n - 1 + k);
+    for (int steps = 0;; ++steps) {
+        const int par = a.parent[node];
+        if (par < 0) return;
+        if (steps > 128) {  // deeper than any tree over 64-bit keys: the links are malformed
+            *a.error_flag = 3;
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(&a.arrivals[par], 1) == 0) return;
+        __threadfence();
+        a.arrivals[par] = 0;
+        const float4 p0 = __ldcg(a.tlas + 2 * par), p1 = __ldcg(a.tlas + 2 * par + 1);
+        const int l = __float_as_int(p0.w), r = __float_as_int(p1.w);
+        const float4 l0 = __ldcg(a.tlas + 2 * l), l1 = __ldcg(a.tlas + 2 * l + 1);
+        const float4 r0 = __ldcg(a.tlas + 2 * r), r1 = __ldcg(a.tlas + 2 * r + 1);
+        a.tlas[2 * par] = make_float4(fminf(l0.x, r0.x), fminf(l0.y, r0.y), fminf(l0.z, r0.z), p0.w);
+        a.tlas[2 * par + 1] = make_float4(fmaxf(l1.x, r1.x), fmaxf(l1.y, r1.y), fmaxf(l1.z, r1.z), p1.w);
+        if (a.tlas_pairs) {
+            const bool leaf_l = l >= n - 1, leaf_r = r >= n - 1;
+            float4 *q = a.tlas_pairs + 4 * static_cast<long long>(par);
+            q[0] = make_float4(l0.x, l0.y, l0.z, l1.x);
+            q[1] = make_float4(l1.y, l1.z, r0.x, r0.y);
+            q[2] = make_float4(r0.z, r1.x, r1.y, r1.z);
+            q[3] = make_float4(__int_as_float(leaf_l ? ~__float_as_int(l0.w) : l), __int_as_float(leaf_l ? -1 : 0),
+                __int_as_float(leaf_r ? ~__float_as_int(r0.w) : r), __int_as_float(leaf_r ? -1 : 0));
+        }
+        node = par;
+    }
+}
+
 template <int G>
 cudaError_t launch_group(const BuildArgs &a, cudaStream_t stream) {
     constexpr int CTA = G < 128 ? 128 : G;
@@ -355,6 +591,44 @@ cudaError_t launch_group(const BuildArgs &a, cudaStream_t stream) {
 }
 
 }  // namespace
+
+int large_sort_blocks(long long n) { return static_cast<int>((n + SORT_BLOCK - 1) / SORT_BLOCK); }
+
+cudaError_t launch_build_large(const BuildArgs &a, const LargeBuildScratch &t, cudaStream_t stream) {
+    if (a.n == 0) return cudaSuccess;
+    const long long n = a.n;
+    const unsigned grid = static_cast<unsigned>((n + 127) / 128);
+    init_bounds_kernel<<<(a.worlds + 127) / 128, 128, 0, stream>>>(t.bounds, a.worlds);
+    place_kernel<<<grid, 128, 0, stream>>>(a, t.aabb, t.bounds);
+    keys_kernel<<<grid, 128, 0, stream>>>(a, t.aabb, t.bounds, t.keys_a, t.ids_a);
+    // Stable LSD radix sort over the Morton bits (0..29) and the world bits (32 and up) of the keys: the order
+    // of cub::DeviceRadixSort::SortPairs over (key, id) with ids ascending (cuda_tlas.cuh:241-243, 273-274).
+    int world_bits = 0;
+    while ((1LL << world_bits) < a.worlds) ++world_bits;
+    int shifts[8], passes = 0;
+    for (int sh = 0; sh < 32; sh += 8) shifts[passes++] = sh;
+    for (int sh = 32; sh < 32 + world_bits; sh += 8) shifts[passes++] = sh;
+    const int blocks = large_sort_blocks(n);
+    unsigned long long *kin = t.keys_a, *kout = t.keys_b;
+    int *iin = t.ids_a, *iout = t.ids_b;
+    for (int pass = 0; pass < passes; ++pass) {
+        radix_count_kernel<<<blocks, SORT_BLOCK, 0, stream>>>(kin, n, shifts[pass], t.counts, blocks);
+        radix_scan_kernel<<<1, 1024, 0, stream>>>(t.counts, static_cast<long long>(RADIX) * blocks);
+        radix_scatter_kernel<<<blocks, SORT_BLOCK, 0, stream>>>(kin, iin, kout, iout, n, shifts[pass], t.counts, blocks);
+        unsigned long long *kt = kin;
+        kin = kout;
+        kout = kt;
+        int *it = iin;
+        iin = iout;
+        iout = it;
+    }
+    leaves_kernel<<<grid, 128, 0, stream>>>(a, iin, t.aabb);
+    if (n > 1) {
+        karras_kernel<<<static_cast<unsigned>((n - 1 + 127) / 128), 128, 0, stream>>>(a, kin);
+        refit_kernel<<<grid, 128, 0, stream>>>(a);
+    }
+    return cudaGetLastError();
+}
 
 int build_group_size(int per_world) {
     int g = 32;

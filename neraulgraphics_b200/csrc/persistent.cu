@@ -29,7 +29,8 @@ namespace {
 
 using namespace tr;
 
-constexpr int STACK = 112;        // world tree (<= 41 deep for 1024 instances) + marker + mesh tree (<= 64)
+// World tree (<= 30 Morton levels + 22 levels among equal keys + 1 for 2^22 instances) + marker + mesh tree (<= 64).
+constexpr int STACK = 128;
 constexpr int MARKER = INT_MIN;   // stack entry that returns the walk from a mesh to its world's tree
 constexpr int ST_IDLE = 0, ST_WALK = 1, ST_DONE = 2;
 constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3;

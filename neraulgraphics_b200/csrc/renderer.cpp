@@ -103,6 +103,12 @@ struct Renderer {
     DevBuf<float4> inst, tlas;
     DevBuf<unsigned long long> keys;
     DevBuf<int> sorted_ids, roots, parent, arrivals;
+    // The global build's scratch (worlds of more than MAX_PER_WORLD instances, or when asked for).
+    int build_mode = 0;  // 0: automatic, 1: the per-world build, 2: the global build
+    DevBuf<float4> large_aabb;
+    DevBuf<int> large_bounds, large_ids_a, large_ids_b;
+    DevBuf<unsigned long long> large_keys_a, large_keys_b;
+    DevBuf<unsigned> large_counts;
     DevBuf<float4> blas_pairs, tlas_pairs;
     DevBuf<int2> slot_root;
     DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
@@ -148,6 +154,7 @@ struct Renderer {
     void build(const float *matrices_in, bool compose, const float *poses);
     void finish();
     void read_timing();
+    bool use_large_build() const { return build_mode == 2 || (build_mode == 0 && per_world > MAX_PER_WORLD); }
     void wait(cudaEvent_t ev, double seconds);
     void set_instance_transforms(const float *m, int memory);
     void bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc);
@@ -169,8 +176,8 @@ Renderer::Renderer(const ngb_scene &s) {
         " are too many");
     check_scene(s);
     check_meshes(s);
-    require(s.instance_count <= MAX_PER_WORLD, "a world holds " + std::to_string(s.instance_count) +
-        " instances, at most " + std::to_string(MAX_PER_WORLD) + " fit the per-world tree build");
+    require(s.instance_count <= MAX_INSTANCES_PER_WORLD, "a world holds " + std::to_string(s.instance_count) +
+        " instances, at most " + std::to_string(MAX_INSTANCES_PER_WORLD) + " are supported");
     require(static_cast<long long>(s.world_count) * s.instance_count <= (INT32_MAX - 1) / 2,
         "too many instances over all worlds");
     int device_count = 0;
@@ -336,6 +343,8 @@ Renderer::~Renderer() {
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
+    large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
+    large_keys_a.release(), large_keys_b.release(), large_counts.release();
     pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release();
     camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
@@ -409,7 +418,19 @@ void Renderer::build(const float *matrices_in, bool compose, const float *poses)
     a.arrivals = arrivals.p;
     a.error_flag = error_flag.p;
     a.tlas_pairs = tlas_pairs.p;
-    CK(launch_build_worlds(a, stream));
+    if (use_large_build()) {
+        LargeBuildScratch t{};
+        t.aabb = large_aabb.ensure(2 * n);
+        t.bounds = large_bounds.ensure(6 * static_cast<size_t>(worlds));
+        t.keys_a = large_keys_a.ensure(n);
+        t.keys_b = large_keys_b.ensure(n);
+        t.ids_a = large_ids_a.ensure(n);
+        t.ids_b = large_ids_b.ensure(n);
+        t.counts = large_counts.ensure(256 * static_cast<size_t>(large_sort_blocks(n)));
+        CK(launch_build_large(a, t, stream));
+    } else {
+        CK(launch_build_worlds(a, stream));
+    }
 }
 
 // src/batch.cpp:91-109 and src/cuda_backend.cu:457-469.
@@ -885,6 +906,15 @@ int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, i
         ngb::require(leaf_batch >= 1 && leaf_batch <= 32, "leaf_batch must be 1 to 32");
         r.kernel_choice = kernel;
         r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers, leaf_batch};
+    });
+}
+
+int ngb_set_build(ngb_renderer *h, int32_t mode) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(mode >= 0 && mode <= 2, "mode must be 0 (automatic), 1 (per world) or 2 (global)");
+        ngb::require(mode != 1 || r.per_world <= ngb::MAX_PER_WORLD,
+            "the per-world build takes at most " + std::to_string(ngb::MAX_PER_WORLD) + " instances per world");
+        r.build_mode = mode;
     });
 }
 

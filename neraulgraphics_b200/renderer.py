@@ -311,6 +311,11 @@ class BatchRenderer:
         check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes), int(registers),
                                        int(leaf_batch)), self._h)
 
+    def set_build(self, mode=0):
+        """Instance-tree build: 0 automatic (per-world groups up to 1024 instances per world, else global),
+        1 per-world, 2 global. Both make the same tree."""
+        check(self._lib.ngb_set_build(self._h, int(mode)), self._h)
+
     def record_hits(self, on=True):
         check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
 

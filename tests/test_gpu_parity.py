@@ -70,8 +70,20 @@ def assert_same_tlas(got, want):
     assert np.array_equal(bits(got["matrices"]), bits(want["matrices"]))
 
 
+@pytest.mark.parametrize("build", [1, 2])
 @pytest.mark.parametrize("case", ["icospheres", "scattered", "coincident", "single_leaf", "bodies", "one_world"])
-def test_tree_build_is_the_oracles(torch_cuda, case):
+def test_tree_build_is_the_oracles(torch_cuda, case, build):
+    """Both tree builds, the per-world groups (1) and the global build (2), against the oracle."""
+    check_tree_build(case, build)
+
+
+@pytest.mark.parametrize("case", ["large_world", "large_worlds"])
+def test_global_build_of_large_worlds_is_the_oracles(torch_cuda, case):
+    """Worlds beyond the per-world build's 1024 instances take the global build automatically."""
+    check_tree_build(case, 0)
+
+
+def check_tree_build(case, build):
     if case == "icospheres":
         wl = workloads.icosphere_worlds()
         desc, mats = wl.desc, wl.matrices
@@ -83,10 +95,15 @@ def test_tree_build_is_the_oracles(torch_cuda, case):
         desc, mats, _ = scenes.single_leaf_worlds()
     elif case == "one_world":
         desc, mats, _ = scenes.scattered_boxes(1, 1000)
+    elif case == "large_world":
+        desc, mats, _ = scenes.scattered_boxes(1, 5000)
+    elif case == "large_worlds":
+        desc, mats, _ = scenes.scattered_boxes(3, 1500)
     else:
         wl = workloads.body_worlds(worlds=256)
         desc, mats = wl.desc, None
     r, o = product(desc), O.Oracle(desc)
+    r.set_build(build)
     if mats is not None:
         r.set_instance_transforms(mats)
         o.set_instance_transforms(mats)
@@ -382,3 +399,25 @@ def test_tile_kernel_on_a_world_of_32_and_of_one_instance(torch_cuda):
         o.set_instance_transforms(wl.matrices)
         want = o.render(wl.cameras, 1.0, 1, **ALL, ties=True)
         assert_same_images(r.render(wl.cameras, 1.0, 1, **ALL), want, ties=want["ties"])
+
+
+def test_large_world_renders_and_casts_rays(torch_cuda):
+    """One world of 3000 instances (global build, the persistent kernel's world-tree walk): images and a LiDAR
+    sweep against the oracle."""
+    desc, mats, cams = scenes.scattered_boxes(1, 3000)
+    r, o = product(desc), O.Oracle(desc)
+    r.set_instance_transforms(mats)
+    o.set_instance_transforms(mats)
+    want = o.render(cams, scenes.FOV, 1, **ALL, ties=True)
+    assert_same_images(r.render(cams, scenes.FOV, 1, **ALL), want, ties=want["ties"])
+    el = np.radians(np.linspace(-15.0, 15.0, 16))
+    az = np.radians(np.linspace(0.0, 360.0, 128, endpoint=False))
+    e, a = np.meshgrid(el, az, indexing="ij")
+    dirs = np.stack([np.cos(e) * np.sin(a), np.sin(e), -np.cos(e) * np.cos(a)], -1).reshape(1, -1, 3).astype(np.float32)
+    origins = np.tile(np.float32([0.0, 0.0, -40.0]), (1, dirs.shape[1], 1))
+    got = r.cast_rays(origins, dirs, 100.0)
+    exp = o.cast_rays(origins, dirs, 100.0)
+    assert (got["object_id"] >= 34).mean() > 0.2
+    assert np.array_equal(got["object_id"], exp["object_id"])
+    assert np.array_equal(bits(got["distance"]), bits(exp["distance"]))
+    assert np.array_equal(bits(got["normal"]), bits(exp["normal"]))
