@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
+    p.add_argument("--config", default="body_worlds", choices=["body_worlds", "large_world"],
+                   help="body_worlds: the headline (4096 worlds x 64x64); large_world: one world of 100,000 "
+                        "instances at 1280x720 with a 64 x 2048 LiDAR sweep, poses redrawn every frame")
     p.add_argument("--profile", action="store_true",
                    help="device-resident steps only (no autotune, e2e, CPU or reference arms): for ncu captures")
     return p.parse_args()
@@ -369,6 +372,113 @@ def run_ours(args, rank, world, local_rank, dist):
     }
 
 
+def run_large(args, rank, world, local_rank, dist):
+    """One world of 100,000 instances: per frame, new instance matrices (device) -> global tree build ->
+    1280x720 RGB + depth + ID -> LiDAR sweep of 131,072 rays. frames/s over the whole job, CUDA events."""
+    import torch
+
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    wl = workloads.large_world(seed=rank, frames=W + K)
+    d = wl.desc
+    r = ng.BatchRenderer(d.width, d.height, 1, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances, device=dev)
+    mats = torch.from_numpy(wl.matrices).to(dev)
+    cams = torch.from_numpy(wl.cameras).to(dev)
+    lidar = wl.info["lidar"]
+    lo, ld = torch.from_numpy(lidar["origins"]).to(dev), torch.from_numpy(lidar["directions"]).to(dev)
+    kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for s in range(W):
+        r.set_instance_transforms(mats[s])
+        r.render(cams, wl.fov, 1, **kw)
+        r.cast_rays(lo, ld, lidar["max_distance"])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    with ClockSampler(local_rank) as clocks:
+        for s in range(K):
+            flush.zero_()
+            e = ev[s]
+            e[0].record()
+            r.set_instance_transforms(mats[W + s])
+            e[1].record()
+            r.render(cams, wl.fov, 1, **kw)
+            e[2].record()
+            hits = r.cast_rays(lo, ld, lidar["max_distance"])
+            e[3].record()
+        torch.cuda.synchronize()
+    stage = [[e[i].elapsed_time(e[i + 1]) for e in ev] for i in range(3)]
+    total_ms = sum(sum(x) for x in stage)
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    hit_frac = float((hits["object_id"] > 0).float().mean())
+    ref = None
+    if rank == 0 and not args.no_reference_cuda:
+        try:
+            ref = reference_cuda_large(wl, torch, mats, cams, lo, ld, min(K, 5), min(W, 2))
+        except Exception as e:  # reported, not fatal
+            ref = {"unavailable": f"{type(e).__name__}: {e}"}
+    if rank != 0:
+        return None
+    rays = lo.shape[1]
+    return {
+        "metric": "frames/s at 1 world x 100,000 instances, 1280x720 RGB+depth+ID + 64x2048 LiDAR, matrices redrawn "
+                  "and tree rebuilt every frame",
+        "value": round(world * K / (total_ms / 1000.0), 2), "unit": "frames/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": round(total_ms / K, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded large_world scene)",
+        "config": {"workload": "large_world: 1 world x 100,000 instances (box 12 / icosphere 320 / cylinder 512 / "
+                               "icosphere 1280 / icosphere 20480 tris), 1280x720, 64x2048 LiDAR, max range 150",
+                   "l2": "flushed between timed frames (256 MiB write)"},
+        "stages_ms": {"set_instance_transforms": round(statistics.median(stage[0]), 4),
+                      "render": round(statistics.median(stage[1]), 4),
+                      "lidar": round(statistics.median(stage[2]), 4)},
+        "lidar_rays_per_s": round(rays / (statistics.median(stage[2]) / 1000.0), 1),
+        "lidar_hit_fraction": round(hit_frac, 4),
+        "reference_cuda": ref,
+        "clocks": clocks.summary(),
+    }
+
+
+def reference_cuda_large(wl, torch, mats, cams, lo, ld, steps, warmup):
+    """The reference's CUDA backend on the same large-world frames, inputs on the device: ms per stage."""
+    import oracle as O
+    if not O.reference_available(cuda=True):
+        return None
+    ref = O.Reference(wl.desc, cuda=True)
+    lidar = wl.info["lidar"]
+    stream = torch.cuda.default_stream()
+    for s in range(warmup):
+        ref.set_instance_transforms(mats[s].data_ptr(), device=True)
+        ref.render_device(cams.data_ptr(), wl.fov, 1, 1 | 2 | 8)
+        ref.cast_rays_device(lo.data_ptr(), ld.data_ptr(), lo.shape[1], lidar["max_distance"])
+    torch.cuda.synchronize()
+    stage = [[], [], []]
+    for s in range(steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record(stream)
+        ref.set_instance_transforms(mats[warmup + s].data_ptr(), device=True)
+        e[1].record(stream)
+        ref.render_device(cams.data_ptr(), wl.fov, 1, 1 | 2 | 8)
+        e[2].record(stream)
+        ref.cast_rays_device(lo.data_ptr(), ld.data_ptr(), lo.shape[1], lidar["max_distance"])
+        e[3].record(stream)
+        e[3].synchronize()
+        for i in range(3):
+            stage[i].append(e[i].elapsed_time(e[i + 1]))
+    ms = [statistics.median(x) for x in stage]
+    return {"value": round(1000.0 / sum(ms), 2), "unit": "frames/s",
+            "stages_ms": {"set_instance_transforms": round(ms[0], 4), "render": round(ms[1], 4), "lidar": round(ms[2], 4)},
+            "what": "neraulgraphics 0.5.0 CudaBackend, same frames on the device, median step"}
+
+
 def run_reference(args, rank):
     """The reference's own CPU implementation, rank 0 only, with every host core."""
     from neraulgraphics_b200 import workloads
@@ -425,7 +535,7 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device(f"cuda:{local_rank}"))
-        line = run_ours(args, rank, world, local_rank, dist)
+        line = (run_large if args.config == "large_world" else run_ours)(args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()
     if line is not None:

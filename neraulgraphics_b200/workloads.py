@@ -7,6 +7,7 @@ on. Every generator is deterministic in its seed (numpy's default_rng).
 - `icosphere_worlds`: 16 worlds at 64x64, each a floor and 8 icospheres (320 triangles) placed by matrices.
 - `body_worlds`: 4096 worlds at 64x64, 20 simulator bodies each carrying one instance of three shared
   meshes (icosphere 1280, box 12, capped cylinder 512 triangles), moved by a Gaussian random walk.
+- `large_world`: one world of 100,000 instances of five meshes at 1280x720, with a 64 x 2048 LiDAR sweep.
 """
 
 from __future__ import annotations
@@ -119,6 +120,47 @@ def body_worlds(worlds=4096, bodies=20, width=64, height=64, seed=0) -> Workload
     return Workload("body_worlds", desc, cams, 1.0, 1, binding=binding, poses=poses,
                     info={"worlds": worlds, "bodies": bodies, "width": width, "height": height, "seed": seed,
                           "triangles": [1280, 12, 512]})
+
+
+def large_world(instances=100_000, width=1280, height=720, seed=0, frames=1) -> Workload:
+    """One world of 100,000 instances of five meshes, rendered at 1280x720 and swept by a LiDAR.
+
+    Meshes: box of half-extent 0.4 (12 triangles), icosphere radius 0.5 subdivision 2 (320), capped cylinder
+    radius 1 half-height 1 with 128 segments (512) at scale (0.3, 0.3, 0.5), icosphere subdivision 3 (1280),
+    icosphere subdivision 5 (20480); instance i uses mesh i % 5. Positions uniform in the box
+    [-100, 100] x [-10, 10] x [-100, 100], rotations uniform on S^3, drawn afresh every frame (matrices:
+    (frames, 1, instances, 3, 4)). Floor y = -11, half-extent 120, z in (-120, 120), checker 1. Camera at
+    (0, 2, -100) looking at the origin, fov 1.0 rad. Light as in icosphere_worlds. info["lidar"]: 64
+    elevations in [-15, 15] degrees x 2048 azimuths from the scene centre, max range 150.
+    """
+    rng = np.random.default_rng(seed)
+    meshes = [make_box((0.4, 0.4, 0.4)), make_icosphere(0.5, 2), cylinder(1.0, 1.0, 128), make_icosphere(0.5, 3),
+              make_icosphere(0.5, 5)]
+    insts = [Instance(i % 5, material=Material(diffuse_color=PALETTE[i % len(PALETTE)])) for i in range(instances)]
+    floor = Plane(y=-11.0, half_extent_x=120.0, z_min=-120.0, z_max=120.0, checker_scale=1.0)
+    desc = SceneDesc(width, height, 1, 1, lights=[LIGHT], floor=floor, meshes=meshes, instances=insts)
+    mats = np.empty((frames, 1, instances, 3, 4), np.float32)
+    scale = np.ones((instances, 3))
+    scale[2::5] = (0.3, 0.3, 0.5)
+    for f in range(frames):
+        pos = rng.uniform((-100.0, -10.0, -100.0), (100.0, 10.0, 100.0), size=(instances, 3))
+        q = uniform_quaternions(rng, instances)
+        x, y, z, w = q.T
+        r = np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                      2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                      2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1).reshape(instances, 3, 3)
+        mats[f, 0, :, :, :3] = r * scale[:, None, :]
+        mats[f, 0, :, :, 3] = pos
+    cams = camera_matrix((0.0, 2.0, -100.0), (0.0, 0.0, 0.0), width, height, 1.0)[None]
+    el = np.radians(np.linspace(-15.0, 15.0, 64))
+    az = np.radians(np.linspace(0.0, 360.0, 2048, endpoint=False))
+    e, a = np.meshgrid(el, az, indexing="ij")
+    dirs = np.stack([np.cos(e) * np.sin(a), np.sin(e), np.cos(e) * np.cos(a)], -1).reshape(1, -1, 3).astype(np.float32)
+    origins = np.zeros_like(dirs)
+    return Workload("large_world", desc, cams.astype(np.float32), 1.0, 1, matrices=mats,
+                    info={"instances": instances, "width": width, "height": height, "seed": seed,
+                          "triangles": [12, 320, 512, 1280, 20480], "lidar": {"origins": origins, "directions": dirs,
+                                                                             "max_distance": 150.0}})
 
 
 def quat_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:

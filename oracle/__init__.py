@@ -227,6 +227,8 @@ def ref_lib(cuda=False):
                                      C.POINTER(_abi.BatchFrameC)]
         lib.ngref_cast_rays_host.argtypes = [C.c_void_p, _f32p, _f32p, C.c_int, C.c_int, C.c_float, _f32p, _f32p,
                                              C.POINTER(C.c_int32)]
+        if hasattr(lib, "ngref_cast_rays_device"):
+            lib.ngref_cast_rays_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float]
         lib.ngref_last_kernel_ms.restype = C.c_float
         lib.ngref_last_kernel_ms.argtypes = [C.c_void_p]
         lib.ngref_device.argtypes = [C.c_void_p]
@@ -315,6 +317,11 @@ class Reference:
         _ref_check(self.lib, self.lib.ngref_render(self.h, C.c_void_p(camera_ptr), float(fov), int(spp), int(outputs),
                                                    int(frame), 1, C.byref(f)))
         return f
+
+    def cast_rays_device(self, origin_ptr, direction_ptr, rays_per_world, max_distance):
+        """Rays already in device memory (CUDA reference only); the hits stay on the device."""
+        _ref_check(self.lib, self.lib.ngref_cast_rays_device(self.h, C.c_void_p(origin_ptr), C.c_void_p(direction_ptr),
+                                                             int(rays_per_world), float(max_distance)))
 
     def cast_rays(self, origins, directions, max_distance=np.inf):
         o = np.ascontiguousarray(origins, np.float32)

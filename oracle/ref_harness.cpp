@@ -228,6 +228,17 @@ int ngref_cast_rays_host(void *h, const float *origins, const float *directions,
     }
 }
 
+// BatchRenderer::cast_rays with the rays in device memory; the hits stay in the renderer's device buffers.
+int ngref_cast_rays_device(void *h, const float *origins, const float *directions, int rays_per_world,
+    float max_distance) {
+    try {
+        static_cast<Handle *>(h)->batch->cast_rays(origins, directions, rays_per_world, max_distance, Memory::Device);
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
 float ngref_last_kernel_ms(void *h) { return static_cast<Handle *>(h)->batch->last_kernel_ms(); }
 
 int ngref_device(void *h) { return static_cast<Handle *>(h)->batch->device() == Device::Cuda ? 1 : 0; }
