@@ -48,9 +48,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
-    p.add_argument("--config", default="body_worlds", choices=["body_worlds", "large_world"],
+    p.add_argument("--config", default="body_worlds", choices=["body_worlds", "large_world", "differentiable"],
                    help="body_worlds: the headline (4096 worlds x 64x64); large_world: one world of 100,000 "
-                        "instances at 1280x720 with a 64 x 2048 LiDAR sweep, poses redrawn every frame")
+                        "instances at 1280x720 with a 64 x 2048 LiDAR sweep, poses redrawn every frame; "
+                        "differentiable: 1024 worlds x 128x128 depth+normals, forward+backward against forward")
     p.add_argument("--profile", action="store_true",
                    help="device-resident steps only (no autotune, e2e, CPU or reference arms): for ncu captures")
     return p.parse_args()
@@ -447,6 +448,88 @@ def run_large(args, rank, world, local_rank, dist):
     }
 
 
+def run_differentiable(args, rank, world, local_rank, dist):
+    """1024 worlds x 128x128, 12 instances: an L2 depth loss against a target rendered from perturbed poses.
+    Forward only = poses -> matrices -> render depth + normals -> loss; forward + backward adds the hit
+    records, the adjoint kernel and autograd back to positions, quaternions and cameras. Both timed per step
+    with CUDA events; the ratio is the metric."""
+    import torch
+
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+    from neraulgraphics_b200.autodiff import pose_matrices, render_depth_normals
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    wl = workloads.differentiable_worlds(worlds=1024, seed=rank)
+    d, info = wl.desc, wl.info
+    r = ng.BatchRenderer(d.width, d.height, d.world_count, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances,
+                         device=dev)
+    T = lambda a: torch.from_numpy(a).to(dev)
+    pos, quat, scale, cams = T(info["positions"]), T(info["quaternions"]), T(info["scales"]), T(wl.cameras)
+    with torch.no_grad():
+        target = render_depth_normals(r, pose_matrices(T(info["target_positions"]), T(info["target_quaternions"]),
+                                                       scale), cams, wl.fov)[0].clone()
+    ok = torch.isfinite(target)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def forward():
+        with torch.no_grad():
+            r.set_instance_transforms(pose_matrices(pos, quat, scale).contiguous())
+            out = r.render(cams, wl.fov, 1, rgb=False, depth=True, normals=True, zero_copy=True)
+            dep = out["depth"]
+            return (torch.where(ok & torch.isfinite(dep), dep - target, 0.0) ** 2).sum()
+
+    p, q, c = pos.clone().requires_grad_(), quat.clone().requires_grad_(), cams.clone().requires_grad_()
+
+    def forward_backward():
+        p.grad = q.grad = c.grad = None
+        dep = render_depth_normals(r, pose_matrices(p, q, scale), c, wl.fov)[0]
+        loss = (torch.where(ok & torch.isfinite(dep), dep - target, 0.0) ** 2).sum()
+        loss.backward()
+        return loss
+
+    def timed(fn):
+        for _ in range(W):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(K):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    with ClockSampler(local_rank) as clocks:
+        fwd_ms = timed(forward)
+        fb_ms = timed(forward_backward)
+    r.set_instance_transforms(pose_matrices(pos, quat, scale).detach().contiguous())
+    forward_backward()
+    adj_ms = r.last_kernel_ms
+    if rank != 0:
+        return None
+    views = d.view_count
+    return {
+        "metric": "forward+backward time / forward-only time at 1024 worlds x 128x128 depth+normals (L2 depth loss)",
+        "value": round(fb_ms / fwd_ms, 4), "unit": "ratio", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(fb_ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded differentiable_worlds scene and perturbed target poses)",
+        "config": {"workload": "differentiable_worlds: 1024 worlds x 12 instances (icosphere 1280 / box 12 tris), "
+                               "128x128, depth+normals, target poses N(0, 0.01) position and 0.02 rad rotation",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "forward_ms": round(fwd_ms, 4), "forward_backward_ms": round(fb_ms, 4), "adjoint_kernel_ms": round(adj_ms, 4),
+        "forward_images_per_s": round(views / (fwd_ms / 1000.0), 1),
+        "forward_backward_images_per_s": round(views / (fb_ms / 1000.0), 1),
+        "gradient_check": "float64 reference and central differences within 1e-3 (tests/test_gpu_adjoint.py)",
+        "clocks": clocks.summary(),
+    }
+
+
 def reference_cuda_large(wl, torch, mats, cams, lo, ld, steps, warmup):
     """The reference's CUDA backend on the same large-world frames, inputs on the device: ms per stage."""
     import oracle as O
@@ -535,7 +618,8 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device(f"cuda:{local_rank}"))
-        line = (run_large if args.config == "large_world" else run_ours)(args, rank, world, local_rank, dist)
+        run = {"body_worlds": run_ours, "large_world": run_large, "differentiable": run_differentiable}[args.config]
+        line = run(args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()
     if line is not None:

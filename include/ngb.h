@@ -306,6 +306,24 @@ float ngb_last_kernel_ms(const ngb_renderer *r);
  * written. No counterpart in the reference, which times the render as one launch. */
 int ngb_last_stage_ms(ngb_renderer *r, float *ms, int32_t capacity, int32_t *count);
 
+/* ---- differentiation ------------------------------------------------------------------------------- */
+
+/* Copies the last render's hit records (ngb_record_hits) into device arrays of view_count x height x width:
+ * the centre ray's instance (-1 when it hit no mesh), its triangle in its mesh's own list, and barycentrics.
+ * Any pointer may be NULL. No counterpart in the reference. */
+int ngb_copy_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *u, float *v);
+
+/* The adjoint of the depth and normal images: adds d(loss)/d(instance matrices) to grad_matrices (world-major,
+ * 12 floats each, the layout of ngb_set_instance_transforms) and d(loss)/d(cameras) to grad_cameras (12 floats
+ * per view), given d(loss)/d(depth) (grad_depth, one float per pixel) and d(loss)/d(normals) (grad_normal, 3
+ * per pixel, or NULL). Visibility is held fixed: each pixel's recorded hit (from ngb_copy_hits after a render
+ * with hit records on) moves with its instance, and the camera rays move with the cameras. matrices, cameras,
+ * fov and depth must be those of that render. Every pointer is device memory. No counterpart in the
+ * reference, which has no derivatives. */
+int ngb_depth_normal_adjoint(ngb_renderer *r, const float *matrices, const float *cameras, float fov,
+    const int32_t *hit_instance, const int32_t *hit_triangle, const float *hit_u, const float *hit_v, const float *depth,
+    const float *grad_depth, const float *grad_normal, float *grad_matrices, float *grad_cameras);
+
 /* ---- inspection, for parity checks ------------------------------------------------------------------ */
 
 /* Copies the last tree build to host arrays (any may be NULL): the sort keys (world << 32 | Morton

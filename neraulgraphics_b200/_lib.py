@@ -67,6 +67,8 @@ def lib():
     L.ngb_build_tlas_noalloc.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
+    L.ngb_copy_hits.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.ngb_depth_normal_adjoint.argtypes = [_vp, _vp, _vp, C.c_float] + [_vp] * 9
     L.ngb_srgb_thresholds.argtypes = [_vp]
     L.ngb_record_hits.argtypes = [_vp, C.c_int32]
     L.ngb_inspect_tlas.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]

@@ -119,4 +119,29 @@ constexpr int TILE_MAX_INSTANCES = 32;
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade);
 
+// The adjoint of the depth and normal images (see adjoint.cu). Every pointer is device memory; grad_normal
+// may be null; the gradients are added to grad_matrices and grad_cameras.
+struct AdjointArgs {
+    const float *matrices;         // instances x 12: world-from-mesh, as the forward render saw them
+    const float *cameras;          // views x 12: camera-to-world
+    float fov_scale;
+    float aspect;
+    int width;
+    int height;
+    int cameras_per_world;
+    int views;
+    const int32_t *hit_instance;   // per pixel: the centre ray's hit, -1 for none or not a mesh
+    const int32_t *hit_triangle;   // triangle index in its mesh's own list
+    const float *hit_u;
+    const float *hit_v;
+    const float *depth;
+    const float *grad_depth;       // per pixel
+    const float *grad_normal;      // per pixel, 3, or null
+    float *grad_matrices;          // instances x 12
+    float *grad_cameras;           // views x 12
+    const int *tri_of_local;       // packed triangle of (mesh's first packed triangle + index in its mesh)
+    const int *slot_tri_base;      // per slot: its mesh's first packed triangle
+};
+cudaError_t launch_depth_normal_adjoint(const SceneParams &s, const AdjointArgs &a, cudaStream_t stream);
+
 }  // namespace ngb

@@ -96,6 +96,7 @@ struct Renderer {
     // The scene: shared meshes and what each slot of a world holds.
     DevBuf<float4> blas, tris, attrs;
     DevBuf<int> tri_index, slot_blas_root;
+    DevBuf<int> tri_of_local, slot_tri_base;  // a mesh-local triangle's packed index, for the adjoint
     DevBuf<float> slot_bounds;
     DevBuf<DevMaterial> slot_material;
     // Per build.
@@ -268,6 +269,14 @@ Renderer::Renderer(const ngb_scene &s) {
     upload(tris, built.triangles);
     if (!built.attributes.empty()) upload(attrs, built.attributes);
     upload(tri_index, built.triangle_index);
+    // Each mesh's triangles are packed together, from its first packed triangle on (in leaf order), so a
+    // mesh-local triangle index finds its packed triangle through one table.
+    std::vector<int> mesh_base(s.mesh_count + 1, 0);
+    for (int m = 0; m < s.mesh_count; ++m) mesh_base[m + 1] = mesh_base[m] + s.meshes[m].index_count / 3;
+    std::vector<int> local_to_packed(built.triangle_index.size());
+    for (int m = 0; m < s.mesh_count; ++m)
+        for (int p = mesh_base[m]; p < mesh_base[m + 1]; ++p) local_to_packed[mesh_base[m] + built.triangle_index[p]] = p;
+    upload(tri_of_local, local_to_packed);
     std::vector<int> root_of_slot(per_world);
     std::vector<float> bounds_of_slot(6 * static_cast<size_t>(per_world));
     std::vector<DevMaterial> material_of_slot(per_world);
@@ -278,6 +287,9 @@ Renderer::Renderer(const ngb_scene &s) {
         material_of_slot[i] = dev_material(s.instances[i].material);
     }
     upload(slot_blas_root, root_of_slot);
+    std::vector<int> tri_base_of_slot(per_world);
+    for (int i = 0; i < per_world; ++i) tri_base_of_slot[i] = mesh_base[s.instances[i].mesh];
+    upload(slot_tri_base, tri_base_of_slot);
     upload(blas_pairs, built.pairs);
     std::vector<int2> root_ref_of_slot(per_world);
     for (int i = 0; i < per_world; ++i) {
@@ -339,6 +351,7 @@ Renderer::~Renderer() {
     if (own_stream) cudaStreamDestroy(own_stream);
     // The DevBufs free themselves; the device must be current while they do, so release them here.
     blas.release(), tris.release(), attrs.release(), tri_index.release(), slot_blas_root.release();
+    tri_of_local.release(), slot_tri_base.release();
     slot_bounds.release(), slot_material.release(), matrices.release(), inst.release(), tlas.release();
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
@@ -940,6 +953,54 @@ int ngb_inspect_tlas(ngb_renderer *h, uint64_t *keys, int32_t *sorted_ids, int32
         if (nodes) CK(cudaMemcpy(nodes, r.tlas.p, (2 * n - 1) * 32, cudaMemcpyDeviceToHost));
         if (roots) CK(cudaMemcpy(roots, r.roots.p, r.worlds * sizeof(int32_t), cudaMemcpyDeviceToHost));
         if (matrices) CK(cudaMemcpy(matrices, r.matrices.p, n * 48, cudaMemcpyDeviceToHost));
+    });
+}
+
+int ngb_copy_hits(ngb_renderer *h, int32_t *instance, int32_t *triangle, float *u, float *v) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(r.hit_instance.p != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
+        const size_t px = r.pixels() * 4;
+        if (instance) CK(cudaMemcpyAsync(instance, r.hit_instance.p, px, cudaMemcpyDeviceToDevice, r.stream));
+        if (triangle) CK(cudaMemcpyAsync(triangle, r.hit_triangle.p, px, cudaMemcpyDeviceToDevice, r.stream));
+        if (u) CK(cudaMemcpyAsync(u, r.hit_u.p, px, cudaMemcpyDeviceToDevice, r.stream));
+        if (v) CK(cudaMemcpyAsync(v, r.hit_v.p, px, cudaMemcpyDeviceToDevice, r.stream));
+        r.finish();
+    });
+}
+
+int ngb_depth_normal_adjoint(ngb_renderer *h, const float *matrices, const float *cameras, float fov,
+    const int32_t *hit_instance, const int32_t *hit_triangle, const float *hit_u, const float *hit_v, const float *depth,
+    const float *grad_depth, const float *grad_normal, float *grad_matrices, float *grad_cameras) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(matrices && cameras && hit_instance && hit_triangle && hit_u && hit_v && depth && grad_depth &&
+            grad_matrices && grad_cameras, "only grad_normal may be null");
+        ngb::require(fov > 0.0f && fov < 3.14159265f, "fov must be between 0 and pi radians");
+        ngb::AdjointArgs a{};
+        a.matrices = matrices;
+        a.cameras = cameras;
+        a.fov_scale = std::tan(fov * 0.5f);
+        a.aspect = static_cast<float>(r.width) / static_cast<float>(r.height);
+        a.width = r.width;
+        a.height = r.height;
+        a.cameras_per_world = r.cpw;
+        a.views = r.worlds * r.cpw;
+        a.hit_instance = hit_instance;
+        a.hit_triangle = hit_triangle;
+        a.hit_u = hit_u;
+        a.hit_v = hit_v;
+        a.depth = depth;
+        a.grad_depth = grad_depth;
+        a.grad_normal = grad_normal;
+        a.grad_matrices = grad_matrices;
+        a.grad_cameras = grad_cameras;
+        a.tri_of_local = r.tri_of_local.p;
+        a.slot_tri_base = r.slot_tri_base.p;
+        CK(cudaEventRecord(r.ev_start, r.stream));
+        CK(ngb::launch_depth_normal_adjoint(r.params, a, r.stream));
+        CK(cudaEventRecord(r.ev_stop, r.stream));
+        r.stages = 1;
+        r.timing_pending = true;
+        r.finish();
     });
 }
 

@@ -331,6 +331,24 @@ class BatchRenderer:
         check(self._lib.ngb_inspect_tlas(self._h, vp(keys), vp(ids), vp(nodes), vp(roots), vp(mats)), self._h)
         return {"keys": keys, "sorted_ids": ids, "nodes": nodes, "roots": roots, "matrices": mats}
 
+    def copy_hits(self, instance, triangle, u, v):
+        """Copies the last render's hit records into CUDA tensors of (views, height, width): int32 instance and
+        triangle, float32 barycentrics (see ngb_copy_hits)."""
+        ptr = lambda t: C.c_void_p(t.data_ptr())
+        self._stream()
+        check(self._lib.ngb_copy_hits(self._h, ptr(instance), ptr(triangle), ptr(u), ptr(v)), self._h)
+
+    def depth_normal_adjoint(self, matrices, cameras, fov, hits, depth, grad_depth, grad_normal, grad_matrices,
+                             grad_cameras):
+        """Adds the gradients of the depth and normal images with respect to the instance matrices and the
+        cameras into grad_matrices and grad_cameras (see ngb_depth_normal_adjoint). CUDA tensors throughout;
+        hits = (instance, triangle, u, v) from copy_hits; grad_normal may be None."""
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(None)
+        self._stream()
+        check(self._lib.ngb_depth_normal_adjoint(self._h, ptr(matrices), ptr(cameras), float(fov), *map(ptr, hits),
+                                                 ptr(depth), ptr(grad_depth), ptr(grad_normal), ptr(grad_matrices),
+                                                 ptr(grad_cameras)), self._h)
+
     def inspect_hits(self) -> dict:
         shape = (self.view_count, self.height, self.width)
         inst, tri = np.zeros(shape, np.int32), np.zeros(shape, np.int32)

@@ -7,6 +7,7 @@ on. Every generator is deterministic in its seed (numpy's default_rng).
 - `icosphere_worlds`: 16 worlds at 64x64, each a floor and 8 icospheres (320 triangles) placed by matrices.
 - `body_worlds`: 4096 worlds at 64x64, 20 simulator bodies each carrying one instance of three shared
   meshes (icosphere 1280, box 12, capped cylinder 512 triangles), moved by a Gaussian random walk.
+- `differentiable_worlds`: 1024 worlds at 128x128 of 12 icospheres and boxes, with target poses, for the adjoint.
 - `large_world`: one world of 100,000 instances of five meshes at 1280x720, with a 64 x 2048 LiDAR sweep.
 """
 
@@ -120,6 +121,53 @@ def body_worlds(worlds=4096, bodies=20, width=64, height=64, seed=0) -> Workload
     return Workload("body_worlds", desc, cams, 1.0, 1, binding=binding, poses=poses,
                     info={"worlds": worlds, "bodies": bodies, "width": width, "height": height, "seed": seed,
                           "triangles": [1280, 12, 512]})
+
+
+def differentiable_worlds(worlds=1024, per_world=12, width=128, height=128, seed=0) -> Workload:
+    """1024 worlds at 128x128, depth and normals, for the adjoint: 12 instances each of an icosphere (radius 0.5,
+    subdivision 3, 1280 triangles, smooth normals) and a box (half-extent 0.4, 12 triangles), alternating.
+
+    Per instance: position U[-2, 2]^3 + (0, 0, -6), rotation uniform on S^3, uniform scale U[0.6, 1.2]. Floor
+    y = -2.5, half-extent 12, z in (-30, -2). One camera per world at (0, 1, 0) + U[-0.2, 0.2]^3 aimed at
+    (0, 0, -6), fov 1.0 rad. The target: the same scene with positions moved by N(0, 0.01^2) and each rotation
+    turned by an angle N(0, 0.02^2) about a random axis. info holds positions (W, N, 3), quaternions (W, N, 4),
+    scales (W, N, 3) and the target's positions and quaternions; matrices are the poses' (W, N, 3, 4).
+    """
+    rng = np.random.default_rng(seed)
+    meshes = [make_icosphere(0.5, 3), make_box((0.4, 0.4, 0.4))]
+    instances = [Instance(i % 2, material=Material(diffuse_color=PALETTE[i % len(PALETTE)])) for i in range(per_world)]
+    floor = Plane(y=-2.5, half_extent_x=12.0, z_min=-30.0, z_max=-2.0, checker_scale=0.0)
+    desc = SceneDesc(width, height, worlds, 1, lights=[LIGHT], floor=floor, meshes=meshes, instances=instances)
+    pos = (rng.uniform(-2.0, 2.0, size=(worlds, per_world, 3)) + np.array([0.0, 0.0, -6.0])).astype(np.float32)
+    quat = uniform_quaternions(rng, worlds * per_world).reshape(worlds, per_world, 4).astype(np.float32)
+    scale = np.repeat(rng.uniform(0.6, 1.2, size=(worlds, per_world, 1)), 3, axis=-1).astype(np.float32)
+    tpos = (pos + rng.normal(0.0, 0.01, size=pos.shape)).astype(np.float32)
+    axis = rng.normal(size=pos.shape)
+    axis /= np.linalg.norm(axis, axis=-1, keepdims=True)
+    ang = rng.normal(0.0, 0.02, size=pos.shape[:-1] + (1,))
+    tquat = quat_mul(quat.astype(np.float64), np.concatenate([axis * np.sin(ang / 2), np.cos(ang / 2)], -1))
+    tquat = (tquat / np.linalg.norm(tquat, axis=-1, keepdims=True)).astype(np.float32)
+    cams = np.empty((worlds, 3, 4), np.float32)
+    for w in range(worlds):
+        eye = np.array([0.0, 1.0, 0.0]) + rng.uniform(-0.2, 0.2, size=3)
+        cams[w] = camera_matrix(eye, (0.0, 0.0, -6.0), width, height, 1.0)
+    return Workload("differentiable_worlds", desc, cams, 1.0, 1, rgb=False, depth=True, normals=True, object_ids=False,
+                    matrices=pose_matrices_np(pos, quat, scale),
+                    info={"worlds": worlds, "per_world": per_world, "width": width, "height": height, "seed": seed,
+                          "positions": pos, "quaternions": quat, "scales": scale, "target_positions": tpos,
+                          "target_quaternions": tquat})
+
+
+def pose_matrices_np(pos, quat, scale) -> np.ndarray:
+    """[R(q) diag(s) | p] in float32, q normalised first (the arithmetic of autodiff.pose_matrices)."""
+    q = quat.astype(np.float32)
+    q = q / np.sqrt((q * q).sum(-1, keepdims=True))
+    x, y, z, w = np.moveaxis(q, -1, 0)
+    r = np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w),
+                  2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w),
+                  2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)
+    r = r.reshape(q.shape[:-1] + (3, 3)) * scale[..., None, :]
+    return np.concatenate([r, pos[..., None]], -1).astype(np.float32)
 
 
 def large_world(instances=100_000, width=1280, height=720, seed=0, frames=1) -> Workload:

@@ -244,3 +244,17 @@ def test_srgb_threshold_table_reproduces_the_host_mapping_for_every_float():
     table = np.zeros(256, np.float32)
     assert lib().ngb_srgb_thresholds(table.ctypes.data_as(ctypes.c_void_p)) == 0
     assert np.array_equal(bits(table), bits(first))
+
+
+def test_pose_matrices_agree_between_torch_and_numpy():
+    """autodiff.pose_matrices (torch, differentiable) and workloads.pose_matrices_np make the same matrices."""
+    import torch
+
+    from neraulgraphics_b200.autodiff import pose_matrices
+    wl = workloads.differentiable_worlds(worlds=3, width=16, height=16)
+    i = wl.info
+    t = pose_matrices(torch.from_numpy(i["positions"]), torch.from_numpy(i["quaternions"]), torch.from_numpy(i["scales"]))
+    assert np.abs(t.numpy() - wl.matrices).max() <= 1e-6
+    q = torch.from_numpy(i["quaternions"][0, :2]).double().requires_grad_()
+    p = torch.from_numpy(i["positions"][0, :2]).double()
+    assert torch.autograd.gradcheck(lambda qq: pose_matrices(p, qq), (q,))
