@@ -1,6 +1,6 @@
 """Picks the render kernel's launch shape for a workload by timing it.
 
-For worlds of at most 32 instances the tile kernel runs, and its shape is the CTA size and the register
+For worlds of at most 256 instances the tile kernel runs, and its shape is the CTA size and the register
 budget per thread (which sets how many warps an SM holds). Otherwise the persistent kernel runs, and its
 shape adds the refill threshold (how many of a warp's lanes must be free before it takes new pixels) and the
 leaf batch. The best depends on the scene (how long rays walk, how much they vary), so it is measured on the
@@ -19,8 +19,8 @@ import time
 
 CANDIDATES = [(threads, regs, refill, batch) for threads, regs in ((128, 64), (256, 64), (128, 48), (64, 64))
               for refill in (16, 24, 28) for batch in (1, 8, 16, 24)]
-TILE_CANDIDATES = [(128, 64, 0, 0), (128, 80, 0, 0), (128, 96, 0, 0), (256, 64, 0, 0), (256, 80, 0, 0)]
-TILE_MAX_INSTANCES = 32
+TILE_CANDIDATES = [(128, 64, 0, 0), (128, 80, 0, 0), (256, 64, 0, 0)]
+TILE_MAX_INSTANCES = 256
 
 
 def cache_path() -> str:

@@ -35,17 +35,21 @@ constexpr int TILE_W = 8, TILE_H = 4;
 constexpr int WALK_STACK = 64;      // a mesh's tree is at most 60 deep
 constexpr int TILES_PER_FETCH = 4;  // tiles a warp takes with one atomic
 
-// A world instance as a warp holds it while it renders a tile: its world box, the instance, and the distance
-// below which no camera ray of the tile can enter the box.
-struct TileBox {
-    float4 lo;  // xyz, w: instance (int bits)
-    float4 hi;  // xyz, w: entry bound
+// A tile's candidate instances as its warp holds them: each one's position in its world's run of sorted
+// leaves and the distance below which no camera ray of the tile can enter its box, collected in leaf order,
+// then sorted by that distance. CAP: the most instances a world holds (32 or TILE_MAX_INSTANCES).
+template <int CAP>
+struct WarpSmem {
+    int leaf[CAP];           // sorted: the candidates' leaves, smallest entry bound first
+    float bound[CAP];        // and their bounds
+    int leaf_in[CAP];        // collected, in leaf order
+    float bound_in[CAP];
 };
 
-struct WarpSmem {
-    TileBox box[TILE_MAX_INSTANCES];
-    int order[TILE_MAX_INSTANCES];  // the camera rays' candidates, smallest entry bound first
-};
+// A world's run of sorted leaves: leaf k of world w is node n - 1 + first + k.
+__device__ __forceinline__ const float4 *world_leaves(const SceneParams &s, int world) {
+    return s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + static_cast<long long>(world) * s.per_world);
+}
 
 // An instance's leaf as the world tree's walk handles it once the ray has passed the leaf's box: the ray
 // moved to mesh space and the mesh root's box test (blas_walk, src/mesh_dev.h:164-175), then the mesh's tree
@@ -140,15 +144,18 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
 
 // A camera ray's closest mesh hit over the tile's candidates, visited by the whole warp in the same order.
 // The warp stops once no lane's closest hit lies beyond the next candidate's entry bound.
-__device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpSmem &sm, int ncand, bool active,
-    float3 o, float3 d, float &tmax, int &hit_inst, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
+template <int CAP>
+__device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpSmem<CAP> &sm, const float4 *leaves,
+    int ncand, bool active, float3 o, float3 d, float &tmax, int &hit_inst, int &hit_tri, float &hu, float &hv,
+    int max_steps, int *err) {
     const float3 inv = safe_inverse(d);
     for (int c = 0; c < ncand; ++c) {
-        const TileBox b = sm.box[sm.order[c]];
-        const bool reach = active && b.hi.w < tmax;
+        const bool reach = active && sm.bound[c] < tmax;
         if (!__any_sync(FULL, reach)) break;
-        if (reach && box_entry(b.lo, b.hi, o, inv, tmax) < NO_HIT) {
-            const int id = __float_as_int(b.lo.w);
+        const float4 *leaf = leaves + 2 * sm.leaf[c];
+        const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
+        if (reach && box_entry(lo, hi, o, inv, tmax) < NO_HIT) {
+            const int id = ~__float_as_int(lo.w);
             if (instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, false, hit_tri,
                     hu, hv, max_steps, err))
                 hit_inst = id;
@@ -268,14 +275,14 @@ constexpr int CODE_NONE = -1, CODE_FLOOR = -2, CODE_SPHERE = -3;
 // Camera kernel. THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget. Per tile: the
 // candidates, then the centre rays (depth, normals, IDs written here) and the picture rays (their closest
 // hits written for the shade kernel).
-template <int THREADS, int MIN_BLOCKS>
+template <int THREADS, int MIN_BLOCKS, int CAP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
-    __shared__ WarpSmem warp_smem[THREADS / 32];
-    WarpSmem &sm = warp_smem[threadIdx.x >> 5];
+    __shared__ WarpSmem<CAP> warp_smem[THREADS / 32];
+    WarpSmem<CAP> &sm = warp_smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const int P = s.instance_count > 0 ? s.per_world : 0;
-    const long long first_leaf = s.tlas_internal;  // leaf k of the sorted leaves is node n - 1 + k
     const int max_steps = s.blas_node_count + 2;
     const bool want_aov = a.depth || a.normal || a.object_id || a.hit_instance;
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
@@ -303,46 +310,61 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
             const float sy_hi = fmaxf(sya, syb) + 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
 
-            __syncwarp();
-            bool cand = false;
-            float bound = 0.0f;
-            if (lane < P) {
-                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(T.world) * P + lane);
-                const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
-                const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
-                const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
-                const float3 rel = c - eye;
-                const float pad = 1e-4f * (fabsf(rel.x) + fabsf(rel.y) + fabsf(rel.z) + h.x + h.y + h.z) + 1e-4f;
-                const float3 k00 = right * sx_lo + up * sy_lo + fwd, k10 = right * sx_hi + up * sy_lo + fwd;
-                const float3 k11 = right * sx_hi + up * sy_hi + fwd, k01 = right * sx_lo + up * sy_hi + fwd;
-                const float3 mid = k00 + k11;
-                const float3 edges[4][2] = {{k00, k10}, {k10, k11}, {k11, k01}, {k01, k00}};
-                cand = true;
+            // Every instance of the world against the pyramid, 32 at a time: the candidates, in leaf order.
+            const float4 *leaves = world_leaves(s, T.world);
+            const float3 k00 = right * sx_lo + up * sy_lo + fwd, k10 = right * sx_hi + up * sy_lo + fwd;
+            const float3 k11 = right * sx_hi + up * sy_hi + fwd, k01 = right * sx_lo + up * sy_hi + fwd;
+            const float3 mid = k00 + k11;
+            float3 planes[4] = {cross(k00, k10), cross(k10, k11), cross(k11, k01), cross(k01, k00)};
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    float3 n = cross(edges[e][0], edges[e][1]);
-                    if (dot(n, mid) < 0.0f) n = -n;
-                    const float reach = dot(n, rel) + abs_dot(n, h) + pad * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
-                    if (reach < 0.0f) cand = false;
+            for (int e = 0; e < 4; ++e)
+                if (dot(planes[e], mid) < 0.0f) planes[e] = -planes[e];
+            __syncwarp();
+            int ncand = 0;
+            for (int base = 0; base < P; base += 32) {
+                const int j = base + lane;
+                bool cand = false;
+                float bound = 0.0f;
+                if (j < P) {
+                    const float4 lo = __ldg(leaves + 2 * j), hi = __ldg(leaves + 2 * j + 1);
+                    const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+                    const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
+                    const float3 rel = c - eye;
+                    const float pad = 1e-4f * (fabsf(rel.x) + fabsf(rel.y) + fabsf(rel.z) + h.x + h.y + h.z) + 1e-4f;
+                    cand = true;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float3 n = planes[e];
+                        const float reach = dot(n, rel) + abs_dot(n, h) + pad * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
+                        if (reach < 0.0f) cand = false;
+                    }
+                    // No ray of the tile can enter the box closer than the eye's distance to it (the rays are
+                    // unit length); the bound sits 1e-5 below that, far beyond the slab test's rounding.
+                    const float dx = fmaxf(fmaxf(lo.x - eye.x, eye.x - hi.x), 0.0f);
+                    const float dy = fmaxf(fmaxf(lo.y - eye.y, eye.y - hi.y), 0.0f);
+                    const float dz = fmaxf(fmaxf(lo.z - eye.z, eye.z - hi.z), 0.0f);
+                    bound = sqrtf(dx * dx + dy * dy + dz * dz) * 0.99999f;
                 }
-                // No ray of the tile can enter the box closer than the eye's distance to it (the rays are unit
-                // length); the bound sits 1e-5 below that, far beyond the slab test's rounding.
-                const float dx = fmaxf(fmaxf(lo.x - eye.x, eye.x - hi.x), 0.0f);
-                const float dy = fmaxf(fmaxf(lo.y - eye.y, eye.y - hi.y), 0.0f);
-                const float dz = fmaxf(fmaxf(lo.z - eye.z, eye.z - hi.z), 0.0f);
-                bound = sqrtf(dx * dx + dy * dy + dz * dz) * 0.99999f;
-                sm.box[lane].lo = make_float4(lo.x, lo.y, lo.z, __int_as_float(~__float_as_int(lo.w)));
-                sm.box[lane].hi = make_float4(hi.x, hi.y, hi.z, bound);
+                const unsigned cmask = __ballot_sync(FULL, cand);
+                if (cand) {
+                    const int at = ncand + __popc(cmask & below);
+                    sm.leaf_in[at] = j;
+                    sm.bound_in[at] = bound;
+                }
+                ncand += __popc(cmask);
             }
-            const unsigned cmask = __ballot_sync(FULL, cand);
-            int rank = 0;
-            for (unsigned m = cmask; m != 0; m &= m - 1) {
-                const int k = __ffs(m) - 1;
-                const float bk = __shfl_sync(FULL, bound, k);
-                rank += (bk < bound) || (bk == bound && k < lane);
+            __syncwarp();
+            // Sorted by bound (ties by leaf order): each candidate's rank is the number before it.
+            for (int i = lane; i < ncand; i += 32) {
+                const float bi = sm.bound_in[i];
+                int rank = 0;
+                for (int k = 0; k < ncand; ++k) {
+                    const float bk = sm.bound_in[k];
+                    rank += (bk < bi) || (bk == bi && k < i);
+                }
+                sm.leaf[rank] = sm.leaf_in[i];
+                sm.bound[rank] = bi;
             }
-            if (cand) sm.order[rank] = lane;
-            const int ncand = __popc(cmask);
             __syncwarp();
 
             // The centre ray for depth, normals and IDs (aov_pixel, src/render_core.h:313-327), then the picture
@@ -362,7 +384,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                 float tmax = spheres_and_floor(s, eye, d, best_sphere, hit_floor);
                 int hit_inst = -1, hit_tri = -1;
                 float hu = 0.0f, hv = 0.0f;
-                closest_meshes(s, sm, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps, a.error_flag);
+                closest_meshes(s, sm, leaves, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps,
+                    a.error_flag);
                 if (!T.pixel) continue;
                 const size_t p = static_cast<size_t>(T.pix);
                 if (pass == 1) {
@@ -496,14 +519,14 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
 // Separating axes: x, y and z, the direction away from the light, and four axes tilted from the sideways
 // directions towards the light by the light sphere's angular radius, which hug the hull's sides. Each support
 // is taken over the segments' own end points, so any axis is a valid test; these make it a tight one.
-template <int THREADS, int MIN_BLOCKS>
+template <int THREADS, int MIN_BLOCKS, int CAP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
-    __shared__ TileBox warp_box[THREADS / 32][TILE_MAX_INSTANCES];
-    TileBox *box = warp_box[threadIdx.x >> 5];
+    __shared__ int warp_cand[THREADS / 32][CAP];
+    int *cand_leaf = warp_cand[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const int P = s.instance_count > 0 ? s.per_world : 0;
-    const long long first_leaf = s.tlas_internal;
     const int max_steps = s.blas_node_count + 2;
     const DevLight &lt = s.lights[0];
     const float INF = __int_as_float(0x7f800000);
@@ -554,39 +577,45 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 for (int k = 0; k < AXES; ++k)
                     support[k] = warp_max(pending ? fmaxf(dot(axis[k], so), dot(axis[k], se)) : -INF);
             }
+            // Every instance of the world against the hull, 32 at a time: the candidates, in leaf order.
+            const float4 *leaves = world_leaves(s, T.world);
+            const float light_scale = fabsf(lt.position.x) + fabsf(lt.position.y) + fabsf(lt.position.z) + lt.radius + 1.0f;
             __syncwarp();
-            bool scand = false;
-            if (lane < P) {
-                const float4 *leaf = s.tlas + 2 * (first_leaf + static_cast<long long>(T.world) * P + lane);
-                const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
-                box[lane].lo = make_float4(lo.x, lo.y, lo.z, __int_as_float(~__float_as_int(lo.w)));
-                box[lane].hi = hi;
-                const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
-                const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
-                const float scale = fabsf(lt.position.x) + fabsf(lt.position.y) + fabsf(lt.position.z) + lt.radius +
-                    fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + h.x + h.y + h.z + 1.0f;
-                const float pad = 1e-4f * scale;
-                scand = hi.x >= mnx - pad && lo.x <= mxx + pad && hi.y >= mny - pad && lo.y <= mxy + pad &&
-                    hi.z >= mnz - pad && lo.z <= mxz + pad;
+            int ncand = 0;
+            for (int base = 0; base < P; base += 32) {
+                const int j = base + lane;
+                bool scand = false;
+                if (j < P) {
+                    const float4 lo = __ldg(leaves + 2 * j), hi = __ldg(leaves + 2 * j + 1);
+                    const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+                    const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
+                    const float pad = 1e-4f * (light_scale + fabsf(c.x) + fabsf(c.y) + fabsf(c.z) + h.x + h.y + h.z);
+                    scand = hi.x >= mnx - pad && lo.x <= mxx + pad && hi.y >= mny - pad && lo.y <= mxy + pad &&
+                        hi.z >= mnz - pad && lo.z <= mxz + pad;
 #pragma unroll
-                for (int k = 0; k < AXES; ++k) {
-                    if (k < axes && dot(axis[k], c) - abs_dot(axis[k], h) >
-                            support[k] + pad * (fabsf(axis[k].x) + fabsf(axis[k].y) + fabsf(axis[k].z)))
-                        scand = false;
+                    for (int k = 0; k < AXES; ++k) {
+                        if (k < axes && dot(axis[k], c) - abs_dot(axis[k], h) >
+                                support[k] + pad * (fabsf(axis[k].x) + fabsf(axis[k].y) + fabsf(axis[k].z)))
+                            scand = false;
+                    }
                 }
+                const unsigned cmask = __ballot_sync(FULL, scand);
+                if (scand) cand_leaf[ncand + __popc(cmask & below)] = j;
+                ncand += __popc(cmask);
             }
             __syncwarp();
             bool blocked = false;
             const float3 sinv = safe_inverse(sd);
-            for (unsigned m = __ballot_sync(FULL, scand); m != 0; m &= m - 1) {
+            for (int c = 0; c < ncand; ++c) {
                 const bool open = pending && !blocked;
                 if (!__any_sync(FULL, open)) break;
-                const TileBox b = box[__ffs(m) - 1];
-                if (open && box_entry(b.lo, b.hi, so, sinv, sdist) < NO_HIT) {
+                const float4 *leaf = leaves + 2 * cand_leaf[c];
+                const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
+                if (open && box_entry(lo, hi, so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris,
-                        __float_as_int(b.lo.w), so, sd, tm, true, ht, hu, hv, max_steps, a.error_flag);
+                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, ~__float_as_int(lo.w),
+                        so, sd, tm, true, ht, hu, hv, max_steps, a.error_flag);
                 }
             }
             if (pending) put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));
@@ -613,7 +642,7 @@ cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const
     return cudaGetLastError();
 }
 
-template <int THREADS, int MIN_BLOCKS>
+template <int THREADS, int MIN_BLOCKS, int CAP>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream,
     cudaEvent_t after_camera, cudaEvent_t after_shade) {
     const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
@@ -631,7 +660,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     }
     e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
     if (e == cudaSuccess)
-        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
+        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
             stream);
     mark(after_camera);
     if (e != cudaSuccess || !a.rgb) {
@@ -649,7 +678,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     e = cudaGetLastError();
     mark(after_shade);
     if (e != cudaSuccess || s.light_count != 1) return e;
-    return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
+    return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
         stream);
 }
 
@@ -658,12 +687,18 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade) {
     if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) return cudaErrorInvalidValue;
-    // (threads per CTA, register budget) -> the instantiation with that budget.
-    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, stream, after_camera, after_shade);
-    if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6>(s, a, counter, stream, after_camera, after_shade);
-    if (t.threads == 128 && t.registers == 96) return launch_variant<128, 5>(s, a, counter, stream, after_camera, after_shade);
-    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, stream, after_camera, after_shade);
-    if (t.threads == 256 && t.registers == 80) return launch_variant<256, 3>(s, a, counter, stream, after_camera, after_shade);
+    // (threads per CTA, register budget) -> the instantiation with that budget, and the candidate lists'
+    // capacity: 32 for worlds of up to 32 instances, else TILE_MAX_INSTANCES.
+    const bool small = s.per_world <= 32;
+    if (t.threads == 128 && t.registers == 64)
+        return small ? launch_variant<128, 8, 32>(s, a, counter, stream, after_camera, after_shade)
+                     : launch_variant<128, 8, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 128 && t.registers == 80)
+        return small ? launch_variant<128, 6, 32>(s, a, counter, stream, after_camera, after_shade)
+                     : launch_variant<128, 6, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 256 && t.registers == 64)
+        return small ? launch_variant<256, 4, 32>(s, a, counter, stream, after_camera, after_shade)
+                     : launch_variant<256, 4, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
     return cudaErrorInvalidValue;
 }
 

@@ -378,7 +378,7 @@ def test_tile_kernel_tunings_agree(torch_cuda):
     ref = r.render(wl.cameras, 1.0, 1, **out)
     ties = oracle_ties(wl.desc, wl.cameras, binding=wl.binding, poses=wl.poses)
     first = None
-    for threads, regs in ((128, 64), (128, 80), (128, 96), (256, 64), (256, 80)):
+    for threads, regs in ((128, 64), (128, 80), (256, 64)):
         r.set_tuning(kernel=3, threads_per_block=threads, registers=regs)
         got = r.render(wl.cameras, 1.0, 1, **out)
         assert_same_images(got, ref, ties=ties)
@@ -388,10 +388,10 @@ def test_tile_kernel_tunings_agree(torch_cuda):
             assert_same_images(got, first, rgb_tol=0)
 
 
-def test_tile_kernel_on_a_world_of_32_and_of_one_instance(torch_cuda):
-    """The tile kernel's limits: a world of exactly 32 instances (one per lane) and worlds of one instance,
-    whose root is their only leaf."""
-    for per_world in (32, 1):
+def test_tile_kernel_on_worlds_of_one_to_256_instances(torch_cuda):
+    """The tile kernel's cases: worlds of one instance (the root is the only leaf), exactly 32 (one per lane),
+    33 (a second chunk of candidates) and 256 (the largest it takes, eight chunks)."""
+    for per_world in (1, 32, 33, 256):
         wl = workloads.icosphere_worlds(worlds=6, per_world=per_world, width=40, height=24, seed=13)
         r, o = product(wl.desc), O.Oracle(wl.desc)
         r.set_tuning(kernel=3, threads_per_block=256, registers=64)
