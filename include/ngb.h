@@ -306,6 +306,27 @@ float ngb_last_kernel_ms(const ngb_renderer *r);
  * written. No counterpart in the reference, which times the render as one launch. */
 int ngb_last_stage_ms(ngb_renderer *r, float *ms, int32_t capacity, int32_t *count);
 
+/* ---- worlds of uneven sizes ------------------------------------------------------------------------- */
+
+/* One world of an uneven batch: its image (its one camera's) and how many instances it holds. */
+typedef struct ngb_uneven_world {
+    int32_t width;
+    int32_t height;
+    int32_t instance_count;   /* 0 to 256 */
+} ngb_uneven_world;
+
+/* Worlds of uneven instance counts and image sizes in one renderer, rendered by one launch of each tile
+ * kernel. scene gives what the worlds share (spheres, lights, floor, meshes, device) and every world's
+ * instances, world after world: scene->instances holds the sum of the worlds' instance_count entries, and
+ * scene->instance_count that sum; scene->width, height, world_count and cameras_per_world are not read.
+ * Matrices (ngb_set_instance_transforms) follow the same order. Renders take one camera per world and need one
+ * sample per pixel, at most one light and no reflective material; their images are packed world after world,
+ * each world's width x height pixels row-major (ngb_pixel_count in all). Body bindings are not supported.
+ * No counterpart in the reference, whose worlds all hold the same instances at one image size. */
+int ngb_create_uneven(const ngb_scene *scene, const ngb_uneven_world *worlds, int32_t world_count, ngb_renderer **out);
+/* Pixels of one image of every view: views x width x height, or the uneven worlds' sum. */
+int64_t ngb_pixel_count(const ngb_renderer *r);
+
 /* ---- differentiation ------------------------------------------------------------------------------- */
 
 /* Copies the last render's hit records (ngb_record_hits) into device arrays of view_count x height x width:

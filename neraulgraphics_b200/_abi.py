@@ -84,3 +84,8 @@ class BatchFrameC(C.Structure):
 class RayHitsC(C.Structure):
     _fields_ = [("memory", C.c_int32), ("device_id", C.c_int32), ("count", C.c_int32), ("distance", C.c_void_p),
                 ("normal", C.c_void_p), ("object_id", C.c_void_p)]
+
+
+class UnevenWorldC(C.Structure):
+    """ngb_uneven_world: one world of an uneven batch."""
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("instance_count", C.c_int32)]

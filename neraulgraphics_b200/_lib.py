@@ -36,6 +36,9 @@ def lib():
         raise CudaError(f"{LIB_PATH} is not built; run `python -m neraulgraphics_b200.build`")
     L = C.CDLL(LIB_PATH)
     L.ngb_create.argtypes = [C.POINTER(_abi.SceneC), C.POINTER(_vp)]
+    L.ngb_create_uneven.argtypes = [C.POINTER(_abi.SceneC), C.POINTER(_abi.UnevenWorldC), C.c_int32, C.POINTER(_vp)]
+    L.ngb_pixel_count.restype = C.c_int64
+    L.ngb_pixel_count.argtypes = [_vp]
     L.ngb_destroy.argtypes = [_vp]
     L.ngb_last_error.restype = C.c_char_p
     L.ngb_last_error.argtypes = [_vp]

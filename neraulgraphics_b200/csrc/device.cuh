@@ -92,8 +92,12 @@ struct SceneParams {
     const float4 *attrs;
     const int *tri_index;
     const DevMaterial *slot_material;
-    int instance_count;
-    int per_world;
+    int instance_count;        // over all worlds
+    int per_world;             // instances per world; the most any world holds when world_first is set
+    // Worlds of uneven instance counts: world w's instances are [world_first[w], world_first[w + 1]) and the
+    // slot tables (slot_*) hold one entry per instance. Null: world w's are [w per_world, (w + 1) per_world)
+    // and the slot tables one entry per slot of a world.
+    const int *world_first;
     int blas_node_count;  // caps a mesh-tree walk: a correct walk visits each node at most once
     // Child-pair records (both children's boxes and references in 64 bytes; see host.h and lbvh.cu):
     // every mesh node, and every world's internal LBVH nodes by their Karras index.
@@ -104,6 +108,17 @@ struct SceneParams {
     int tlas_internal;         // n - 1: nodes below this index are internal
     const float *srgb_table;   // 256 sRGB byte thresholds made on the host (see host.h: srgb_thresholds)
 };
+
+// The first instance of world w, its instance count, and the slot-table entry of its instance g.
+__device__ __forceinline__ int world_first_of(const SceneParams &s, int w) {
+    return s.world_first ? __ldg(s.world_first + w) : w * s.per_world;
+}
+__device__ __forceinline__ int world_count_of(const SceneParams &s, int w) {
+    return s.world_first ? __ldg(s.world_first + w + 1) - __ldg(s.world_first + w) : s.per_world;
+}
+__device__ __forceinline__ int table_of(const SceneParams &s, int g, int w) {
+    return s.world_first ? g : g - w * s.per_world;
+}
 
 // ---------------------------------------------------------------------------------------------- math --
 

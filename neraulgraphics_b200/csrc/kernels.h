@@ -32,6 +32,9 @@ struct BuildArgs {
     int *arrivals;                 // n - 1 counters, zero between builds
     int *error_flag;               // set nonzero if a climb runs longer than any valid tree allows
     float4 *tlas_pairs;            // (n - 1) x 4 child-pair records of the internal nodes, or null
+    // Worlds of uneven sizes (the per-world build only; per_world is then the largest): world w's instances
+    // are [world_first[w], world_first[w + 1]) and the slot tables hold one entry per instance. Null: uniform.
+    const int *world_first;
 };
 
 // Group size (threads per world) of the per-world build: a power of two, at least 32.
@@ -81,6 +84,11 @@ struct RenderArgs {
     int *pic_code;                 // its object code, then the shadowed pixel's bytes
     float4 *shadow_o;              // the shadow ray's origin and length (0: no shadow ray)
     float4 *shadow_d;              // its direction and the lit pixel's bytes
+    // Views of uneven sizes (tile kernels only): per view (width, height, first pixel, first tile), with the
+    // totals; null when every view is width x height.
+    const int4 *view_info;
+    long long total_pixels;
+    long long total_tiles;
 };
 
 // The per-view camera basis of camera_from_matrix (src/render_core.h:264-273): (position.xyz, right.x)

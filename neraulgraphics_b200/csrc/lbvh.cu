@@ -104,14 +104,25 @@ struct GroupSmem {
 // alone: keys of different worlds first differ in the world bits, so their shared prefix is clz32(w ^ wx).
 template <int G>
 __device__ __forceinline__ int delta(const GroupSmem<G> &sm, int p, long long x, long long n, long long base, int P,
-    uint32_t world, uint32_t key_p) {
+    uint32_t world, uint32_t key_p, const int *world_first, int worlds) {
     if (x < 0 || x >= n) return -1;
     if (x >= base && x < base + P) {
         const uint32_t kx = sm.key[x - base];
         if (kx == key_p) return 64 + __clz(static_cast<int>(static_cast<uint32_t>(p) ^ static_cast<uint32_t>(x)));
         return 32 + __clz(static_cast<int>(key_p ^ kx));
     }
-    const uint32_t wx = static_cast<uint32_t>(x / P);
+    uint32_t wx;
+    if (world_first) {  // uneven worlds: the last world whose first instance is at most x
+        int lo = 0, hi = worlds - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(world_first + mid) <= x) lo = mid;
+            else hi = mid - 1;
+        }
+        wx = static_cast<uint32_t>(lo);
+    } else {
+        wx = static_cast<uint32_t>(x / P);
+    }
     return __clz(static_cast<int>(world ^ wx));
 }
 
@@ -123,12 +134,14 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
     const int grp = threadIdx.x / G, i = threadIdx.x % G;
     GroupSmem<G> &sm = reinterpret_cast<GroupSmem<G> *>(smem_raw)[grp];
     const long long w = static_cast<long long>(blockIdx.x) * WPC + grp;
-    const int P = a.per_world;
     const long long n = a.n;
     const bool world_ok = w < a.worlds;
+    // This world's instances: [base, base + P) (worlds of uneven sizes: from world_first).
+    const int P = !world_ok ? 0 : a.world_first ? __ldg(a.world_first + w + 1) - __ldg(a.world_first + w) : a.per_world;
     const bool valid = world_ok && i < P;
-    const long long base = w * P;
+    const long long base = !world_ok ? 0 : a.world_first ? __ldg(a.world_first + w) : w * a.per_world;
     const long long g = base + i;
+    const int slot = a.world_first ? static_cast<int>(g) : i;  // the slot tables' entry of this instance
 
     for (int k = i; k < 2 * G; k += G) sm.parent[k] = -1;
     sm.arrive[i] = 0;
@@ -157,8 +170,8 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
         rec[0] = make_float4(inv[0], inv[1], inv[2], inv[3]);
         rec[1] = make_float4(inv[4], inv[5], inv[6], inv[7]);
         rec[2] = make_float4(inv[8], inv[9], inv[10], inv[11]);
-        rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + i)), __int_as_float(i), 0.0f, 0.0f);
-        const float *lb = a.slot_bounds + 6 * i;
+        rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + slot)), __int_as_float(slot), 0.0f, 0.0f);
+        const float *lb = a.slot_bounds + 6 * slot;
         float b[6];
         for (int k = 0; k < 6; ++k) b[k] = __ldg(lb + k);
         for (int corner = 0; corner < 8; ++corner) {
@@ -175,6 +188,7 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
             atomicMax(&sm.bounds[3 + ax], c);
         }
     }
+    if (world_ok && P == 0 && i == 0) a.roots[w] = -1;  // a world without instances has no tree
     __syncthreads();
 
     // Key (make_keys, cuda_tlas.cuh:99-115).
@@ -224,7 +238,7 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
         const uint32_t kp = sm.key[i];
         const uint32_t wu = static_cast<uint32_t>(w);
         const int ip = static_cast<int>(p);
-        auto dlt = [&](long long x) { return delta<G>(sm, ip, x, n, base, P, wu, kp); };
+        auto dlt = [&](long long x) { return delta<G>(sm, ip, x, n, base, P, wu, kp, a.world_first, a.worlds); };
         const int d = dlt(p + 1) > dlt(p - 1) ? 1 : -1;
         const int min_prefix = dlt(p - d);
         long long max_length = 2;
@@ -319,6 +333,7 @@ __global__ void __launch_bounds__(128) fit_world_links_kernel(const int *roots, 
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= worlds) return;
     int node = roots[w];
+    if (node < 0) return;
     // Keys of different worlds differ in their 32 world bits, so the tree over worlds is at most 33 deep.
     for (int steps = 0;; ++steps) {
         const int p = parent[node];

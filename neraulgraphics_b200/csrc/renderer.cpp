@@ -86,6 +86,12 @@ DevMaterial dev_material(const ngb_material &m) {
 
 }  // namespace
 
+// Worlds of uneven instance counts and image sizes (one camera each), as ngb_create_uneven lays them out.
+struct UnevenLayout {
+    std::vector<int> first;          // world w's instances are [first[w], first[w + 1])
+    std::vector<int> width, height;  // its image
+};
+
 struct Renderer {
     std::mutex mutex;
     std::string last_error;
@@ -149,7 +155,14 @@ struct Renderer {
     float kernel_ms = 0.0f;
     bool timing_pending = false;
 
-    explicit Renderer(const ngb_scene &s);
+    // Uneven worlds: per-world instance ranges, per-view image sizes and offsets (see ngb_create_uneven).
+    bool uneven = false;
+    std::vector<int> world_first_host;
+    DevBuf<int> world_first;
+    DevBuf<int4> view_info;
+    long long total_pixels = 0, total_tiles = 0;
+
+    explicit Renderer(const ngb_scene &s, const UnevenLayout *layout = nullptr);
     ~Renderer();
 
     void build(const float *matrices_in, bool compose, const float *poses);
@@ -165,32 +178,69 @@ struct Renderer {
         float *depth, float *normal, int32_t *ids);
     void cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory, ngb_ray_hits *out,
         float *distance, float *normal, int32_t *ids);
-    size_t pixels() const { return static_cast<size_t>(worlds) * cpw * height * width; }
+    size_t pixels() const {
+        return uneven ? static_cast<size_t>(total_pixels) : static_cast<size_t>(worlds) * cpw * height * width;
+    }
+    int world_of_instance(long long g) const {
+        if (!uneven) return static_cast<int>(g / per_world);
+        return static_cast<int>(std::upper_bound(world_first_host.begin(), world_first_host.end(), g) -
+            world_first_host.begin()) - 1;
+    }
 };
 
-Renderer::Renderer(const ngb_scene &s) {
-    check_frame_size(s.width, s.height);
-    require(s.world_count >= 1, "world_count must be 1 or more, got " + std::to_string(s.world_count));
-    require(s.cameras_per_world >= 1, "cameras_per_world must be 1 or more, got " + std::to_string(s.cameras_per_world));
-    const long long views = static_cast<long long>(s.world_count) * s.cameras_per_world;
-    require(views * s.height <= INT32_MAX, std::to_string(views) + " views of height " + std::to_string(s.height) +
-        " are too many");
+Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
+    if (layout) {
+        // The shared scene is checked as it is; each world's image and instance range on their own.
+        uneven = true;
+        const int W = static_cast<int>(layout->width.size());
+        require(W >= 1, "world_count must be 1 or more, got " + std::to_string(W));
+        require(layout->first.back() == s.instance_count, "the worlds' instance counts add up to " +
+            std::to_string(layout->first.back()) + ", but the scene lists " + std::to_string(s.instance_count));
+        for (int w = 0; w < W; ++w) {
+            check_frame_size(layout->width[w], layout->height[w]);
+            const int count = layout->first[w + 1] - layout->first[w];
+            require(count >= 0 && count <= TILE_MAX_INSTANCES, "world " + std::to_string(w) + " holds " +
+                std::to_string(count) + " instances; uneven worlds hold 0 to " + std::to_string(TILE_MAX_INSTANCES));
+            total_pixels += static_cast<long long>(layout->width[w]) * layout->height[w];
+        }
+        require(total_pixels <= INT32_MAX, "the worlds' images hold " + std::to_string(total_pixels) +
+            " pixels, at most 2^31 - 1 are supported");
+    } else {
+        check_frame_size(s.width, s.height);
+        require(s.world_count >= 1, "world_count must be 1 or more, got " + std::to_string(s.world_count));
+        require(s.cameras_per_world >= 1, "cameras_per_world must be 1 or more, got " + std::to_string(s.cameras_per_world));
+        const long long views = static_cast<long long>(s.world_count) * s.cameras_per_world;
+        require(views * s.height <= INT32_MAX, std::to_string(views) + " views of height " + std::to_string(s.height) +
+            " are too many");
+    }
     check_scene(s);
     check_meshes(s);
-    require(s.instance_count <= MAX_INSTANCES_PER_WORLD, "a world holds " + std::to_string(s.instance_count) +
-        " instances, at most " + std::to_string(MAX_INSTANCES_PER_WORLD) + " are supported");
-    require(static_cast<long long>(s.world_count) * s.instance_count <= (INT32_MAX - 1) / 2,
-        "too many instances over all worlds");
+    if (!layout) {
+        require(s.instance_count <= MAX_INSTANCES_PER_WORLD, "a world holds " + std::to_string(s.instance_count) +
+            " instances, at most " + std::to_string(MAX_INSTANCES_PER_WORLD) + " are supported");
+        require(static_cast<long long>(s.world_count) * s.instance_count <= (INT32_MAX - 1) / 2,
+            "too many instances over all worlds");
+    }
     int device_count = 0;
     CK(cudaGetDeviceCount(&device_count));
     require(s.device >= 0 && s.device < device_count, "device " + std::to_string(s.device) + " does not exist");
-    width = s.width;
-    height = s.height;
-    worlds = s.world_count;
-    cpw = s.cameras_per_world;
-    per_world = s.instance_count;
     device = s.device;
-    n = static_cast<long long>(worlds) * per_world;
+    if (layout) {
+        width = height = 0;
+        worlds = static_cast<int>(layout->width.size());
+        cpw = 1;
+        world_first_host = layout->first;
+        per_world = 0;
+        for (int w = 0; w < worlds; ++w) per_world = std::max(per_world, layout->first[w + 1] - layout->first[w]);
+        n = s.instance_count;
+    } else {
+        width = s.width;
+        height = s.height;
+        worlds = s.world_count;
+        cpw = s.cameras_per_world;
+        per_world = s.instance_count;
+        n = static_cast<long long>(worlds) * per_world;
+    }
     DeviceGuard guard(device);
     CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
@@ -251,7 +301,24 @@ Renderer::Renderer(const ngb_scene &s) {
     params.ambient = 0.0f;
     params.instance_count = static_cast<int>(n);
     params.per_world = per_world;
-    if (per_world == 0) {
+    if (uneven) {
+        // Per view: (width, height, first pixel, first tile of 8 x 4 pixels).
+        std::vector<int4> info(worlds);
+        long long pix = 0, tile = 0;
+        for (int w = 0; w < worlds; ++w) {
+            const int vw = layout->width[w], vh = layout->height[w];
+            info[w] = make_int4(vw, vh, static_cast<int>(pix), static_cast<int>(tile));
+            pix += static_cast<long long>(vw) * vh;
+            tile += static_cast<long long>((vw + 7) / 8) * ((vh + 3) / 4);
+        }
+        total_tiles = tile;
+        view_info.ensure(worlds);
+        CK(cudaMemcpy(view_info.p, info.data(), info.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        world_first.ensure(worlds + 1);
+        CK(cudaMemcpy(world_first.p, world_first_host.data(), (worlds + 1) * sizeof(int), cudaMemcpyHostToDevice));
+        params.world_first = world_first.p;
+    }
+    if (n == 0) {
         CK(cudaEventRecord(ev_done, stream));
         wait(ev_done, timeout);
         return;
@@ -277,22 +344,24 @@ Renderer::Renderer(const ngb_scene &s) {
     for (int m = 0; m < s.mesh_count; ++m)
         for (int p = mesh_base[m]; p < mesh_base[m + 1]; ++p) local_to_packed[mesh_base[m] + built.triangle_index[p]] = p;
     upload(tri_of_local, local_to_packed);
-    std::vector<int> root_of_slot(per_world);
-    std::vector<float> bounds_of_slot(6 * static_cast<size_t>(per_world));
-    std::vector<DevMaterial> material_of_slot(per_world);
-    for (int i = 0; i < per_world; ++i) {
+    // The slot tables: one entry per slot of a world, or per instance when worlds are uneven.
+    const int slots = uneven ? static_cast<int>(n) : per_world;
+    std::vector<int> root_of_slot(slots);
+    std::vector<float> bounds_of_slot(6 * static_cast<size_t>(slots));
+    std::vector<DevMaterial> material_of_slot(slots);
+    for (int i = 0; i < slots; ++i) {
         const int mesh = s.instances[i].mesh;
         root_of_slot[i] = built.roots[mesh];
         std::copy(built.bounds.begin() + 6 * mesh, built.bounds.begin() + 6 * mesh + 6, bounds_of_slot.begin() + 6 * i);
         material_of_slot[i] = dev_material(s.instances[i].material);
     }
     upload(slot_blas_root, root_of_slot);
-    std::vector<int> tri_base_of_slot(per_world);
-    for (int i = 0; i < per_world; ++i) tri_base_of_slot[i] = mesh_base[s.instances[i].mesh];
+    std::vector<int> tri_base_of_slot(slots);
+    for (int i = 0; i < slots; ++i) tri_base_of_slot[i] = mesh_base[s.instances[i].mesh];
     upload(slot_tri_base, tri_base_of_slot);
     upload(blas_pairs, built.pairs);
-    std::vector<int2> root_ref_of_slot(per_world);
-    for (int i = 0; i < per_world; ++i) {
+    std::vector<int2> root_ref_of_slot(slots);
+    for (int i = 0; i < slots; ++i) {
         const int mesh = s.instances[i].mesh;
         root_ref_of_slot[i] = make_int2(built.root_refs[2 * mesh], built.root_refs[2 * mesh + 1]);
     }
@@ -327,9 +396,13 @@ Renderer::Renderer(const ngb_scene &s) {
 
     // Every world starts with the transforms the instances were given (src/cuda_backend.cu:765-770).
     std::vector<float> initial(12 * n);
-    for (int w = 0; w < worlds; ++w)
-        for (int i = 0; i < per_world; ++i)
-            std::memcpy(&initial[12 * (static_cast<size_t>(w) * per_world + i)], s.instances[i].transform, 48);
+    if (uneven) {
+        for (long long g = 0; g < n; ++g) std::memcpy(&initial[12 * g], s.instances[g].transform, 48);
+    } else {
+        for (int w = 0; w < worlds; ++w)
+            for (int i = 0; i < per_world; ++i)
+                std::memcpy(&initial[12 * (static_cast<size_t>(w) * per_world + i)], s.instances[i].transform, 48);
+    }
     CK(cudaMemcpy(matrices.p, initial.data(), initial.size() * sizeof(float), cudaMemcpyHostToDevice));
     build(matrices.p, false, nullptr);
     CK(cudaEventRecord(ev_done, stream));
@@ -431,6 +504,7 @@ void Renderer::build(const float *matrices_in, bool compose, const float *poses)
     a.arrivals = arrivals.p;
     a.error_flag = error_flag.p;
     a.tlas_pairs = tlas_pairs.p;
+    a.world_first = uneven ? world_first.p : nullptr;
     if (use_large_build()) {
         LargeBuildScratch t{};
         t.aabb = large_aabb.ensure(2 * n);
@@ -449,13 +523,16 @@ void Renderer::build(const float *matrices_in, bool compose, const float *poses)
 // src/batch.cpp:91-109 and src/cuda_backend.cu:457-469.
 void Renderer::set_instance_transforms(const float *m, int memory) {
     require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
-    if (per_world == 0) return;
+    if (n == 0) return;
     require(m != nullptr, "matrices must not be null");
     if (memory == NGB_MEMORY_HOST) {
         for (long long g = 0; g < n; ++g)
-            if (!transform_ok(m + 12 * g))
-                check_transform(m + 12 * g, "world " + std::to_string(g / per_world) + " instance " +
-                    std::to_string(g % per_world) + " transform");
+            if (!transform_ok(m + 12 * g)) {
+                const int w = world_of_instance(g);
+                const long long first = uneven ? world_first_host[w] : static_cast<long long>(w) * per_world;
+                check_transform(m + 12 * g, "world " + std::to_string(w) + " instance " + std::to_string(g - first) +
+                    " transform");
+            }
         CK(cudaMemcpyAsync(matrices.p, m, static_cast<size_t>(n) * 12 * sizeof(float), cudaMemcpyHostToDevice, stream));
         build(matrices.p, false, nullptr);
     } else {
@@ -466,6 +543,7 @@ void Renderer::set_instance_transforms(const float *m, int memory) {
 
 // src/batch.cpp:111-129 and src/cuda_backend.cu:472-491.
 void Renderer::bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc) {
+    require(!uneven, "worlds of uneven sizes take instance matrices (set_instance_transforms), not body poses");
     const int P = per_world;
     require(bpw >= 0, "bodies_per_world must be 0 or more");
     require(P == 0 || (boi != nullptr && lp != nullptr && sc != nullptr),
@@ -541,7 +619,7 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     RenderArgs a{};
     a.cameras = cam;
     a.fov_scale = std::tan(fov * 0.5f);  // tanf on the host, as the reference's CPU backend computes it
-    a.aspect = static_cast<float>(width) / static_cast<float>(height);
+    a.aspect = uneven ? 1.0f : static_cast<float>(width) / static_cast<float>(height);
     a.width = width;
     a.height = height;
     a.cameras_per_world = cpw;
@@ -564,11 +642,18 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     // which runs trace in full.
     const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
     const bool tiles_ok = persistent_ok && (params.instance_count == 0 || params.per_world <= TILE_MAX_INSTANCES);
-    const bool tiles = tiles_ok && (kernel_choice == 0 || kernel_choice == 3);
+    const bool tiles = tiles_ok && (kernel_choice == 0 || kernel_choice == 3 || uneven);
     const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
+    require(!uneven || tiles, "worlds of uneven sizes render with one sample per pixel, at most one light and no "
+        "reflective material");
     CK(cudaEventRecord(ev_start, stream));
     if (tiles) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
+        if (uneven) {
+            a.view_info = view_info.p;
+            a.total_pixels = total_pixels;
+            a.total_tiles = total_tiles;
+        }
         if (a.rgb) {
             a.pic_hit = pic_hit.ensure(pixels());
             a.pic_code = pic_code.ensure(pixels());
@@ -639,7 +724,7 @@ void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, flo
 
 struct ngb_renderer {
     ngb::Renderer r;
-    explicit ngb_renderer(const ngb_scene &s) : r(s) {}
+    explicit ngb_renderer(const ngb_scene &s, const ngb::UnevenLayout *layout = nullptr) : r(s, layout) {}
 };
 
 namespace {
@@ -703,6 +788,37 @@ int ngb_create(const ngb_scene *scene, ngb_renderer **out) {
         return NGB_CUDA_ERROR;
     }
 }
+
+int ngb_create_uneven(const ngb_scene *scene, const ngb_uneven_world *worlds, int32_t world_count, ngb_renderer **out) {
+    if (out) *out = nullptr;
+    try {
+        ngb::require(scene != nullptr && out != nullptr && (worlds != nullptr || world_count == 0),
+            "scene, worlds and out must not be null");
+        ngb::require(world_count >= 1, "world_count must be 1 or more, got " + std::to_string(world_count));
+        ngb::UnevenLayout layout;
+        layout.first.assign(1, 0);
+        for (int w = 0; w < world_count; ++w) {
+            ngb::require(worlds[w].instance_count >= 0, "world " + std::to_string(w) + " has a negative instance count");
+            layout.first.push_back(layout.first.back() + worlds[w].instance_count);
+            layout.width.push_back(worlds[w].width);
+            layout.height.push_back(worlds[w].height);
+        }
+        *out = new ngb_renderer(*scene, &layout);
+        g_create_error.clear();
+        return NGB_OK;
+    } catch (const ngb::InvalidArgument &e) {
+        g_create_error = e.what();
+        return NGB_INVALID_ARGUMENT;
+    } catch (const ngb::Timeout &e) {
+        g_create_error = e.what();
+        return NGB_TIMEOUT;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return NGB_CUDA_ERROR;
+    }
+}
+
+int64_t ngb_pixel_count(const ngb_renderer *h) { return h ? static_cast<int64_t>(h->r.pixels()) : 0; }
 
 void ngb_destroy(ngb_renderer *r) { delete r; }
 
@@ -975,6 +1091,7 @@ int ngb_depth_normal_adjoint(ngb_renderer *h, const float *matrices, const float
         ngb::require(matrices && cameras && hit_instance && hit_triangle && hit_u && hit_v && depth && grad_depth &&
             grad_matrices && grad_cameras, "only grad_normal may be null");
         ngb::require(fov > 0.0f && fov < 3.14159265f, "fov must be between 0 and pi radians");
+        ngb::require(!r.uneven, "the adjoint takes worlds of one size");
         ngb::AdjointArgs a{};
         a.matrices = matrices;
         a.cameras = cameras;

@@ -48,7 +48,7 @@ struct WarpSmem {
 
 // A world's run of sorted leaves: leaf k of world w is node n - 1 + first + k.
 __device__ __forceinline__ const float4 *world_leaves(const SceneParams &s, int world) {
-    return s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + static_cast<long long>(world) * s.per_world);
+    return s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + world_first_of(s, world));
 }
 
 // An instance's leaf as the world tree's walk handles it once the ray has passed the leaf's box: the ray
@@ -190,9 +190,8 @@ __device__ __forceinline__ void resolve(const SceneParams &s, int world, float3 
     int hit_tri, float hu, float hv, int best_sphere, bool hit_floor, float3 &normal, DevMaterial &mat, int &object) {
     if (hit_inst >= 0) {
         normal = mesh_surface(s, hit_inst, hit_tri, hu, hv, d);
-        const int slot = hit_inst - world * s.per_world;
-        mat = s.slot_material[slot];
-        object = OBJECT_INSTANCE + slot;
+        mat = s.slot_material[table_of(s, hit_inst, world)];
+        object = OBJECT_INSTANCE + (hit_inst - world_first_of(s, world));
     } else if (hit_floor) {
         object = OBJECT_FLOOR;
         normal = mk3(0.0f, 1.0f, 0.0f);
@@ -230,21 +229,52 @@ __device__ __forceinline__ float abs_dot(float3 n, float3 h) { return fabsf(n.x)
 // The tile kernels' common start: which tile of which view, and the pixel of this lane.
 struct TileAt {
     int view, world, x0, y0, x, y;
+    int width, height;  // the view's image
+    float aspect;
     bool pixel;
     long long pix;
 };
 
+// The last view whose first tile (uneven views: view_info[v].w) or first pixel (.z) is at most at.
+__device__ __forceinline__ int view_of(const int4 *info, int views, long long at, bool by_tile) {
+    int lo = 0, hi = views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int4 v = __ldg(info + mid);
+        if ((by_tile ? v.w : v.z) <= at) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view, int lane) {
     TileAt t;
-    t.view = static_cast<int>(tile / tiles_per_view);
-    const int q = static_cast<int>(tile % tiles_per_view);
+    int q;
+    long long first_pixel;
+    if (a.view_info) {
+        t.view = view_of(a.view_info, a.views, tile, true);
+        const int4 v = __ldg(a.view_info + t.view);
+        t.width = v.x;
+        t.height = v.y;
+        t.aspect = static_cast<float>(v.x) / static_cast<float>(v.y);
+        tiles_x = (v.x + TILE_W - 1) / TILE_W;
+        q = static_cast<int>(tile - v.w);
+        first_pixel = v.z;
+    } else {
+        t.view = static_cast<int>(tile / tiles_per_view);
+        t.width = a.width;
+        t.height = a.height;
+        t.aspect = a.aspect;
+        q = static_cast<int>(tile % tiles_per_view);
+        first_pixel = static_cast<long long>(t.view) * a.height * a.width;
+    }
     t.x0 = (q % tiles_x) * TILE_W;
     t.y0 = (q / tiles_x) * TILE_H;
     t.x = t.x0 + (lane % TILE_W);
     t.y = t.y0 + lane / TILE_W;
-    t.pixel = t.x < a.width && t.y < a.height;
+    t.pixel = t.x < t.width && t.y < t.height;
     t.world = t.view / a.cameras_per_world;
-    t.pix = (static_cast<long long>(t.view) * a.height + t.y) * a.width + t.x;
+    t.pix = first_pixel + static_cast<long long>(t.y) * t.width + t.x;
     return t;
 }
 
@@ -259,13 +289,13 @@ __device__ __forceinline__ long long fetch_tiles(int *counter, int lane) {
 
 // The picture ray of pixel (x, y): its jitter draws from the pixel's random stream, which is left where the
 // light sample continues it (sample_pixel, src/render_core.h:248-258).
-__device__ __forceinline__ float3 picture_ray(const RenderArgs &a, int x, int y, float3 right, float3 up, float3 fwd,
-    uint32_t &rng) {
-    rng = pcg_hash(static_cast<uint32_t>(y * a.width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
+__device__ __forceinline__ float3 picture_ray(const RenderArgs &a, int x, int y, int width, int height, float aspect,
+    float3 right, float3 up, float3 fwd, uint32_t &rng) {
+    rng = pcg_hash(static_cast<uint32_t>(y * width + x) ^ pcg_hash(static_cast<uint32_t>(a.frame) + 1u));
     const float jx = rand_float(rng);
     const float jy = rand_float(rng);
-    return camera_dir(right, up, fwd, static_cast<float>(x) + jx, static_cast<float>(y) + jy,
-        static_cast<float>(a.width), static_cast<float>(a.height), a.fov_scale, a.aspect);
+    return camera_dir(right, up, fwd, static_cast<float>(x) + jx, static_cast<float>(y) + jy, static_cast<float>(width),
+        static_cast<float>(height), a.fov_scale, aspect);
 }
 
 // The picture ray's closest hit as the camera kernel hands it to the shade kernel: the object code
@@ -282,17 +312,17 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
     WarpSmem<CAP> &sm = warp_smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    const int P = s.instance_count > 0 ? s.per_world : 0;
     const int max_steps = s.blas_node_count + 2;
     const bool want_aov = a.depth || a.normal || a.object_id || a.hit_instance;
-    const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
-    const float fs = a.fov_scale, asp = a.aspect;
+    const float fs = a.fov_scale;
     for (;;) {
         const long long first = fetch_tiles(counter, lane);
         if (first >= tiles) break;
         const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
         for (long long tile = first; tile < last; ++tile) {
             const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
+            const int P = s.instance_count > 0 ? world_count_of(s, T.world) : 0;
+            const float fw = static_cast<float>(T.width), fh = static_cast<float>(T.height), asp = T.aspect;
             // The view's camera (camera_from_matrix, src/render_core.h:264-273).
             const float4 c0 = __ldg(a.camera_basis + 3 * T.view), c1 = __ldg(a.camera_basis + 3 * T.view + 1);
             const float4 c2 = __ldg(a.camera_basis + 3 * T.view + 2);
@@ -377,7 +407,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                         fs, asp);
                 } else {
                     uint32_t rng;
-                    d = picture_ray(a, T.x, T.y, right, up, fwd, rng);
+                    d = picture_ray(a, T.x, T.y, T.width, T.height, asp, right, up, fwd, rng);
                 }
                 int best_sphere;
                 bool hit_floor;
@@ -431,16 +461,27 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
     const float3 zero = mk3(0.0f, 0.0f, 0.0f);
     for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < pixels;
          p += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int view = static_cast<int>(p / per_view);
-        const int rem = static_cast<int>(p % per_view);
-        const int y = rem / a.width, x = rem % a.width;
+        int view, rem, width = a.width, height = a.height;
+        float aspect = a.aspect;
+        if (a.view_info) {
+            view = view_of(a.view_info, a.views, p, false);
+            const int4 v = __ldg(a.view_info + view);
+            width = v.x;
+            height = v.y;
+            aspect = static_cast<float>(v.x) / static_cast<float>(v.y);
+            rem = static_cast<int>(p - v.z);
+        } else {
+            view = static_cast<int>(p / per_view);
+            rem = static_cast<int>(p % per_view);
+        }
+        const int y = rem / width, x = rem % width;
         const int world = view / a.cameras_per_world;
         const float4 c0 = __ldg(a.camera_basis + 3 * view), c1 = __ldg(a.camera_basis + 3 * view + 1);
         const float4 c2 = __ldg(a.camera_basis + 3 * view + 2);
         const float3 eye = mk3(c0.x, c0.y, c0.z), right = mk3(c0.w, c1.x, c1.y);
         const float3 up = mk3(c1.z, c1.w, c2.x), fwd = mk3(c2.y, c2.z, c2.w);
         uint32_t rng;
-        const float3 d = picture_ray(a, x, y, right, up, fwd, rng);
+        const float3 d = picture_ray(a, x, y, width, height, aspect, right, up, fwd, rng);
         const int code = a.pic_code[p];
         const float4 h = a.pic_hit[p];
         float3 radiance;
@@ -526,7 +567,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
     int *cand_leaf = warp_cand[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    const int P = s.instance_count > 0 ? s.per_world : 0;
     const int max_steps = s.blas_node_count + 2;
     const DevLight &lt = s.lights[0];
     const float INF = __int_as_float(0x7f800000);
@@ -536,6 +576,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
         const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
         for (long long tile = first; tile < last; ++tile) {
             const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
+            const int P = s.instance_count > 0 ? world_count_of(s, T.world) : 0;
             float4 o4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (T.pixel) o4 = a.shadow_o[T.pix];
             const bool pending = o4.w > 0.0f;
@@ -647,7 +688,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     cudaEvent_t after_camera, cudaEvent_t after_shade) {
     const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
     const int tiles_per_view = tiles_x * tiles_y;
-    const long long tiles = static_cast<long long>(tiles_per_view) * a.views;
+    const long long tiles = a.view_info ? a.total_tiles : static_cast<long long>(tiles_per_view) * a.views;
     const bool aov = a.depth || a.normal || a.object_id || a.hit_instance;
     cudaError_t e = cudaSuccess;
     auto mark = [&](cudaEvent_t ev) {
@@ -667,7 +708,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         mark(after_shade);
         return e;
     }
-    const long long pixels = static_cast<long long>(a.views) * a.width * a.height;
+    const long long pixels = a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.height;
     int device = 0, sms = 0;
     e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

@@ -140,6 +140,7 @@ __device__ __noinline__ bool mesh_query(const SceneParams &s, int world, float3 
     const float3 inv_d = safe_inverse(d);
     const int root = __ldg(s.roots + world);
     bool found = false;
+    if (root < 0) return false;  // a world without instances
     if (box_entry(__ldg(tlas + 2 * root), __ldg(tlas + 2 * root + 1), o, inv_d, tmax) >= NO_HIT) return false;
     int stack[TLAS_STACK];
     float stack_t[TLAS_STACK];
@@ -280,9 +281,8 @@ __device__ __forceinline__ bool scene_intersect(const SceneParams &s, int world,
     hit.u = hit.v = 0.0f;
     if (best_instance >= 0) {
         hit.normal = mesh_surface(s, best_instance, best_triangle, bu, bv, dir);
-        const int slot = best_instance - world * s.per_world;
-        hit.material = s.slot_material[slot];
-        hit.object = OBJECT_INSTANCE + slot;
+        hit.material = s.slot_material[table_of(s, best_instance, world)];
+        hit.object = OBJECT_INSTANCE + (best_instance - world_first_of(s, world));
         hit.instance = best_instance;
         hit.triangle = best_triangle;
         hit.u = bu;

@@ -357,3 +357,91 @@ class BatchRenderer:
         check(self._lib.ngb_inspect_hits(self._h, vp(inst), vp(tri), vp(u), vp(v)), self._h)
         return {"hit_instance": inst, "hit_triangle": tri, "hit_u": u, "hit_v": v}
 
+
+class UnevenBatchRenderer(BatchRenderer):
+    """Worlds of uneven instance counts and image sizes in one renderer (ngb_create_uneven).
+
+    worlds: a list of (width, height, instances), one camera per world; every world may hold its own list of
+    0 to 256 instances of the shared meshes. Matrices for set_instance_transforms are every world's instances,
+    world after world: (total_instances, 3, 4). render takes (world_count, 3, 4) cameras and returns the images
+    packed world after world: 'rgb' (pixels, 3), 'depth' (pixels,), 'normals' (pixels, 3), 'object_ids'
+    (pixels,); image(out, w) views world w's image as (height, width[, 3]). One sample per pixel, at most one
+    light and no reflective material.
+    """
+
+    def __init__(self, worlds, spheres=(), lights=(), floor=None, meshes=(), device="auto"):
+        self._device = _parse_device(device)
+        flat = [inst for _, _, insts in worlds for inst in insts]
+        self._desc = SceneDesc(1, 1, 1, 1, spheres, lights, floor if floor is not None else Plane(), meshes, flat,
+                               self._device)
+        self._sizes = [(int(w), int(h)) for w, h, _ in worlds]
+        self._counts = [len(insts) for _, _, insts in worlds]
+        arr = (_abi.UnevenWorldC * len(worlds))(*[_abi.UnevenWorldC(w, h, c) for (w, h), c in zip(self._sizes,
+                                                                                                  self._counts)])
+        self._lib = lib()
+        h = C.c_void_p()
+        check(self._lib.ngb_create_uneven(C.byref(self._desc.c), arr, len(worlds), C.byref(h)), None)
+        self._h = h
+        check(self._lib.ngb_set_sync(self._h, 0, _TIMEOUT_S), self._h)
+        self._out = {}
+        self._rays = {}
+        self.pixel_first = np.concatenate([[0], np.cumsum([w * hh for w, hh in self._sizes])]).astype(np.int64)
+        self.instance_first = np.concatenate([[0], np.cumsum(self._counts)]).astype(np.int64)
+
+    @property
+    def pixel_count(self) -> int:
+        return int(self._lib.ngb_pixel_count(self._h))
+
+    @property
+    def instance_count(self) -> int:
+        return int(self.instance_first[-1])
+
+    def set_instance_transforms(self, matrices):
+        """Every world's instance matrices, world after world: (total_instances, 3, 4) float32."""
+        _require_count(matrices, self.instance_count * 12, "matrices", "(total_instances, 3, 4)")
+        p, mem, keep = self._input(matrices, "matrices")
+        self._stream()
+        check(self._lib.ngb_set_instance_transforms(self._h, p, mem), self._h)
+        self._keep = keep
+        if mem == _abi.MEMORY_HOST:
+            self.synchronize()
+
+    def bind_bodies(self, *args, **kwargs):
+        raise ValueError("worlds of uneven sizes take instance matrices (set_instance_transforms), not body poses")
+
+    def render(self, cameras, fov=1.0, samples_per_pixel=1, *, rgb=True, depth=False, normals=False,
+               object_ids=False, frame=0, zero_copy=False):
+        torch = _torch()
+        P, worlds = self.pixel_count, len(self._sizes)
+        _require_count(cameras, worlds * 12, "cameras", f"{worlds} cameras of 3 x 4 numbers (camera-to-world)")
+        if not zero_copy and _is_cuda_tensor(cameras):
+            raise ValueError("cameras on the GPU need zero_copy=True: the results then stay on the GPU too")
+        outputs = ((_abi.OUTPUT_RGB if rgb else 0) | (_abi.OUTPUT_DEPTH if depth else 0) |
+                   (_abi.OUTPUT_NORMAL if normals else 0) | (_abi.OUTPUT_OBJECT_ID if object_ids else 0))
+        bufs = {}
+        if rgb:
+            bufs["rgb"] = self._buffer("rgb", (P, 3), torch.uint8)
+        if depth:
+            bufs["depth"] = self._buffer("depth", (P,), torch.float32)
+        if normals:
+            bufs["normals"] = self._buffer("normals", (P, 3), torch.float32)
+        if object_ids:
+            bufs["object_ids"] = self._buffer("object_ids", (P,), torch.int32)
+        p, mem, keep = self._input(cameras, "cameras")
+        ptr = lambda k: C.c_void_p(bufs[k].data_ptr()) if k in bufs else None
+        self._stream()
+        check(self._lib.ngb_render_into(self._h, p, float(fov), int(samples_per_pixel), outputs, int(frame), mem,
+                                        ptr("rgb"), ptr("depth"), ptr("normals"), ptr("object_ids")), self._h)
+        self._keep = keep
+        if zero_copy:
+            return dict(bufs)
+        host = {k: v.cpu().numpy() for k, v in bufs.items()}
+        self.synchronize()
+        return host
+
+    def image(self, packed, w):
+        """World w's image out of a packed output: (height, width) or (height, width, 3)."""
+        a, b = int(self.pixel_first[w]), int(self.pixel_first[w + 1])
+        width, height = self._sizes[w]
+        x = packed[a:b]
+        return x.reshape((height, width) + tuple(x.shape[1:]))

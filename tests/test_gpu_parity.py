@@ -421,3 +421,49 @@ def test_large_world_renders_and_casts_rays(torch_cuda):
     assert np.array_equal(got["object_id"], exp["object_id"])
     assert np.array_equal(bits(got["distance"]), bits(exp["distance"]))
     assert np.array_equal(bits(got["normal"]), bits(exp["normal"]))
+
+
+def uneven_scene(seed=4):
+    """Seven worlds of 0 to 200 instances of three meshes at five image sizes, with their cameras and matrices."""
+    rng = np.random.default_rng(seed)
+    meshes = [ng.make_box((0.4, 0.4, 0.4)), ng.make_icosphere(0.5, 2), ng.cylinder(1.0, 1.0, 32)]
+    counts = [1, 5, 33, 0, 12, 200, 3]
+    sizes = [(32, 32), (64, 64), (48, 40), (64, 64), (128, 128), (64, 48), (40, 24)]
+    worlds, mats, cams = [], [], []
+    for w, (count, (width, height)) in enumerate(zip(counts, sizes)):
+        insts = [ng.Instance(int(rng.integers(0, 3)), material=ng.Material(diffuse_color=tuple(rng.uniform(0.2, 0.9, 3))))
+                 for _ in range(count)]
+        worlds.append((width, height, insts))
+        for i in range(count):
+            q = rng.normal(size=4)
+            mats.append(ng.make_transform(rng.uniform(-2, 2, 3) + (0, 0, -6), q / np.linalg.norm(q),
+                                          float(rng.uniform(0.3, 0.8))).matrix)
+        eye = np.array([0.0, 1.0, 0.0]) + rng.uniform(-0.3, 0.3, 3)
+        cams.append(workloads.camera_matrix(eye, (0.0, 0.0, -6.0), width, height, 1.0))
+    floor = ng.Plane(y=-2.5, half_extent_x=12.0, z_min=-30.0, z_max=-2.0, checker_scale=1.0)
+    lights = [ng.Light((-10.0, 20.0, 10.0), 1.6, 1.0)]
+    return worlds, meshes, floor, lights, np.stack(mats).astype(np.float32), np.stack(cams).astype(np.float32)
+
+
+def test_uneven_worlds_are_each_worlds_own_render(torch_cuda):
+    """One uneven renderer against, world by world, a plain renderer of that world alone (bit for bit: the
+    same kernels see the same world) and the oracle (apart from near-ties)."""
+    worlds, meshes, floor, lights, mats, cams = uneven_scene()
+    u = ng.UnevenBatchRenderer(worlds, lights=lights, floor=floor, meshes=meshes, device="cuda:0")
+    u.set_instance_transforms(mats)
+    got = u.render(cams, 1.0, 1, **ALL, frame=2)
+    assert got["depth"].shape == (u.pixel_count,)
+    first = u.instance_first
+    for w, (width, height, insts) in enumerate(worlds):
+        desc = ng.SceneDesc(width, height, 1, 1, [], lights, floor, meshes, insts)
+        m = mats[first[w]:first[w + 1]].reshape(1, len(insts), 3, 4)
+        mine = {k: u.image(v, w)[None] for k, v in got.items()}
+        plain = product(desc)
+        if insts:
+            plain.set_instance_transforms(m)
+        assert_same_images(mine, plain.render(cams[w:w + 1], 1.0, 1, **ALL, frame=2), rgb_tol=0)
+        o = O.Oracle(desc)
+        if insts:
+            o.set_instance_transforms(m)
+        want = o.render(cams[w:w + 1], 1.0, 1, **ALL, frame=2, ties=True)
+        assert_same_images(mine, want, ties=want["ties"])
