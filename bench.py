@@ -48,10 +48,13 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
-    p.add_argument("--config", default="body_worlds", choices=["body_worlds", "large_world", "differentiable"],
+    p.add_argument("--config", default="body_worlds",
+                   choices=["body_worlds", "large_world", "differentiable", "uneven"],
                    help="body_worlds: the headline (4096 worlds x 64x64); large_world: one world of 100,000 "
                         "instances at 1280x720 with a 64 x 2048 LiDAR sweep, poses redrawn every frame; "
-                        "differentiable: 1024 worlds x 128x128 depth+normals, forward+backward against forward")
+                        "differentiable: 1024 worlds x 128x128 depth+normals, forward+backward against forward; "
+                        "uneven: 2048 worlds of 1..200 instances at 32/64/128 px, one CUDA graph per step, against "
+                        "bucketed plain renderers")
     p.add_argument("--profile", action="store_true",
                    help="device-resident steps only (no autotune, e2e, CPU or reference arms): for ncu captures")
     return p.parse_args()
@@ -530,6 +533,126 @@ def run_differentiable(args, rank, world, local_rank, dist):
     }
 
 
+def run_uneven(args, rank, world, local_rank, dist):
+    """2048 worlds of 1..200 instances at 32x32, 64x64 or 128x128, RGB + depth + ID. Per step the instance
+    matrices of the random walk go to the device (one copy into the graph's input), then one CUDA graph
+    replays the whole step: the tree build of every world and the render of every view (camera, shade and
+    shadow kernels). Against the same steps through plain renderers, one per (resolution, instance count)
+    bucket, launched one after another."""
+    import torch
+
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    wl = workloads.uneven_worlds(seed=rank)
+    mats = torch.from_numpy(workloads.walk_uneven(wl, W + K, seed=1 + rank)).to(dev)
+    cams = torch.from_numpy(wl["cameras"]).to(dev)
+    r = ng.UnevenBatchRenderer(wl["worlds"], lights=wl["lights"], floor=wl["floor"], meshes=wl["meshes"], device=dev)
+    kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
+    static = mats[0].clone()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    # The tile kernel's shape, timed on this batch.
+    r.set_instance_transforms(static)
+    shapes = []
+    for threads, regs in ((128, 64), (128, 80), (256, 64)):
+        r.set_tuning(kernel=3, threads_per_block=threads, registers=regs)
+        r.render(cams, wl["fov"], 1, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            r.render(cams, wl["fov"], 1, **kw)
+        e1.record()
+        e1.synchronize()
+        shapes.append((e0.elapsed_time(e1) / 3, threads, regs))
+    best = min(shapes)
+    r.set_tuning(kernel=3, threads_per_block=best[1], registers=best[2])
+    # One graph for the whole step, captured after warm-up renders on the capture stream.
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            r.set_instance_transforms(static)
+            r.render(cams, wl["fov"], 1, **kw)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        r.set_instance_transforms(static)
+        out = r.render(cams, wl["fov"], 1, **kw)
+    # The graph's images equal an eager render's.
+    static.copy_(mats[1])
+    graph.replay()
+    torch.cuda.synchronize()
+    graph_ids = out["object_ids"].clone()
+    r.set_instance_transforms(mats[1].clone())
+    same = bool(torch.equal(graph_ids, r.render(cams, wl["fov"], 1, **kw)["object_ids"]))
+
+    def timed(step):
+        for s in range(W):
+            step(s)
+        torch.cuda.synchronize()
+        ms = []
+        for s in range(K):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step(W + s)
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms)
+
+    def graph_step(s):
+        static.copy_(mats[s])
+        graph.replay()
+
+    with ClockSampler(local_rank) as clocks:
+        graph_ms = timed(graph_step)
+    # Plain renderers, one per (resolution, instance count) bucket, launched one after another.
+    first = r.instance_first
+    buckets = {}
+    for w, (size, _, insts) in enumerate(wl["worlds"]):
+        buckets.setdefault((size, len(insts)), []).append(w)
+    plain = []
+    for (size, count), ws in sorted(buckets.items()):
+        insts = wl["worlds"][ws[0]][2]
+        rb = ng.BatchRenderer(size, size, len(ws), 1, [], wl["lights"], wl["floor"], wl["meshes"], insts, device=dev)
+        idx = torch.from_numpy(np.concatenate([np.arange(first[w], first[w + 1]) for w in ws])).to(dev)
+        plain.append((rb, mats[:, idx].contiguous(), cams[torch.tensor(ws, device=dev)].contiguous()))
+
+    def plain_step(s):
+        for rb, mb, cb in plain:
+            rb.set_instance_transforms(mb[s])
+            rb.render(cb, wl["fov"], 1, **kw)
+
+    plain_ms = timed(plain_step)
+    if rank != 0:
+        return None
+    views = len(wl["worlds"])
+    return {
+        "metric": "images/s at 2048 uneven worlds (1..200 instances, 32/64/128 px) RGB+depth+ID, one CUDA graph per "
+                  "step (tree build + render)",
+        "value": round(world * views / (graph_ms / 1000.0), 1), "unit": "images/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": round(graph_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uneven_worlds scene and random-walk poses)",
+        "config": {"workload": f"uneven_worlds: {views} worlds, {int(first[-1])} instances, {r.pixel_count} pixels; "
+                               "six meshes of 12 to 20480 triangles; one light, spp 1",
+                   "l2": "flushed before every timed step (256 MiB write)"},
+        "kernel_shape": {"threads": best[1], "registers": best[2], "timings_ms": [round(x[0], 4) for x in shapes]},
+        "graph_matches_eager": same,
+        "bucketed_plain": {"value": round(views / (plain_ms / 1000.0), 1), "unit": "images/s",
+                           "ms_per_step": round(plain_ms, 4), "buckets": len(plain),
+                           "what": "one plain BatchRenderer per (resolution, instance count) bucket, set_instance_"
+                                   "transforms + render each, launched one after another"},
+        "gpu_launches_per_step": 6,
+        "clocks": clocks.summary(),
+    }
+
+
 def reference_cuda_large(wl, torch, mats, cams, lo, ld, steps, warmup):
     """The reference's CUDA backend on the same large-world frames, inputs on the device: ms per stage."""
     import oracle as O
@@ -618,7 +741,8 @@ def main():
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device(f"cuda:{local_rank}"))
-        run = {"body_worlds": run_ours, "large_world": run_large, "differentiable": run_differentiable}[args.config]
+        run = {"body_worlds": run_ours, "large_world": run_large, "differentiable": run_differentiable,
+               "uneven": run_uneven}[args.config]
         line = run(args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()

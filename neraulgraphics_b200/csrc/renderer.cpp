@@ -168,6 +168,11 @@ struct Renderer {
     void build(const float *matrices_in, bool compose, const float *poses);
     void finish();
     void read_timing();
+    // Whether the stream is being captured into a CUDA graph.
+    bool capturing() const {
+        cudaStreamCaptureStatus status = cudaStreamCaptureStatusNone;
+        return cudaStreamIsCapturing(stream, &status) == cudaSuccess && status != cudaStreamCaptureStatusNone;
+    }
     bool use_large_build() const { return build_mode == 2 || (build_mode == 0 && per_world > MAX_PER_WORLD); }
     void wait(cudaEvent_t ev, double seconds);
     void set_instance_transforms(const float *m, int memory);
@@ -471,6 +476,7 @@ void Renderer::read_timing() {
 
 void Renderer::finish() {
     CK(cudaMemcpyAsync(host_error, error_flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (capturing()) return;  // a graph's replays report through ngb_synchronize
     CK(cudaEventRecord(ev_done, stream));
     if (!synchronous) return;
     wait(ev_done, timeout);
@@ -646,7 +652,10 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
     require(!uneven || tiles, "worlds of uneven sizes render with one sample per pixel, at most one light and no "
         "reflective material");
-    CK(cudaEventRecord(ev_start, stream));
+    // Inside a CUDA graph capture the timing events would be graph nodes whose times cannot be read: the
+    // render is then not timed (last_kernel_ms keeps the previous figure).
+    const bool timed = !capturing();
+    if (timed) CK(cudaEventRecord(ev_start, stream));
     if (tiles) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
         if (uneven) {
@@ -660,8 +669,8 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
             a.shadow_o = shadow_o.ensure(pixels());
             a.shadow_d = shadow_d.ensure(pixels());
         }
-        CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream, ev_stage[0],
-            ev_stage[1]));
+        CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream,
+            timed ? ev_stage[0] : nullptr, timed ? ev_stage[1] : nullptr));
         stages = 3;
     } else if (persistent) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
@@ -671,8 +680,10 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
         CK(launch_render(params, a, stream));
         stages = 1;
     }
-    CK(cudaEventRecord(ev_stop, stream));
-    timing_pending = true;
+    if (timed) {
+        CK(cudaEventRecord(ev_stop, stream));
+        timing_pending = true;
+    }
     finish();
 }
 
@@ -707,11 +718,14 @@ void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, flo
     a.normal = normal ? normal : ray_normal.ensure(3 * count);
     a.object_id = ids ? ids : ray_id.ensure(count);
     a.error_flag = error_flag.p;
-    CK(cudaEventRecord(ev_start, stream));
+    const bool timed = !capturing();
+    if (timed) CK(cudaEventRecord(ev_start, stream));
     CK(launch_rays(params, a, stream));
-    stages = 1;
-    CK(cudaEventRecord(ev_stop, stream));
-    timing_pending = true;
+    if (timed) {
+        stages = 1;
+        CK(cudaEventRecord(ev_stop, stream));
+        timing_pending = true;
+    }
     finish();
     out->distance = a.distance;
     out->normal = a.normal;

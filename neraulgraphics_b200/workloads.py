@@ -7,6 +7,7 @@ on. Every generator is deterministic in its seed (numpy's default_rng).
 - `icosphere_worlds`: 16 worlds at 64x64, each a floor and 8 icospheres (320 triangles) placed by matrices.
 - `body_worlds`: 4096 worlds at 64x64, 20 simulator bodies each carrying one instance of three shared
   meshes (icosphere 1280, box 12, capped cylinder 512 triangles), moved by a Gaussian random walk.
+- `uneven_worlds`: 2048 worlds of 1 to 200 instances of six meshes at 32x32, 64x64 or 128x128.
 - `differentiable_worlds`: 1024 worlds at 128x128 of 12 icospheres and boxes, with target poses, for the adjoint.
 - `large_world`: one world of 100,000 instances of five meshes at 1280x720, with a 64 x 2048 LiDAR sweep.
 """
@@ -121,6 +122,54 @@ def body_worlds(worlds=4096, bodies=20, width=64, height=64, seed=0) -> Workload
     return Workload("body_worlds", desc, cams, 1.0, 1, binding=binding, poses=poses,
                     info={"worlds": worlds, "bodies": bodies, "width": width, "height": height, "seed": seed,
                           "triangles": [1280, 12, 512]})
+
+
+def uneven_worlds(worlds=2048, seed=0):
+    """2048 worlds of uneven sizes: instance counts uniform in 1..200, images of 32x32, 64x64 or 128x128.
+
+    Six shared meshes: box of half-extent 0.4 (12 triangles), icosphere radius 0.5 subdivision 2 (320), capped
+    cylinder radius 1 half-height 1 with 128 segments (512) at scale (0.3, 0.3, 0.5), icosphere subdivision 3
+    (1280), 4 (5120) and 5 (20480). Instance i of a world uses mesh i % 6 with colour PALETTE[i % 8], so worlds
+    of the same instance count hold the same instance list (they can share a plain renderer). Each instance is
+    its own body: position uniform in [-r, r]^3 with r = 2 (count / 20)^(1/3) (the density of body_worlds),
+    rotation uniform on S^3, uniform scale U[0.6, 1.2] (the cylinder's as above); the random walk of body_worlds
+    moves them (walk_uneven). One camera per world on a ring of radius 2 r at height r / 2, world w at angle
+    2 pi w / worlds, looking at the origin; fov 1.0 rad. Floor y = -r - 0.5, half-extent 4 r, z in (-4 r, 4 r),
+    checker 1. Light as in icosphere_worlds (one floor and light for all worlds: the floor's placement follows
+    the largest r).
+    """
+    rng = np.random.default_rng(seed)
+    meshes = [make_box((0.4, 0.4, 0.4)), make_icosphere(0.5, 2), cylinder(1.0, 1.0, 128), make_icosphere(0.5, 3),
+              make_icosphere(0.5, 4), make_icosphere(0.5, 5)]
+    counts = rng.integers(1, 201, size=worlds)
+    res = np.array([32, 64, 128])[rng.integers(0, 3, size=worlds)]
+    spec, pos, quat, scale, cams = [], [], [], [], []
+    rmax = 2.0 * (200 / 20.0) ** (1.0 / 3.0)
+    for w in range(worlds):
+        c, size = int(counts[w]), int(res[w])
+        r = 2.0 * (c / 20.0) ** (1.0 / 3.0)
+        insts = [Instance(i % 6, material=Material(diffuse_color=PALETTE[i % len(PALETTE)])) for i in range(c)]
+        spec.append((size, size, insts))
+        pos.append(rng.uniform(-r, r, size=(c, 3)))
+        quat.append(uniform_quaternions(rng, c))
+        sc = np.repeat(rng.uniform(0.6, 1.2, size=(c, 1)), 3, axis=1)
+        sc[2::6] = np.array([0.3, 0.3, 0.5]) * sc[2::6]
+        scale.append(sc)
+        a = 2.0 * np.pi * w / worlds
+        cams.append(camera_matrix((2 * r * np.cos(a), r / 2, 2 * r * np.sin(a)), (0.0, 0.0, 0.0), size, size, 1.0))
+    floor = Plane(y=-rmax - 0.5, half_extent_x=4 * rmax, z_min=-4 * rmax, z_max=4 * rmax, checker_scale=1.0)
+    pos, quat, scale = (np.concatenate(x).astype(np.float32) for x in (pos, quat, scale))
+    return {"worlds": spec, "meshes": meshes, "floor": floor, "lights": [LIGHT], "cameras": np.stack(cams).astype(np.float32),
+            "positions": pos, "quaternions": quat, "scales": scale, "counts": counts, "resolutions": res,
+            "fov": 1.0, "seed": seed}
+
+
+def walk_uneven(wl, steps, seed=1, sigma_pos=0.02, sigma_rot=0.05) -> np.ndarray:
+    """(steps, total_instances, 3, 4) matrices of uneven_worlds' instances after each step of the random walk of
+    body_worlds (random_walk), every instance its own body."""
+    poses = np.concatenate([wl["positions"], wl["quaternions"]], -1)[None]
+    walk = random_walk(poses, steps, seed=seed, sigma_pos=sigma_pos, sigma_rot=sigma_rot)[:, 0]
+    return pose_matrices_np(walk[..., :3], walk[..., 3:], wl["scales"])
 
 
 def differentiable_worlds(worlds=1024, per_world=12, width=128, height=128, seed=0) -> Workload:
