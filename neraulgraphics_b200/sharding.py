@@ -1,0 +1,86 @@
+"""Worlds across GPUs: one process per GPU, each rendering its own contiguous range of the worlds.
+
+Worlds are independent, so the render shards with no exchange on the data path: every rank composes, builds
+and renders its own worlds, and its images stay on its GPU for the consumer there (a policy, a loss). A
+consumer that wants every image calls gather(), one all-gather over the process group (NCCL over NVLink on
+GPUs; gloo on CPUs). Timing is the slowest rank's: max_over_ranks().
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl")
+    shard = ShardedWorlds(world_count=16384)              # this rank's worlds: shard.start .. shard.stop
+    r = BatchRenderer(64, 64, shard.count, ...)           # a renderer of those worlds only
+    r.set_body_poses(shard.take(all_poses))               # or poses made on this rank for its worlds
+    images = r.render(shard.take(all_cameras), zero_copy=True)
+    everything = shard.gather(images["depth"])            # (16384, 64, 64) on every rank, if wanted
+"""
+
+from __future__ import annotations
+
+
+def world_range(world_count: int, rank: int, world_size: int) -> tuple[int, int]:
+    """[start, stop) of rank's worlds: contiguous ranges, in rank order, whose sizes differ by at most one."""
+    if world_size < 1 or not 0 <= rank < world_size:
+        raise ValueError(f"rank {rank} is not in a group of {world_size}")
+    if world_count < 0:
+        raise ValueError(f"world_count must be 0 or more, got {world_count}")
+    base, extra = divmod(world_count, world_size)
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+class ShardedWorlds:
+    """This rank's share of world_count worlds in a torch.distributed process group (the default group when
+    group is None; one rank when torch.distributed is not initialised)."""
+
+    def __init__(self, world_count: int, group=None):
+        import torch.distributed as dist
+        self.group = group
+        if dist.is_available() and dist.is_initialized():
+            self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
+        else:
+            self.rank, self.size = 0, 1
+        self.world_count = world_count
+        self.start, self.stop = world_range(world_count, self.rank, self.size)
+        self.ranges = [world_range(world_count, r, self.size) for r in range(self.size)]
+
+    @property
+    def count(self) -> int:
+        return self.stop - self.start
+
+    def take(self, per_world):
+        """This rank's slice of an array or tensor whose first axis runs over every world."""
+        if len(per_world) != self.world_count:
+            raise ValueError(f"expected {self.world_count} worlds on the first axis, got {len(per_world)}")
+        return per_world[self.start:self.stop]
+
+    def gather(self, local):
+        """Every rank's local tensor (first axis: its worlds, or its views world-major with a fixed number per
+        world) concatenated in world order, on every rank: one all-gather of equal-sized, padded pieces."""
+        import torch
+        import torch.distributed as dist
+        if self.size == 1:
+            return local
+        # Every rank's row count; the ranks must agree on the rows per world, and the largest piece sets the
+        # padded size of the all-gather.
+        rows = torch.tensor([local.shape[0], self.count], dtype=torch.int64, device=local.device)
+        all_rows = [torch.zeros_like(rows) for _ in range(self.size)]
+        dist.all_gather(all_rows, rows, group=self.group)
+        per_world = {int(r[0]) / int(r[1]) for r in all_rows if int(r[1]) > 0}
+        if len(per_world) > 1 or any(float(p) != int(p) for p in per_world):
+            raise ValueError("every rank's local tensor must hold the same number of rows per world")
+        pad = max(int(r[0]) for r in all_rows)
+        piece = torch.zeros((pad,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+        piece[:local.shape[0]] = local
+        pieces = [torch.empty_like(piece) for _ in range(self.size)]
+        dist.all_gather(pieces, piece, group=self.group)
+        return torch.cat([p[:int(r[0])] for p, r in zip(pieces, all_rows)], 0)
+
+    def max_over_ranks(self, value: float, device=None) -> float:
+        """The largest value over the ranks (a time: the job takes as long as its slowest rank)."""
+        import torch
+        import torch.distributed as dist
+        if self.size == 1:
+            return float(value)
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+        return float(t.item())

@@ -1,0 +1,83 @@
+"""Worlds across ranks (neraulgraphics_b200.sharding): the partition, and two gloo ranks on CPU that each
+render their own worlds and gather every image, against one rank rendering them all. The per-rank renderer
+here is the oracle, the CPU stand-in for each rank's GPU; the sharding logic is what is under test."""
+
+import datetime
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+from neraulgraphics_b200.sharding import world_range
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.parametrize("worlds,size", [(5, 2), (4096, 8), (3, 4), (0, 2), (17, 1)])
+def test_world_ranges_cover_every_world_once_in_order(worlds, size):
+    ranges = [world_range(worlds, r, size) for r in range(size)]
+    assert ranges[0][0] == 0 and ranges[-1][1] == worlds
+    assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+    sizes = [b - a for a, b in ranges]
+    assert max(sizes) - min(sizes) <= 1 and sorted(sizes, reverse=True) == sizes
+    with pytest.raises(ValueError):
+        world_range(worlds, size, size)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, size, port, worlds, out):
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch
+    import torch.distributed as dist
+
+    import oracle as O
+    from neraulgraphics_b200 import workloads
+    from neraulgraphics_b200.scene import SceneDesc
+    from neraulgraphics_b200.sharding import ShardedWorlds
+    dist.init_process_group("gloo", rank=rank, world_size=size, timeout=datetime.timedelta(seconds=120))
+    try:
+        wl = workloads.body_worlds(worlds=worlds, width=24, height=16, seed=3)
+        d = wl.desc
+        shard = ShardedWorlds(worlds)
+        local = SceneDesc(d.width, d.height, shard.count, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+        o = O.Oracle(local)
+        o.bind_bodies(**wl.binding)
+        o.set_body_poses(shard.take(wl.poses))
+        img = o.render(shard.take(wl.cameras), wl.fov, 1, rgb=True, depth=True, object_ids=True)
+        got = {k: shard.gather(torch.from_numpy(v)).numpy() for k, v in img.items()}
+        slowest = shard.max_over_ranks(0.5 + rank)
+        if rank == 0:
+            full = O.Oracle(d)
+            full.bind_bodies(**wl.binding)
+            full.set_body_poses(wl.poses)
+            want = full.render(wl.cameras, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+            ok = all(np.array_equal(got[k].view(np.uint8), want[k].view(np.uint8)) for k in want)
+            np.save(out, np.array([ok, slowest == size - 0.5, shard.start, shard.stop], dtype=np.float64))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("worlds", [5, 2])
+def test_two_ranks_render_their_worlds_and_gather_everything(tmp_path, worlds):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    port, out = _free_port(), str(tmp_path / "rank0.npy")
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, worlds, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    ok, slowest, start, stop = np.load(out)
+    assert ok and slowest and (start, stop) == (0, (worlds + 1) // 2)
