@@ -557,7 +557,8 @@ def run_uneven(args, rank, world, local_rank, dist):
     # The tile kernel's shape, timed on this batch.
     r.set_instance_transforms(static)
     shapes = []
-    for threads, regs in ((128, 64), (128, 80), (256, 64)):
+    from neraulgraphics_b200.autotune import TILE_CANDIDATES
+    for threads, regs, _, _ in TILE_CANDIDATES:
         r.set_tuning(kernel=3, threads_per_block=threads, registers=regs)
         r.render(cams, wl["fov"], 1, **kw)
         torch.cuda.synchronize()

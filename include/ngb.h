@@ -271,8 +271,8 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
  * light, no material with reflectivity >= 1e-3, at most 256 instances per world; else the persistent kernel
  * where it applies: the same without the instance limit; else the per-pixel kernel), 1 the per-pixel kernel,
  * 2 the persistent kernel where it applies, 3 the tile kernel where it applies.
- * With kernel 3 the call sets the tile kernel's shape: threads_per_block and registers as one of 128/64,
- * 128/80, 256/64 (default 128/64); refill_lanes and leaf_batch are not read.
+ * With kernel 3 the call sets the tile kernel's shape: threads_per_block and registers as one of 128/48,
+ * 128/56, 128/64, 128/80, 256/64 (default 128/56); refill_lanes and leaf_batch are not read.
  * Otherwise it sets the persistent kernel's shape: threads_per_block and registers (the register budget per
  * thread) as one of 128/48, 128/64, 128/72, 256/48, 256/64, 64/64, refill_lanes (1..32: a warp takes new
  * pixels once this many of its lanes are free) and leaf_batch (1..32: lanes at a leaf wait until this many do,

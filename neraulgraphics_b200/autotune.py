@@ -19,7 +19,7 @@ import time
 
 CANDIDATES = [(threads, regs, refill, batch) for threads, regs in ((128, 64), (256, 64), (128, 48), (64, 64))
               for refill in (16, 24, 28) for batch in (1, 8, 16, 24)]
-TILE_CANDIDATES = [(128, 64, 0, 0), (128, 80, 0, 0), (256, 64, 0, 0)]
+TILE_CANDIDATES = [(128, 48, 0, 0), (128, 56, 0, 0), (128, 64, 0, 0), (256, 64, 0, 0)]
 TILE_MAX_INSTANCES = 256
 
 

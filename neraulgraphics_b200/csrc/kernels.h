@@ -121,7 +121,7 @@ cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, 
     const PersistentTuning &t, cudaStream_t stream);
 
 // The tile render: the persistent kernel's cases, for worlds of at most TILE_MAX_INSTANCES instances (see
-// tiles.cu). Of the tuning, threads and registers are read: 128/64, 128/80 or 256/64.
+// tiles.cu). Of the tuning, threads and registers are read: 128/48, 128/56, 128/64, 128/80 or 256/64.
 constexpr int TILE_MAX_INSTANCES = 256;
 // after_camera / after_shade (may be null) are recorded on the stream after the camera and shade kernels.
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,

@@ -126,7 +126,7 @@ struct Renderer {
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
     PersistentTuning tuning{128, 28, 72, 16};
-    PersistentTuning tile_tuning{128, 0, 64, 0};
+    PersistentTuning tile_tuning{128, 0, 56, 0};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -1034,10 +1034,10 @@ int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, i
         ngb::require(kernel >= 0 && kernel <= 3,
             "kernel must be 0 (automatic), 1 (per pixel), 2 (persistent) or 3 (tiles)");
         if (kernel == 3) {
-            const bool built = (threads_per_block == 128 && (registers == 64 || registers == 80)) ||
-                (threads_per_block == 256 && registers == 64);
-            ngb::require(built, "for the tile kernel, threads_per_block and registers must be one of 128/64, 128/80, "
-                "256/64");
+            const bool built = (threads_per_block == 128 && (registers == 48 || registers == 56 || registers == 64 ||
+                registers == 80)) || (threads_per_block == 256 && registers == 64);
+            ngb::require(built, "for the tile kernel, threads_per_block and registers must be one of 128/48, 128/56, "
+                "128/64, 128/80, 256/64");
             r.kernel_choice = kernel;
             r.tile_tuning = ngb::PersistentTuning{threads_per_block, 0, registers, 0};
             return;

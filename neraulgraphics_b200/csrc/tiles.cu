@@ -734,6 +734,12 @@ cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *
     if (t.threads == 128 && t.registers == 64)
         return small ? launch_variant<128, 8, 32>(s, a, counter, stream, after_camera, after_shade)
                      : launch_variant<128, 8, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 128 && t.registers == 56)
+        return small ? launch_variant<128, 9, 32>(s, a, counter, stream, after_camera, after_shade)
+                     : launch_variant<128, 9, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+    if (t.threads == 128 && t.registers == 48)
+        return small ? launch_variant<128, 10, 32>(s, a, counter, stream, after_camera, after_shade)
+                     : launch_variant<128, 10, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
     if (t.threads == 128 && t.registers == 80)
         return small ? launch_variant<128, 6, 32>(s, a, counter, stream, after_camera, after_shade)
                      : launch_variant<128, 6, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);

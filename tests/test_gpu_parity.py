@@ -378,7 +378,7 @@ def test_tile_kernel_tunings_agree(torch_cuda):
     ref = r.render(wl.cameras, 1.0, 1, **out)
     ties = oracle_ties(wl.desc, wl.cameras, binding=wl.binding, poses=wl.poses)
     first = None
-    for threads, regs in ((128, 64), (128, 80), (256, 64)):
+    for threads, regs in ((128, 48), (128, 56), (128, 64), (128, 80), (256, 64)):
         r.set_tuning(kernel=3, threads_per_block=threads, registers=regs)
         got = r.render(wl.cameras, 1.0, 1, **out)
         assert_same_images(got, ref, ties=ties)
