@@ -151,30 +151,42 @@ class BatchRenderer:
         return t
 
     def render(self, cameras, fov=1.0, samples_per_pixel=1, *, rgb=True, depth=False, normals=False,
-               object_ids=False, frame=0, zero_copy=False, out=None):
+               object_ids=False, frame=0, zero_copy=False, out=None, into=None):
         """Render every view; returns a dict of 'rgb' (V,H,W,3) uint8, 'depth' (V,H,W) float32, 'normals'
         (V,H,W,3) float32, 'object_ids' (V,H,W) int32, for the images asked for.
 
         out: optional dict of preallocated host (NumPy) arrays, pinned or not, to copy the images into
-        (BatchRenderer::render_host, src/batch.cpp:164-178); cameras must then be on the host."""
+        (BatchRenderer::render_host, src/batch.cpp:164-178); cameras must then be on the host.
+        into: optional dict of the caller's CUDA tensors (contiguous, those shapes and dtypes, on the renderer's
+        device) to render into instead of the renderer's own buffers, queued on PyTorch's current stream (as
+        zero_copy): the caller may then copy them out while the next render runs."""
         torch = _torch()
         views, h, w = self.view_count, self.height, self.width
         if out is not None:
             return self._render_host(cameras, fov, samples_per_pixel, rgb, depth, normals, object_ids, frame, out)
         _require_count(cameras, views * 12, "cameras", f"{views} cameras of 3 x 4 numbers (camera-to-world)")
+        if into is not None:
+            zero_copy = True
         if not zero_copy and _is_cuda_tensor(cameras):
             raise ValueError("cameras on the GPU need zero_copy=True: the results then stay on the GPU too")
         outputs = ((_abi.OUTPUT_RGB if rgb else 0) | (_abi.OUTPUT_DEPTH if depth else 0) |
                    (_abi.OUTPUT_NORMAL if normals else 0) | (_abi.OUTPUT_OBJECT_ID if object_ids else 0))
+        want = {"rgb": ((views, h, w, 3), torch.uint8, rgb), "depth": ((views, h, w), torch.float32, depth),
+                "normals": ((views, h, w, 3), torch.float32, normals),
+                "object_ids": ((views, h, w), torch.int32, object_ids)}
         bufs = {}
-        if rgb:
-            bufs["rgb"] = self._buffer("rgb", (views, h, w, 3), torch.uint8)
-        if depth:
-            bufs["depth"] = self._buffer("depth", (views, h, w), torch.float32)
-        if normals:
-            bufs["normals"] = self._buffer("normals", (views, h, w, 3), torch.float32)
-        if object_ids:
-            bufs["object_ids"] = self._buffer("object_ids", (views, h, w), torch.int32)
+        for k, (shape, dtype, on) in want.items():
+            if not on:
+                continue
+            if into is None:
+                bufs[k] = self._buffer(k, shape, dtype)
+                continue
+            t = into.get(k)
+            if (t is None or not _is_cuda_tensor(t) or tuple(t.shape) != shape or t.dtype != dtype or
+                    not t.is_contiguous() or t.device.index != self._device):
+                raise ValueError(f"into['{k}'] must be a contiguous {dtype} CUDA tensor of shape {shape} on "
+                                 f"cuda:{self._device}")
+            bufs[k] = t
         p, mem, keep = self._input(cameras, "cameras")
         ptr = lambda k: C.c_void_p(bufs[k].data_ptr()) if k in bufs else None
         self._stream()
