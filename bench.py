@@ -420,6 +420,11 @@ def run_large(args, rank, world, local_rank, dist):
     lo, ld = torch.from_numpy(lidar["origins"]).to(dev), torch.from_numpy(lidar["directions"]).to(dev)
     kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    r.set_instance_transforms(mats[0])
+    tuned = None
+    if not args.no_autotune:
+        from neraulgraphics_b200.autotune import tune
+        tuned = tune(r, cams, wl.fov, rgb=True, depth=True, object_ids=True, use_cache=False, budget_s=30.0)
     for s in range(W):
         r.set_instance_transforms(mats[s])
         r.render(cams, wl.fov, 1, **kw)
@@ -469,6 +474,8 @@ def run_large(args, rank, world, local_rank, dist):
                       "render": round(statistics.median(stage[1]), 4),
                       "lidar": round(statistics.median(stage[2]), 4)},
         "lidar_rays_per_s": round(rays / (statistics.median(stage[2]) / 1000.0), 1),
+        "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
+                                                                            "leaf_batch", "ms")},
         "lidar_hit_fraction": round(hit_frac, 4),
         "reference_cuda": ref,
         "clocks": clocks.summary(),

@@ -374,26 +374,31 @@ __global__ void __launch_bounds__(128) init_bounds_kernel(int *bounds, int world
 // Matrix, inverse, record and world box of each instance, and its world's centre bounds (place_instances,
 // cuda_tlas.cuh:69-96): the per-world kernel's first step, one thread per instance.
 __global__ void __launch_bounds__(128) place_kernel(const BuildArgs a, float4 *aabb, int *bounds) {
-    const long long g = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (g >= a.n) return;
+    const long long g0 = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    const bool valid = g0 < a.n;
+    const long long g = valid ? g0 : a.n - 1;  // lanes past the end repeat the last instance's bounds
     const long long w = g / a.per_world;
     const int i = static_cast<int>(g % a.per_world);
     float m[12];
     if (a.compose) {
         compose(a, w, i, m);
-        float *mo = a.matrices_out + 12 * g;
-        for (int k = 0; k < 12; ++k) mo[k] = m[k];
+        if (valid) {
+            float *mo = a.matrices_out + 12 * g;
+            for (int k = 0; k < 12; ++k) mo[k] = m[k];
+        }
     } else {
         const float *mi = a.matrices_in + 12 * g;
         for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
     }
     float inv[12];
     invert_affine(m, inv);
-    float4 *rec = a.inst + 4 * g;
-    rec[0] = make_float4(inv[0], inv[1], inv[2], inv[3]);
-    rec[1] = make_float4(inv[4], inv[5], inv[6], inv[7]);
-    rec[2] = make_float4(inv[8], inv[9], inv[10], inv[11]);
-    rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + i)), __int_as_float(i), 0.0f, 0.0f);
+    if (valid) {
+        float4 *rec = a.inst + 4 * g;
+        rec[0] = make_float4(inv[0], inv[1], inv[2], inv[3]);
+        rec[1] = make_float4(inv[4], inv[5], inv[6], inv[7]);
+        rec[2] = make_float4(inv[8], inv[9], inv[10], inv[11]);
+        rec[3] = make_float4(__int_as_float(__ldg(a.slot_blas_root + i)), __int_as_float(i), 0.0f, 0.0f);
+    }
     const float *lb = a.slot_bounds + 6 * i;
     float b[6], lo[3] = {1e30f, 1e30f, 1e30f}, hi[3] = {-1e30f, -1e30f, -1e30f};
     for (int k = 0; k < 6; ++k) b[k] = __ldg(lb + k);
@@ -405,12 +410,22 @@ __global__ void __launch_bounds__(128) place_kernel(const BuildArgs a, float4 *a
             hi[ax] = fmaxf(hi[ax], v);
         }
     }
-    aabb[2 * g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
-    aabb[2 * g + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    if (valid) {
+        aabb[2 * g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        aabb[2 * g + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+    // The world's centre bounds: a warp whose lanes all sit in one world (a large world's case) reduces first
+    // and adds one atomic per bound; otherwise every lane adds its own.
+    const bool one_world = __all_sync(0xffffffffu, w == __shfl_sync(0xffffffffu, w, 0));
     for (int ax = 0; ax < 3; ++ax) {
-        const int c = to_ordered(0.5f * (lo[ax] + hi[ax]));
-        atomicMin(&bounds[6 * w + ax], c);
-        atomicMax(&bounds[6 * w + 3 + ax], c);
+        int cmin = to_ordered(0.5f * (lo[ax] + hi[ax])), cmax = cmin;
+        if (one_world) {
+            cmin = __reduce_min_sync(0xffffffffu, cmin);
+            cmax = __reduce_max_sync(0xffffffffu, cmax);
+            if ((threadIdx.x & 31) != 0) continue;
+        }
+        atomicMin(&bounds[6 * w + ax], cmin);
+        atomicMax(&bounds[6 * w + 3 + ax], cmax);
     }
 }
 
@@ -453,26 +468,38 @@ __global__ void __launch_bounds__(SORT_BLOCK) radix_count_kernel(const unsigned 
     if (threadIdx.x < RADIX) counts[static_cast<long long>(threadIdx.x) * blocks + blockIdx.x] = hist[threadIdx.x];
 }
 
-// Radix pass, step 2: exclusive prefix sum of the counts in place, one block.
+// Radix pass, step 2: exclusive prefix sum of the counts in place, one block: the block walks the array in
+// chunks of 1024 (coalesced), each chunk scanned with warp shuffles and a scan of the 32 warp totals.
 __global__ void __launch_bounds__(1024) radix_scan_kernel(unsigned *counts, long long total) {
-    __shared__ unsigned partial[1024];
-    const long long per = (total + 1023) / 1024;
-    const long long begin = threadIdx.x * per, end = begin + per < total ? begin + per : total;
-    unsigned sum = 0;
-    for (long long k = begin; k < end; ++k) sum += counts[k];
-    partial[threadIdx.x] = sum;
+    __shared__ unsigned warp_sum[32];
+    __shared__ unsigned carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan of the partial sums
-        const unsigned v = threadIdx.x >= off ? partial[threadIdx.x - off] : 0u;
+    for (long long base = 0; base < total; base += 1024) {
+        const long long k = base + threadIdx.x;
+        const unsigned v = k < total ? counts[k] : 0u;
+        unsigned x = v;  // inclusive scan within the warp
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
         __syncthreads();
-        partial[threadIdx.x] += v;
+        if (warp == 0) {
+            unsigned t = warp_sum[lane];
+            for (int off = 1; off < 32; off <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, t, off);
+                if (lane >= off) t += y;
+            }
+            warp_sum[lane] = t;  // inclusive over the warps
+        }
         __syncthreads();
-    }
-    unsigned run = threadIdx.x > 0 ? partial[threadIdx.x - 1] : 0u;
-    for (long long k = begin; k < end; ++k) {
-        const unsigned c = counts[k];
-        counts[k] = run;
-        run += c;
+        const unsigned before = carry + (warp > 0 ? warp_sum[warp - 1] : 0u) + x - v;
+        if (k < total) counts[k] = before;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + v;
+        __syncthreads();
     }
 }
 
