@@ -119,6 +119,9 @@ struct PersistentTuning {
 };
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
     const PersistentTuning &t, cudaStream_t stream);
+// Ray queries on the persistent kernel: each lane a ray, refilled from the queue as its walk ends.
+cudaError_t launch_rays_persistent(const SceneParams &s, const RayArgs &r, int *counter, const PersistentTuning &t,
+    cudaStream_t stream);
 
 // The tile render: the persistent kernel's cases, for worlds of at most TILE_MAX_INSTANCES instances (see
 // tiles.cu). Of the tuning, threads and registers are read: 128/48, 128/56, 128/64, 128/80 or 256/64.

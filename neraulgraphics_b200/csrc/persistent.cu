@@ -33,7 +33,8 @@ using namespace tr;
 constexpr int STACK = 128;
 constexpr int MARKER = INT_MIN;   // stack entry that returns the walk from a mesh to its world's tree
 constexpr int ST_IDLE = 0, ST_WALK = 1, ST_DONE = 2;
-constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3;
+constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3, JOB_RAY = 4;
+constexpr int KINDS_RAYS = 4;  // a launch of ray queries (cast_rays) instead of views
 constexpr unsigned FULL = 0xffffffffu;
 
 // A lane's hot state, in registers: the current ray (world space, or mesh space inside an instance), the
@@ -229,8 +230,50 @@ __device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const C
 
 // A new job from its item number. Items run over views, then 4 x 4 pixel tiles, then the pixels of a tile,
 // then (when both are asked for) the picture ray and the centre ray of a pixel.
-__device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, Lane &L, const ColdRef &cold,
-    long long item, int kinds, int tiles_x, int tiles_per_view) {
+__device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, const RayArgs &ra, Lane &L,
+    const ColdRef &cold, long long item, int kinds, int tiles_x, int tiles_per_view) {
+    if (kinds == KINDS_RAYS) {
+        // A ray query (cast_ray, src/render_core.h:331-349): the direction normalised, a miss if its length is
+        // out of range; spheres and the floor, then the meshes; a hit beyond max_distance is a miss.
+        const long long i = item;
+        const float3 o = mk3(__ldg(ra.origins + 3 * i), __ldg(ra.origins + 3 * i + 1), __ldg(ra.origins + 3 * i + 2));
+        float3 d = mk3(__ldg(ra.directions + 3 * i), __ldg(ra.directions + 3 * i + 1), __ldg(ra.directions + 3 * i + 2));
+        const float len2 = dot(d, d);
+        if (!(len2 > 1e-30f && len2 < 1e30f)) {
+            ra.distance[i] = __int_as_float(0x7f800000);
+            ra.normal[3 * i] = ra.normal[3 * i + 1] = ra.normal[3 * i + 2] = 0.0f;
+            ra.object_id[i] = OBJECT_NONE;
+            L.state = ST_IDLE;
+            return;
+        }
+        d = d * (1.0f / sqrtf(len2));
+        L.job = JOB_RAY;
+        cold.put_pix(i);
+        L.world = static_cast<int>(i / ra.rays_per_world);
+        L.o = o;
+        L.d = d;
+        float best = 1e30f;
+        int best_sphere = -1;
+        for (int k = 0; k < s.sphere_count; ++k) {
+            float t;
+            if (sphere_hit(s.spheres[k], o, d, t) && t < best) {
+                best = t;
+                best_sphere = k;
+            }
+        }
+        bool hit_floor = false;
+        float dd;
+        if (floor_hit(s.floor, o, d, best, dd)) {
+            best = dd;
+            hit_floor = true;
+        }
+        cold.i(C_SPHERE) = best_sphere;
+        cold.i(C_FLOOR) = hit_floor ? 1 : 0;
+        L.tmax = best;
+        L.any = false;
+        start_walk(s, L);
+        return;
+    }
     int job = JOB_RGB;
     if (kinds == 3) {
         job = (item & 1) ? JOB_AOV : JOB_RGB;
@@ -298,7 +341,8 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
 }
 
 // What happens when a lane's walk ends: outputs, and for a lit picture hit, its shadow ray.
-__device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, Lane &L, const ColdRef &cold) {
+__device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, const RayArgs &ra, Lane &L,
+    const ColdRef &cold) {
     const long long pix = cold.pix();
     if (L.job == JOB_SHADOW) {
         write_rgb(s.srgb_table, a.rgb, pix, cold.get3(L.blocked ? C_SHADOW : C_LIT));
@@ -332,6 +376,18 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             mat = s.spheres[best_sphere].m;
             object = OBJECT_SPHERE + best_sphere;
         }
+    }
+    if (L.job == JOB_RAY) {
+        const long long i = cold.pix();
+        const bool hit = found && L.tmax <= ra.max_distance;
+        ra.distance[i] = hit ? L.tmax : __int_as_float(0x7f800000);
+        const float3 n = hit ? normal : mk3(0.0f, 0.0f, 0.0f);
+        ra.normal[3 * i] = n.x;
+        ra.normal[3 * i + 1] = n.y;
+        ra.normal[3 * i + 2] = n.z;
+        ra.object_id[i] = hit ? object : OBJECT_NONE;
+        L.state = ST_IDLE;
+        return;
     }
     if (L.job == JOB_AOV) {  // aov_pixel (src/render_core.h:313-327)
         const size_t p = static_cast<size_t>(pix);
@@ -412,8 +468,8 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
 // compiler's unbounded choice (92).
 template <int THREADS, int MIN_BLOCKS>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(const __grid_constant__ SceneParams s,
-    const RenderArgs a, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view, int refill,
-    int leaf_batch) {
+    const RenderArgs a, const RayArgs ra, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view,
+    int refill, int leaf_batch) {
     extern __shared__ float cold_smem[];
     int st_ref[STACK], st_cnt[STACK];
     float st_t[STACK];
@@ -427,7 +483,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
     const int max_steps = cap > INT_MAX ? INT_MAX : static_cast<int>(cap);
     bool exhausted = false;
     for (;;) {
-        if (L.state == ST_DONE) complete(s, a, L, cold);
+        if (L.state == ST_DONE) complete(s, a, ra, L, cold);
         const unsigned idle = __ballot_sync(FULL, L.state == ST_IDLE);
         if (!exhausted && idle != 0 && (__popc(idle) >= refill || idle == FULL)) {
             const int k = __popc(idle);
@@ -438,7 +494,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
             if (base + k >= total) exhausted = true;
             if (L.state == ST_IDLE) {
                 const long long item = base + __popc(idle & lanes_below);
-                if (item < total) start_job(s, a, L, cold, item, kinds, tiles_x, tiles_per_view);
+                if (item < total) start_job(s, a, ra, L, cold, item, kinds, tiles_x, tiles_per_view);
             }
         }
         const unsigned busy = __ballot_sync(FULL, L.state != ST_IDLE);
@@ -461,12 +517,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
             const bool leaf_phase = __popc(at_leaf) >= leaf_batch || at_inner == 0;
             if (walking && (L.count != 0) == leaf_phase) {
                 if (++L.steps > max_steps) {  // a lane's own steps; only a malformed tree gets past the cap
-                    *a.error_flag = 2;
+                    *(kinds == KINDS_RAYS ? ra.error_flag : a.error_flag) = 2;
                     L.state = ST_DONE;
                 } else if (leaf_phase) {
-                    walk_leaf(s, L, cold, st_ref, st_cnt, st_t, a.error_flag);
+                    walk_leaf(s, L, cold, st_ref, st_cnt, st_t, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
                 } else {
-                    walk_inner(s, L, cold, st_ref, st_cnt, st_t, a.error_flag);
+                    walk_inner(s, L, cold, st_ref, st_cnt, st_t, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
                 }
             }
         }
@@ -474,13 +530,15 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
 }
 
 template <int THREADS, int MIN_BLOCKS>
-cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, int refill, int leaf_batch,
-    cudaStream_t stream) {
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayArgs *rays, int *counter, int refill,
+    int leaf_batch, cudaStream_t stream) {
     const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
     const int tiles_per_view = tiles_x * tiles_y;
-    const int kinds = (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
+    const int kinds = rays ? KINDS_RAYS : (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
     if (kinds == 0) return cudaSuccess;
-    const long long total = 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
+    const long long total = rays ? rays->count : 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
+    if (total == 0) return cudaSuccess;
+    const RayArgs ra = rays ? *rays : RayArgs{};
     auto kernel = render_persistent_kernel<THREADS, MIN_BLOCKS>;
     const size_t smem = static_cast<size_t>(C_FIELDS) * THREADS * sizeof(float);
     int device = 0, sms = 0, per_sm = 0;
@@ -495,25 +553,37 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
-    if (e != cudaSuccess) return e;
-    kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, counter, total, kinds, tiles_x, tiles_per_view,
-        refill, leaf_batch);
+    if (!rays) {
+        e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+        if (e != cudaSuccess) return e;
+    }
+    kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, ra, counter, total, kinds, tiles_x,
+        tiles_per_view, refill, leaf_batch);
     return cudaGetLastError();
 }
 
 }  // namespace
 
+// (threads per CTA, register budget) -> the instantiation with that budget; rays: a launch of ray queries.
+cudaError_t launch_persistent(const SceneParams &s, const RenderArgs &a, const RayArgs *rays, int *counter,
+    const PersistentTuning &t, cudaStream_t stream) {
+    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 128 && t.registers == 72) return launch_variant<128, 7>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 256 && t.registers == 48) return launch_variant<256, 5>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    if (t.threads == 64 && t.registers == 64) return launch_variant<64, 16>(s, a, rays, counter, t.refill, t.leaf_batch, stream);
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream) {
-    // (threads per CTA, register budget) -> the instantiation with that budget.
-    if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8>(s, a, counter, t.refill, t.leaf_batch, stream);
-    if (t.threads == 128 && t.registers == 72) return launch_variant<128, 7>(s, a, counter, t.refill, t.leaf_batch, stream);
-    if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10>(s, a, counter, t.refill, t.leaf_batch, stream);
-    if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4>(s, a, counter, t.refill, t.leaf_batch, stream);
-    if (t.threads == 256 && t.registers == 48) return launch_variant<256, 5>(s, a, counter, t.refill, t.leaf_batch, stream);
-    if (t.threads == 64 && t.registers == 64) return launch_variant<64, 16>(s, a, counter, t.refill, t.leaf_batch, stream);
-    return cudaErrorInvalidValue;
+    return launch_persistent(s, a, nullptr, counter, t, stream);
+}
+
+cudaError_t launch_rays_persistent(const SceneParams &s, const RayArgs &r, int *counter, const PersistentTuning &t,
+    cudaStream_t stream) {
+    return launch_persistent(s, RenderArgs{}, &r, counter, t, stream);
 }
 
 }  // namespace ngb

@@ -720,7 +720,9 @@ void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, flo
     a.error_flag = error_flag.p;
     const bool timed = !capturing();
     if (timed) CK(cudaEventRecord(ev_start, stream));
-    CK(launch_rays(params, a, stream));
+    // The persistent kernel's lane-refilling walk; the per-thread kernel when the per-pixel kernel is chosen.
+    if (kernel_choice == 1) CK(launch_rays(params, a, stream));
+    else CK(launch_rays_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
     if (timed) {
         stages = 1;
         CK(cudaEventRecord(ev_stop, stream));

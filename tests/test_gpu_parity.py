@@ -467,3 +467,26 @@ def test_uneven_worlds_are_each_worlds_own_render(torch_cuda):
             o.set_instance_transforms(m)
         want = o.render(cams[w:w + 1], 1.0, 1, **ALL, frame=2, ties=True)
         assert_same_images(mine, want, ties=want["ties"])
+
+
+def test_ray_queries_on_both_kernels(torch_cuda):
+    """Ray queries through the persistent kernel's walk (the default) and the per-thread kernel: the same
+    distances, normals and IDs, with rays of zero length, rays stopped by max_distance and rays in worlds
+    of their own."""
+    wl = workloads.body_worlds(worlds=8, seed=6)
+    r, o = product(wl.desc), O.Oracle(wl.desc)
+    for x in (r, o):
+        x.bind_bodies(**wl.binding)
+        x.set_body_poses(wl.poses)
+    rng = np.random.default_rng(3)
+    origins = rng.uniform(-3.0, 3.0, size=(8, 500, 3)).astype(np.float32)
+    dirs = rng.normal(size=(8, 500, 3)).astype(np.float32)
+    dirs[:, ::50] = 0.0  # no direction: a miss
+    want = o.cast_rays(origins, dirs, 4.0)
+    got = r.cast_rays(origins, dirs, 4.0)
+    r.set_tuning(kernel=1)
+    per_thread = r.cast_rays(origins, dirs, 4.0)
+    assert (want["object_id"] > 0).mean() > 0.2 and np.isinf(want["distance"]).mean() > 0.1
+    for k in ("object_id", "distance", "normal"):
+        assert np.array_equal(np.asarray(got[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
+        assert np.array_equal(np.asarray(per_thread[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
