@@ -28,9 +28,10 @@ class _DepthNormals(torch.autograd.Function):
         c = cameras.detach().contiguous()
         renderer.set_instance_transforms(m)
         renderer.record_hits(True)
-        out = renderer.render(c, fov, 1, rgb=False, depth=True, normals=True, zero_copy=True)
-        depth = out["depth"].clone()
-        normals = out["normals"].clone()
+        views, h, w = renderer.view_count, renderer.height, renderer.width
+        depth = torch.empty((views, h, w), dtype=torch.float32, device=m.device)
+        normals = torch.empty((views, h, w, 3), dtype=torch.float32, device=m.device)
+        renderer.render(c, fov, 1, rgb=False, depth=True, normals=True, into={"depth": depth, "normals": normals})
         hits = (torch.empty(depth.shape, dtype=torch.int32, device=depth.device),
                 torch.empty(depth.shape, dtype=torch.int32, device=depth.device),
                 torch.empty(depth.shape, dtype=torch.float32, device=depth.device),

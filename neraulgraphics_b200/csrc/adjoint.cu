@@ -85,7 +85,7 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-__global__ void __launch_bounds__(ADJ_THREADS) depth_normal_adjoint_kernel(const __grid_constant__ SceneParams s,
+__global__ void __launch_bounds__(ADJ_THREADS, 4) depth_normal_adjoint_kernel(const __grid_constant__ SceneParams s,
     const AdjointArgs a, int tiles_x, int tiles_per_view, bool shared_sums) {
     extern __shared__ float sums[];  // per instance of the world 12, then the camera's 12
     const int view = blockIdx.x / tiles_per_view;
