@@ -107,6 +107,11 @@ struct SceneParams {
     const float *slot_bounds;  // per slot: its mesh's box in mesh space, 6 floats
     int tlas_internal;         // n - 1: nodes below this index are internal
     const float *srgb_table;   // 256 sRGB byte thresholds made on the host (see host.h: srgb_thresholds)
+    // Per slot (per instance for uneven worlds): its mesh's vertex mean in mesh space and, in w, its radius
+    // when the mesh is convex, else -1 (host.h: mesh_hull). Per instance: its leaf's position among the sorted
+    // leaves (leaf node n - 1 + leaf_of[g]).
+    const float4 *slot_hull;
+    const int *leaf_of;
 };
 
 // The first instance of world w, its instance count, and the slot-table entry of its instance g.

@@ -394,6 +394,42 @@ BuiltMeshes build_meshes(const ngb_scene &s) {
     return out;
 }
 
+std::array<float, 4> mesh_hull(const ngb_mesh &mesh) {
+    const int V = mesh.vertex_count, T = mesh.index_count / 3;
+    double c[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < V; ++i)
+        for (int k = 0; k < 3; ++k) c[k] += mesh.vertices[3 * i + k];
+    for (int k = 0; k < 3; ++k) c[k] /= std::max(V, 1);
+    double radius = 0.0;
+    for (int i = 0; i < V; ++i) {
+        double d2 = 0.0;
+        for (int k = 0; k < 3; ++k) d2 += (mesh.vertices[3 * i + k] - c[k]) * (mesh.vertices[3 * i + k] - c[k]);
+        radius = std::max(radius, std::sqrt(d2));
+    }
+    std::array<float, 4> out = {static_cast<float>(c[0]), static_cast<float>(c[1]), static_cast<float>(c[2]), -1.0f};
+    if (V == 0 || T == 0 || radius <= 0.0 || static_cast<double>(T) * V > 33554432.0) return out;
+    for (int t = 0; t < T; ++t) {
+        const float *a = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t]);
+        const float *b = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t + 1]);
+        const float *d = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t + 2]);
+        const double e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {d[0] - a[0], d[1] - a[1], d[2] - a[2]};
+        double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        const double len = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (!(len > 0.0)) return out;  // a degenerate triangle: no plane to test against
+        for (double &x : n) x /= len;
+        const double side = (c[0] - a[0]) * n[0] + (c[1] - a[1]) * n[1] + (c[2] - a[2]) * n[2];
+        if (std::fabs(side) < 1e-3 * radius) return out;
+        const double s = side > 0.0 ? 1.0 : -1.0;
+        for (int i = 0; i < V; ++i) {
+            const float *v = mesh.vertices + 3 * static_cast<size_t>(i);
+            const double h = ((v[0] - a[0]) * n[0] + (v[1] - a[1]) * n[1] + (v[2] - a[2]) * n[2]) * s;
+            if (h < -1e-6 * radius) return out;
+        }
+    }
+    out[3] = static_cast<float>(radius);
+    return out;
+}
+
 uint8_t srgb_byte(float v) {
     const float x = std::fmin(std::fmax(v, 0.0f), 1.0f);
     const float c = x <= 0.0031308f ? 12.92f * x : 1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f;

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <stdexcept>
+#include <array>
 #include <string>
 #include <vector>
 
@@ -59,6 +60,12 @@ struct BuiltMeshes {
 };
 
 BuiltMeshes build_meshes(const ngb_scene &s);
+
+// A mesh's hull facts for the shadow rays: the vertices' mean (x, y, z) and, in w, their largest distance from
+// it when the mesh is convex (every vertex on the mean's side of every triangle's plane, within 1e-6 of that
+// distance, and the mean at least 1e-3 of it inside), else -1. Meshes above 2^25 triangle-vertex pairs are
+// not checked (-1).
+std::array<float, 4> mesh_hull(const ngb_mesh &mesh);
 
 // The sRGB byte of a linear value, (uint8)(saturate(srgb(saturate(v))) * 255 + 0.5) with srgb's 1/2.4 power
 // taken by the host's powf (src/geom_dev.h:169-182, render_core.h:280-282), as 255 thresholds: t[k] (k = 1..255)

@@ -35,6 +35,7 @@ struct BuildArgs {
     // Worlds of uneven sizes (the per-world build only; per_world is then the largest): world w's instances
     // are [world_first[w], world_first[w + 1]) and the slot tables hold one entry per instance. Null: uniform.
     const int *world_first;
+    int *leaf_of;                  // n: each instance's sorted position, or null
 };
 
 // Group size (threads per world) of the per-world build: a power of two, at least 32.
@@ -84,6 +85,7 @@ struct RenderArgs {
     int *pic_code;                 // its object code, then the shadowed pixel's bytes
     float4 *shadow_o;              // the shadow ray's origin and length (0: no shadow ray)
     float4 *shadow_d;              // its direction and the lit pixel's bytes
+    int *shadow_self;              // the shadow ray's own instance: instance * 4 + mode (1 skip, 2 first), or -1
     // Views of uneven sizes (tile kernels only): per view (width, height, first pixel, first tile), with the
     // totals; null when every view is width x height.
     const int4 *view_info;

@@ -219,6 +219,7 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
         sm.key[rank] = morton;
         sm.sorted[rank] = i;
         a.sorted_ids[base + rank] = static_cast<int>(g);
+        if (a.leaf_of) a.leaf_of[g] = static_cast<int>(base + rank);
         for (int ax = 0; ax < 3; ++ax) {
             sm.box[G + rank][ax] = lo[ax];
             sm.box[G + rank][3 + ax] = hi[ax];
@@ -534,6 +535,7 @@ __global__ void __launch_bounds__(128) leaves_kernel(const BuildArgs a, const in
     if (k >= a.n) return;
     const int g = ids_sorted[k];
     a.sorted_ids[k] = g;
+    if (a.leaf_of) a.leaf_of[g] = static_cast<int>(k);
     const float4 lo = aabb[2 * static_cast<long long>(g)], hi = aabb[2 * static_cast<long long>(g) + 1];
     float4 *leaf = a.tlas + 2 * (a.n - 1 + k);
     leaf[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(~g));

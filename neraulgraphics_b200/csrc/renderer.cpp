@@ -109,7 +109,8 @@ struct Renderer {
     DevBuf<float> matrices;
     DevBuf<float4> inst, tlas;
     DevBuf<unsigned long long> keys;
-    DevBuf<int> sorted_ids, roots, parent, arrivals;
+    DevBuf<int> sorted_ids, roots, parent, arrivals, leaf_of;
+    DevBuf<float4> slot_hull;
     // The global build's scratch (worlds of more than MAX_PER_WORLD instances, or when asked for).
     int build_mode = 0;  // 0: automatic, 1: the per-world build, 2: the global build
     DevBuf<float4> large_aabb;
@@ -121,7 +122,7 @@ struct Renderer {
     DevBuf<unsigned long long> work_counter;  // the persistent render's job counter
     DevBuf<float4> camera_basis;              // the persistent and tile renders' per-view cameras
     DevBuf<float4> pic_hit, shadow_o, shadow_d;  // the tile render's per-pixel hand-over between its kernels
-    DevBuf<int> pic_code;
+    DevBuf<int> pic_code, shadow_self;
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
@@ -361,6 +362,13 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
         material_of_slot[i] = dev_material(s.instances[i].material);
     }
     upload(slot_blas_root, root_of_slot);
+    std::vector<float4> hull_of_mesh(s.mesh_count), hull_of_slot(slots);
+    for (int m = 0; m < s.mesh_count; ++m) {
+        const std::array<float, 4> h = mesh_hull(s.meshes[m]);
+        hull_of_mesh[m] = make_float4(h[0], h[1], h[2], h[3]);
+    }
+    for (int i = 0; i < slots; ++i) hull_of_slot[i] = hull_of_mesh[s.instances[i].mesh];
+    upload(slot_hull, hull_of_slot);
     std::vector<int> tri_base_of_slot(slots);
     for (int i = 0; i < slots; ++i) tri_base_of_slot[i] = mesh_base[s.instances[i].mesh];
     upload(slot_tri_base, tri_base_of_slot);
@@ -381,6 +389,7 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
     sorted_ids.ensure(n);
     roots.ensure(worlds);
     parent.ensure(2 * n - 1);
+    leaf_of.ensure(n);
     arrivals.ensure(std::max<long long>(n - 1, 1));
     CK(cudaMemset(parent.p, 0xFF, (2 * n - 1) * sizeof(int)));
     CK(cudaMemset(arrivals.p, 0, arrivals.n * sizeof(int)));
@@ -398,6 +407,8 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
     params.slot_root = slot_root.p;
     params.slot_bounds = slot_bounds.p;
     params.tlas_internal = static_cast<int>(n - 1);
+    params.slot_hull = slot_hull.p;
+    params.leaf_of = leaf_of.p;
 
     // Every world starts with the transforms the instances were given (src/cuda_backend.cu:765-770).
     std::vector<float> initial(12 * n);
@@ -436,7 +447,8 @@ Renderer::~Renderer() {
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
-    pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release();
+    pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release(), shadow_self.release();
+    leaf_of.release(), slot_hull.release();
     camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
@@ -511,6 +523,7 @@ void Renderer::build(const float *matrices_in, bool compose, const float *poses)
     a.error_flag = error_flag.p;
     a.tlas_pairs = tlas_pairs.p;
     a.world_first = uneven ? world_first.p : nullptr;
+    a.leaf_of = leaf_of.p;
     if (use_large_build()) {
         LargeBuildScratch t{};
         t.aabb = large_aabb.ensure(2 * n);
@@ -668,6 +681,7 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
             a.pic_code = pic_code.ensure(pixels());
             a.shadow_o = shadow_o.ensure(pixels());
             a.shadow_d = shadow_d.ensure(pixels());
+            a.shadow_self = shadow_self.ensure(pixels());
         }
         CK(launch_render_tiles(params, a, reinterpret_cast<int *>(work_counter.p), tile_tuning, stream,
             timed ? ev_stage[0] : nullptr, timed ? ev_stage[1] : nullptr));

@@ -451,6 +451,40 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
     }
 }
 
+// Whether a shadow ray that leaves a mesh hit cannot meet that mesh again: the mesh is convex (host.h:
+// mesh_hull), the hit face's normal facing the picture ray points away from the mesh's body, the shading normal
+// agrees with it (so the ray starts 1e-3 * cos above the face's plane) and the ray moves away from that plane.
+// The whole body lies below the plane, within 1e-6 of its radius, so no triangle of it can be met; the margin
+// asked of the start (at least 1e-4 with the shading normal within 84 degrees of the face's) stays far above
+// the rounding of the coordinates and of the convexity test.
+__device__ __forceinline__ bool shadow_misses_own_mesh(const SceneParams &s, int world, int g, int tri, float hu,
+    float hv, float3 dir, float3 shading, float3 light_dir, float3 point) {
+    const float4 hull = __ldg(s.slot_hull + table_of(s, g, world));
+    if (!(hull.w > 0.0f)) return false;
+    const float4 *rec = s.inst + 4LL * g;
+    const float3 r0 = xyz(__ldg(rec)), r1 = xyz(__ldg(rec + 1)), r2 = xyz(__ldg(rec + 2));
+    const float3 v0 = xyz(__ldg(s.tris + 3LL * tri)), e1 = xyz(__ldg(s.tris + 3LL * tri + 1));
+    const float3 e2 = xyz(__ldg(s.tris + 3LL * tri + 2));
+    const float3 nl = cross(e1, e2);
+    const float3 nw = r0 * nl.x + r1 * nl.y + r2 * nl.z;  // the face normal in the world (inverse-transpose)
+    const float nw_len = sqrtf(dot(nw, nw)), nl_len = sqrtf(dot(nl, nl));
+    float3 ng = nw * (1.0f / nw_len);
+    float sigma = 1.0f;
+    if (dot(ng, dir) > 0.0f) {
+        ng = -ng;
+        sigma = -1.0f;
+    }
+    const float3 pl = v0 + e1 * hu + e2 * hv;
+    if (!(dot(mk3(hull.x, hull.y, hull.z) - pl, nl) * sigma < -5e-4f * hull.w * nl_len)) return false;
+    const float cos_sg = dot(shading, ng);
+    if (!(cos_sg > 0.1f) || !(dot(light_dir, ng) > 0.0f)) return false;
+    // A vertex h above the face's plane in the mesh's frame (along the unit normal) lies h * |nl| / |nw| above it
+    // in the world.
+    const float above = 1e-6f * hull.w * nl_len / nw_len;
+    const float mag = fmaxf(fmaxf(fabsf(point.x), fabsf(point.y)), fmaxf(fabsf(point.z), 1.0f));
+    return 1e-3f * cos_sg > 2e-5f * mag + above;
+}
+
 // Shade kernel: one thread per pixel, straight-line code. The picture ray's hit resolved and lit (trace's
 // first bounce, src/render_core.h:202-245): a pixel with nothing left to trace gets its bytes here; a lit
 // surface leaves its shadow ray (origin, light distance) (direction, lit bytes) and its shadowed bytes (over
@@ -485,6 +519,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
         const int code = a.pic_code[p];
         const float4 h = a.pic_hit[p];
         float3 radiance;
+        float3 self_normal = zero, self_point = zero;  // the picture hit's shading normal and point
         bool pending = false;
         float3 so = zero, sd = zero;
         float sdist = 0.0f;
@@ -503,6 +538,8 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
             DevMaterial mat;
             int object;
             resolve(s, world, point, d, hit_inst, __float_as_int(h.w), h.y, h.z, best_sphere, hit_floor, normal, mat, object);
+            self_normal = normal;
+            self_point = point;
             radiance = radiance_of(mat, s.ambient, zero, zero);
             if (s.light_count == 1) {
                 const DevLight &lt = s.lights[0];
@@ -545,6 +582,16 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
         const int bytes = rgb_bytes(s.srgb_table, radiance);
         if (pending) {
             lit_bytes = bytes;
+            // The shadow ray's own mesh: walked first when the ray starts on its body's side (the light is behind
+            // the surface), left out when it cannot be met (shadow_misses_own_mesh), else walked in turn.
+            int self = -1;
+            if (code >= 0) {
+                if (dot(sd, self_normal) < 0.0f) self = code * 4 + 2;
+                else if (shadow_misses_own_mesh(s, world, code, __float_as_int(h.w), h.y, h.z, d, self_normal, sd,
+                             self_point))
+                    self = code * 4 + 1;
+            }
+            a.shadow_self[p] = self;
             a.shadow_o[p] = make_float4(so.x, so.y, so.z, sdist);
             a.shadow_d[p] = make_float4(sd.x, sd.y, sd.z, __int_as_float(lit_bytes));
             a.pic_code[p] = shadow_bytes;
@@ -645,18 +692,32 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 ncand += __popc(cmask);
             }
             __syncwarp();
+            // The ray's own mesh first when the shade kernel found it starts on that body's side, or not at all when
+            // it cannot meet it; any hit ends the ray whatever the order, so the answer is the same.
+            const int self_code = pending ? a.shadow_self[T.pix] : -1;
+            const int self = self_code >= 0 ? self_code >> 2 : -1;
             bool blocked = false;
             const float3 sinv = safe_inverse(sd);
+            if (self_code >= 0 && (self_code & 3) == 2) {
+                const float4 *leaf = s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + __ldg(s.leaf_of + self));
+                if (box_entry(__ldg(leaf), __ldg(leaf + 1), so, sinv, sdist) < NO_HIT) {
+                    float tm = sdist, hu, hv;
+                    int ht;
+                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd, tm,
+                        true, ht, hu, hv, max_steps, a.error_flag);
+                }
+            }
             for (int c = 0; c < ncand; ++c) {
                 const bool open = pending && !blocked;
                 if (!__any_sync(FULL, open)) break;
                 const float4 *leaf = leaves + 2 * cand_leaf[c];
                 const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
-                if (open && box_entry(lo, hi, so, sinv, sdist) < NO_HIT) {
+                const int id = ~__float_as_int(lo.w);
+                if (open && id != self && box_entry(lo, hi, so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, ~__float_as_int(lo.w),
-                        so, sd, tm, true, ht, hu, hv, max_steps, a.error_flag);
+                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, so, sd, tm,
+                        true, ht, hu, hv, max_steps, a.error_flag);
                 }
             }
             if (pending) put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));

@@ -490,3 +490,65 @@ def test_ray_queries_on_both_kernels(torch_cuda):
     for k in ("object_id", "distance", "normal"):
         assert np.array_equal(np.asarray(got[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
         assert np.array_equal(np.asarray(per_thread[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
+
+
+def l_prism(depth=0.6):
+    """A concave mesh: an L-shaped outline (2 x 2 with a 1 x 1 notch) extruded along z, 20 triangles."""
+    outline = np.float32([[0, 0], [2, 0], [2, 1], [1, 1], [1, 2], [0, 2]]) - np.float32(0.8)
+    verts = np.concatenate([np.c_[outline, np.full(6, -depth)], np.c_[outline, np.full(6, depth)]]).astype(np.float32)
+    tris = [(0, i, i + 1) for i in range(1, 5)] + [(6, 6 + i + 1, 6 + i) for i in range(1, 5)]
+    for i in range(6):
+        j = (i + 1) % 6
+        tris += [(i, j, 6 + j), (i, 6 + j, 6 + i)]
+    return ng.Mesh(verts, np.uint32(tris))
+
+
+def open_bowl(radius=0.7, rings=6, segments=16):
+    """An open mesh: the lower half of a sphere, without a lid, so it is seen from inside and outside."""
+    verts = [(0.0, -radius, 0.0)]
+    for k in range(1, rings + 1):
+        a = 0.5 * np.pi * k / rings
+        for j in range(segments):
+            b = 2 * np.pi * j / segments
+            verts.append((radius * np.sin(a) * np.cos(b), -radius * np.cos(a), radius * np.sin(a) * np.sin(b)))
+    tris = [(0, 1 + j, 1 + (j + 1) % segments) for j in range(segments)]
+    for k in range(1, rings):
+        a0, a1 = 1 + (k - 1) * segments, 1 + k * segments
+        for j in range(segments):
+            jn = (j + 1) % segments
+            tris += [(a0 + j, a1 + j, a1 + jn), (a0 + j, a1 + jn, a0 + jn)]
+    return ng.Mesh(np.float32(verts), np.uint32(tris))
+
+
+@pytest.mark.parametrize("light_y", [20.0, -1.0])
+def test_shadows_of_convex_concave_and_open_meshes(torch_cuda, light_y):
+    """Shadow rays leaving convex meshes (box, smooth icosphere), a concave one (an L prism, which shadows
+    itself) and an open bowl, under shears and uneven scales, with the light high (most surfaces lit) and low
+    (many lit from behind, the shadow ray starting inside its own mesh): the oracle's images on every kernel."""
+    rng = np.random.default_rng(21)
+    meshes = [ng.make_box((0.5, 0.3, 0.4)), ng.make_icosphere(0.6, 2), l_prism(), open_bowl()]
+    per_world, worlds = 12, 6
+    instances = [ng.Instance(i % 4, material=ng.Material(diffuse_color=workloads.PALETTE[i % 8])) for i in range(per_world)]
+    floor = ng.Plane(y=-2.0, half_extent_x=10.0, z_min=-20.0, z_max=2.0, checker_scale=1.0)
+    lights = [ng.Light((3.0, light_y, -2.0), 1.5, 0.0)]
+    desc = ng.SceneDesc(48, 40, worlds, 1, [], lights, floor, meshes, instances)
+    mats = np.empty((worlds, per_world, 3, 4), np.float32)
+    for w in range(worlds):
+        for i in range(per_world):
+            m = ng.make_transform(rng.uniform([-2.5, -1.5, -8.0], [2.5, 1.5, -4.0]), rng.normal(size=4),
+                                  1.0).matrix
+            shear = np.eye(3, dtype=np.float32) + np.float32(rng.uniform(-0.4, 0.4, (3, 3)) * (1 - np.eye(3)))
+            m[:, :3] = m[:, :3] @ (shear * np.float32(rng.uniform(0.5, 1.5, 3)))
+            mats[w, i] = m
+    cams = np.stack([workloads.camera_matrix(rng.uniform(-0.5, 0.5, 3) + (0.0, 1.0, 0.0), (0.0, 0.0, -6.0), 48, 40,
+                                             1.0) for _ in range(worlds)]).astype(np.float32)
+    o = O.Oracle(desc)
+    o.set_instance_transforms(mats)
+    want = o.render(cams, 1.0, 1, **ALL, ties=True)
+    ids = want["object_ids"]
+    assert len(np.unique(ids[ids > 0])) >= 10  # most instances and the floor are in view
+    for kernel in (1, 2, 3):
+        r = product(desc)
+        r.set_tuning(kernel=kernel, threads_per_block=128, refill_lanes=8, registers=64)
+        r.set_instance_transforms(mats)
+        assert_same_images(r.render(cams, 1.0, 1, **ALL), want, ties=want["ties"] if kernel == 3 else None)
