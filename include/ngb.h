@@ -11,6 +11,7 @@
  *   BatchRenderer::set_instance_transforms  batch.h:79, backend.h:62      ngb_set_instance_transforms
  *   BatchRenderer::bind_bodies     batch.h:84, backend.h:63               ngb_bind_bodies
  *   BatchRenderer::set_body_poses  batch.h:90, backend.h:65               ngb_set_body_poses
+ *   MJWarpBatchRenderer.update     python/neraulgraphics/mujoco.py:304-314  ngb_bind_geoms / ngb_set_geom_poses
  *   BatchRenderer::render          batch.h:103-104, backend.h:67-68       ngb_render / ngb_render_into
  *   BatchRenderer::render_host     batch.h:105-106                        ngb_render_host
  *   BatchRenderer::cast_rays       batch.h:110-111, backend.h:69-70       ngb_cast_rays
@@ -220,6 +221,18 @@ int ngb_bind_bodies(ngb_renderer *r, int32_t bodies_per_world, const int32_t *bo
  * matrix and rebuilds the trees, in one launch. Replaces BatchRenderer::set_body_poses
  * (src/batch.cpp:131-144) and CudaBackend::set_body_poses (src/cuda_backend.cu:493-507). */
 int ngb_set_body_poses(ngb_renderer *r, const float *body_poses, int32_t memory);
+
+/* How a MuJoCo (or MuJoCo Warp) model's geoms carry the instances: per instance of a world, its geom index
+ * in [0, geoms_per_world) and its scale (x, y, z). Host arrays. Replaces the geom list and scales that
+ * MJWarpBatchRenderer keeps (python/neraulgraphics/mujoco.py:199-243). Replaces a body binding. */
+int ngb_bind_geoms(ngb_renderer *r, int32_t geoms_per_world, const int32_t *geom_of_instance, const float *scale);
+
+/* Every geom's world position and rotation as a simulator's data holds them: geom_xpos world_count x
+ * geoms_per_world x 3 floats and geom_xmat world_count x geoms_per_world x 9 floats (row-major 3x3), world-major,
+ * both in memory. Each instance's matrix is [R * diag(scale) | p] of its geom, composed inside the tree build's
+ * launch: the same matrices as MJWarpBatchRenderer's compose kernel followed by set_instance_transforms
+ * (python/neraulgraphics/mujoco.py:287-314), without that kernel or the matrices' round trip through memory. */
+int ngb_set_geom_poses(ngb_renderer *r, const float *geom_xpos, const float *geom_xmat, int32_t memory);
 
 /* ---- rendering ------------------------------------------------------------------------------------- */
 

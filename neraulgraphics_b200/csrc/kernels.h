@@ -13,13 +13,18 @@ struct BuildArgs {
     int worlds;
     int per_world;
     long long n;                   // worlds * per_world
-    int compose;                   // 1: matrices from body poses; 0: matrices_in
+    int compose;                   // 0: matrices_in; 1: matrices from body poses; 2: from geom poses
     const float *matrices_in;      // n x 12, when !compose
     const float *body_poses;       // worlds x bodies_per_world x 7, when compose
     const int *body_of_instance;   // per slot
     const float *local_pose;       // per slot, 7
     const float *local_scale;      // per slot, 3
     int bodies_per_world;
+    const float *geom_xpos;        // worlds x geoms_per_world x 3, when compose == 2
+    const float *geom_xmat;        // worlds x geoms_per_world x 9, when compose == 2
+    const int *geom_of_instance;   // per slot, when compose == 2
+    const float *geom_scale;       // per slot, 3, when compose == 2
+    int geoms_per_world;
     float *matrices_out;           // n x 12, written when compose
     const float *slot_bounds;      // per slot: its mesh's box in mesh space, 6
     const int *slot_blas_root;     // per slot

@@ -42,8 +42,24 @@ __device__ __forceinline__ void quat_matrix(const float *q, float *r) {
     r[8] = 1 - 2 * (x * x + y * y);
 }
 
+// An instance's matrix from its geom's position and rotation and its scale, [R * diag(s) | p]: the products
+// of MJWarpBatchRenderer's compose kernel (python/neraulgraphics/mujoco.py:291-302).
+__device__ __forceinline__ void compose_geom(const BuildArgs &a, long long w, int i, float *m) {
+    const long long geom = w * a.geoms_per_world + __ldg(a.geom_of_instance + i);
+    const float *p = a.geom_xpos + 3 * geom, *r = a.geom_xmat + 9 * geom, *sc = a.geom_scale + 3 * i;
+    const float s[3] = {__ldg(sc), __ldg(sc + 1), __ldg(sc + 2)};
+    for (int row = 0; row < 3; ++row) {
+        for (int col = 0; col < 3; ++col) m[4 * row + col] = __ldg(r + 3 * row + col) * s[col];
+        m[4 * row + 3] = __ldg(p + row);
+    }
+}
+
 // An instance's matrix from its body's pose, its own offset and its scale (src/cuda_backend.cu:176-202).
 __device__ __forceinline__ void compose(const BuildArgs &a, long long w, int i, float *m) {
+    if (a.compose == 2) {
+        compose_geom(a, w, i, m);
+        return;
+    }
     const float *lp = a.local_pose + 7 * i, *sc = a.local_scale + 3 * i;
     float lpv[7], scv[3];
     for (int k = 0; k < 7; ++k) lpv[k] = __ldg(lp + k);

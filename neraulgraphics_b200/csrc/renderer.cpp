@@ -133,6 +133,11 @@ struct Renderer {
     int bodies_per_world = 0;
     DevBuf<int> body_of_instance;
     DevBuf<float> local_pose, local_scale, body_poses;
+    // Geoms carrying the instances (bind_geoms): per slot its geom and scale, and host poses' device copies.
+    int geoms_per_world = 0;
+    bool geoms_bound = false;
+    DevBuf<int> geom_of_instance;
+    DevBuf<float> geom_scale, geom_xpos, geom_xmat;
     // Staging for host inputs and the renderer's own outputs.
     DevBuf<float> cameras, ray_origins, ray_directions;
     DevBuf<uint8_t> out_rgb;
@@ -166,7 +171,7 @@ struct Renderer {
     explicit Renderer(const ngb_scene &s, const UnevenLayout *layout = nullptr);
     ~Renderer();
 
-    void build(const float *matrices_in, bool compose, const float *poses);
+    void build(const float *matrices_in, int compose, const float *poses, const float *xmat = nullptr);
     void finish();
     void read_timing();
     // Whether the stream is being captured into a CUDA graph.
@@ -179,6 +184,8 @@ struct Renderer {
     void set_instance_transforms(const float *m, int memory);
     void bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc);
     void set_body_poses(const float *poses, int memory);
+    void bind_geoms(int gpw, const int32_t *goi, const float *sc);
+    void set_geom_poses(const float *xpos, const float *xmat, int memory);
     void check_render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory);
     void render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
         float *depth, float *normal, int32_t *ids);
@@ -420,7 +427,7 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
                 std::memcpy(&initial[12 * (static_cast<size_t>(w) * per_world + i)], s.instances[i].transform, 48);
     }
     CK(cudaMemcpy(matrices.p, initial.data(), initial.size() * sizeof(float), cudaMemcpyHostToDevice));
-    build(matrices.p, false, nullptr);
+    build(matrices.p, 0, nullptr);
     CK(cudaEventRecord(ev_done, stream));
     wait(ev_done, timeout);
 }
@@ -444,6 +451,7 @@ Renderer::~Renderer() {
     slot_bounds.release(), slot_material.release(), matrices.release(), inst.release(), tlas.release();
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
+    geom_of_instance.release(), geom_scale.release(), geom_xpos.release(), geom_xmat.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
@@ -496,19 +504,25 @@ void Renderer::finish() {
     if (*host_error) throw CudaFailure(-1, device_error_message(*host_error));
 }
 
-// Queues the tree build of every world: from matrices in device memory, or composed from body poses.
-void Renderer::build(const float *matrices_in, bool compose, const float *poses) {
+// Queues the tree build of every world: from matrices in device memory (compose 0), or composed from body
+// poses (1: poses) or geom poses (2: poses are the positions, xmat the rotations).
+void Renderer::build(const float *matrices_in, int compose, const float *poses, const float *xmat) {
     BuildArgs a{};
     a.worlds = worlds;
     a.per_world = per_world;
     a.n = n;
-    a.compose = compose ? 1 : 0;
+    a.compose = compose;
     a.matrices_in = matrices_in;
-    a.body_poses = poses;
+    a.body_poses = compose == 1 ? poses : nullptr;
     a.body_of_instance = body_of_instance.p;
     a.local_pose = local_pose.p;
     a.local_scale = local_scale.p;
     a.bodies_per_world = bodies_per_world;
+    a.geom_xpos = compose == 2 ? poses : nullptr;
+    a.geom_xmat = xmat;
+    a.geom_of_instance = geom_of_instance.p;
+    a.geom_scale = geom_scale.p;
+    a.geoms_per_world = geoms_per_world;
     // Composed matrices, and matrices given in the caller's device memory, are kept for inspection.
     a.matrices_out = (compose || matrices_in != matrices.p) ? matrices.p : nullptr;
     a.slot_bounds = slot_bounds.p;
@@ -553,9 +567,9 @@ void Renderer::set_instance_transforms(const float *m, int memory) {
                     " transform");
             }
         CK(cudaMemcpyAsync(matrices.p, m, static_cast<size_t>(n) * 12 * sizeof(float), cudaMemcpyHostToDevice, stream));
-        build(matrices.p, false, nullptr);
+        build(matrices.p, 0, nullptr);
     } else {
-        build(m, false, nullptr);
+        build(m, 0, nullptr);
     }
     finish();
 }
@@ -590,6 +604,7 @@ void Renderer::bind_bodies(int bpw, const int32_t *boi, const float *lp, const f
     }
     bodies_per_world = bpw;
     bound = true;
+    geoms_bound = false;
 }
 
 // src/batch.cpp:131-144 and src/cuda_backend.cu:493-507.
@@ -608,7 +623,60 @@ void Renderer::set_body_poses(const float *poses, int memory) {
         CK(cudaMemcpyAsync(body_poses.p, poses, bodies * 7 * sizeof(float), cudaMemcpyHostToDevice, stream));
         src = body_poses.p;
     }
-    build(nullptr, true, src);
+    build(nullptr, 1, src);
+    finish();
+}
+
+// The geom list and scales of MJWarpBatchRenderer (python/neraulgraphics/mujoco.py:199-243), checked as a
+// body binding is.
+void Renderer::bind_geoms(int gpw, const int32_t *goi, const float *sc) {
+    require(!uneven, "worlds of uneven sizes take instance matrices (set_instance_transforms), not geom poses");
+    const int P = per_world;
+    require(gpw >= 0, "geoms_per_world must be 0 or more");
+    require(P == 0 || (goi != nullptr && sc != nullptr),
+        "a geom binding needs one geom index and 3 scale floats for each of the " + std::to_string(P) +
+        " instances of a world");
+    for (int i = 0; i < P; ++i) {
+        const int g = goi[i];
+        require(g >= 0 && g < gpw, "instance " + std::to_string(i) + " is on geom " + std::to_string(g) +
+            ", but there are " + std::to_string(gpw) + " geoms per world");
+        require(all_finite(sc + 3 * i, 3), "instance " + std::to_string(i) + " has a scale with a NaN or infinite value");
+    }
+    require(static_cast<long long>(worlds) * gpw * 9 <= INT32_MAX, "too many geoms");
+    if (P > 0) {
+        geom_of_instance.ensure(P);
+        geom_scale.ensure(3 * static_cast<size_t>(P));
+        CK(cudaMemcpyAsync(geom_of_instance.p, goi, P * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(geom_scale.p, sc, 3 * P * sizeof(float), cudaMemcpyHostToDevice, stream));
+        geom_xpos.ensure(3 * static_cast<size_t>(worlds) * gpw);
+        geom_xmat.ensure(9 * static_cast<size_t>(worlds) * gpw);
+        CK(cudaEventRecord(ev_done, stream));
+        wait(ev_done, timeout);  // the host arrays are the caller's; the copies must be done
+    }
+    geoms_per_world = gpw;
+    geoms_bound = true;
+    bound = false;
+}
+
+// MJWarpBatchRenderer.update (python/neraulgraphics/mujoco.py:304-314): compose and build in one launch.
+void Renderer::set_geom_poses(const float *xpos, const float *xmat, int memory) {
+    require(geoms_bound, "set_geom_poses needs bind_geoms to be called first");
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    const size_t geoms = static_cast<size_t>(worlds) * geoms_per_world;
+    require(geoms == 0 || (xpos != nullptr && xmat != nullptr), "geom_xpos and geom_xmat must not be null");
+    if (memory == NGB_MEMORY_HOST)
+        for (size_t g = 0; g < geoms; ++g)
+            require(all_finite(xpos + 3 * g, 3) && all_finite(xmat + 9 * g, 9),
+                "geom " + std::to_string(g) + " has a NaN or infinite position or rotation");
+    if (per_world == 0) return;
+    const float *p = xpos, *r = xmat;
+    if (memory == NGB_MEMORY_HOST && geoms > 0) {
+        CK(cudaMemcpyAsync(geom_xpos.p, xpos, geoms * 3 * sizeof(float), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(geom_xmat.p, xmat, geoms * 9 * sizeof(float), cudaMemcpyHostToDevice, stream));
+        p = geom_xpos.p;
+        r = geom_xmat.p;
+    }
+    build(nullptr, 2, p, r);
     finish();
 }
 
@@ -864,6 +932,14 @@ int ngb_bind_bodies(ngb_renderer *h, int32_t bpw, const int32_t *boi, const floa
 
 int ngb_set_body_poses(ngb_renderer *h, const float *poses, int32_t memory) {
     return guarded(h, [&](ngb::Renderer &r) { r.set_body_poses(poses, memory); });
+}
+
+int ngb_bind_geoms(ngb_renderer *h, int32_t gpw, const int32_t *goi, const float *sc) {
+    return guarded(h, [&](ngb::Renderer &r) { r.bind_geoms(gpw, goi, sc); });
+}
+
+int ngb_set_geom_poses(ngb_renderer *h, const float *xpos, const float *xmat, int32_t memory) {
+    return guarded(h, [&](ngb::Renderer &r) { r.set_geom_poses(xpos, xmat, memory); });
 }
 
 int ngb_render(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint32_t outputs, int32_t frame,

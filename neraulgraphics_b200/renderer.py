@@ -30,6 +30,14 @@ def _is_cuda_tensor(a) -> bool:
     return type(a).__module__.startswith("torch") and getattr(a, "is_cuda", False)
 
 
+def _cuda_view(a):
+    """A CUDA tensor over a's memory when a is a CUDA array of another library (a Warp, CuPy or Numba array:
+    anything with __cuda_array_interface__), so that a simulator's arrays are read in place; else a itself."""
+    if not _is_cuda_tensor(a) and hasattr(a, "__cuda_array_interface__"):
+        return _torch().as_tensor(a)
+    return a
+
+
 def _count(a) -> int:
     return int(np.prod(a.shape)) if len(a.shape) else 1
 
@@ -91,7 +99,8 @@ class BatchRenderer:
         check(self._lib.ngb_set_stream(self._h, C.c_void_p(s if s else 1)), self._h)
 
     def _input(self, a, what):
-        """(pointer, memory, keep-alive) for a float32 input: a CUDA tensor in place, else a host copy."""
+        """(pointer, memory, keep-alive) for a float32 input: a CUDA array in place, else a host copy."""
+        a = _cuda_view(a)
         if _is_cuda_tensor(a):
             torch = _torch()
             if a.device.index != self._device:
@@ -129,16 +138,51 @@ class BatchRenderer:
                                         lp.ctypes.data_as(C.POINTER(C.c_float)),
                                         sc.ctypes.data_as(C.POINTER(C.c_float))), self._h)
         self._bodies_per_world = int(bodies_per_world)
+        self._geoms_per_world = None
 
     def set_body_poses(self, body_poses):
         """Place every instance from body poses: (world_count, bodies_per_world, 7) floats, x y z qx qy qz qw."""
         p, mem, keep = self._input(body_poses, "body poses")
         bpw = getattr(self, "_bodies_per_world", None)
+        body_poses = _cuda_view(body_poses)
         if bpw is not None:
             _require_count(body_poses, self.world_count * bpw * 7, "body poses", "(world_count, bodies_per_world, 7)")
         self._stream()
         check(self._lib.ngb_set_body_poses(self._h, p, mem), self._h)
         self._keep = keep
+
+    def bind_geoms(self, geom_of_instance, scale, geoms_per_world):
+        """How a MuJoCo model's geoms carry the instances: per instance its geom index and scale (x, y, z), as
+        MJWarpBatchRenderer keeps them (python/neraulgraphics/mujoco.py:199-243). Replaces a body binding."""
+        g = np.ascontiguousarray(geom_of_instance, np.int32)
+        sc = np.ascontiguousarray(scale, np.float32)
+        n = self.instances_per_world
+        if g.size != n or sc.size != 3 * n:
+            raise ValueError(f"a geom binding needs one geom index and 3 scale floats for each of the {n} instances "
+                             f"of a world")
+        self._stream()
+        check(self._lib.ngb_bind_geoms(self._h, int(geoms_per_world), g.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       sc.ctypes.data_as(C.POINTER(C.c_float))), self._h)
+        self._geoms_per_world = int(geoms_per_world)
+        self._bodies_per_world = None
+
+    def set_geom_poses(self, geom_xpos, geom_xmat):
+        """Place every instance from its geom's pose, as a MuJoCo Warp data holds them: geom_xpos
+        (world_count, geoms_per_world, 3) and geom_xmat (world_count, geoms_per_world, 3, 3) floats, read in
+        place when they are CUDA arrays. Composes [R * diag(scale) | p] and rebuilds the trees in one launch
+        (MJWarpBatchRenderer.update, python/neraulgraphics/mujoco.py:304-314)."""
+        gpw = getattr(self, "_geoms_per_world", None)
+        if gpw is None:
+            raise ValueError("set_geom_poses needs bind_geoms to be called first")
+        _require_count(geom_xpos, self.world_count * gpw * 3, "geom_xpos", "(world_count, geoms_per_world, 3)")
+        _require_count(geom_xmat, self.world_count * gpw * 9, "geom_xmat", "(world_count, geoms_per_world, 3, 3)")
+        p, mem_p, keep_p = self._input(geom_xpos, "geom_xpos")
+        r, mem_r, keep_r = self._input(geom_xmat, "geom_xmat")
+        if mem_p != mem_r:
+            raise ValueError("geom_xpos and geom_xmat must both be CUDA arrays or both host arrays")
+        self._stream()
+        check(self._lib.ngb_set_geom_poses(self._h, p, r, mem_p), self._h)
+        self._keep = (keep_p, keep_r)
 
     # ------------------------------------------------------------------------------------------ rendering --
 

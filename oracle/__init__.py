@@ -198,6 +198,20 @@ def compose(worlds, per_world, bodies_per_world, body_of_instance, local_pose, s
     return out
 
 
+def geom_matrices(geom_xpos, geom_xmat, geom_of_instance, scale):
+    """Instance matrices from MuJoCo geom poses, [R * diag(scale) | p] per instance in float32: the products
+    of MJWarpBatchRenderer's compose kernel (python/neraulgraphics/mujoco.py:291-302), one rounding each.
+    geom_xpos (worlds, geoms, 3), geom_xmat (worlds, geoms, 3, 3) -> (worlds, instances, 3, 4)."""
+    g = np.asarray(geom_of_instance, np.int64)
+    xpos = np.asarray(geom_xpos, np.float32)
+    xmat = np.asarray(geom_xmat, np.float32).reshape(xpos.shape[0], xpos.shape[1], 3, 3)
+    s = np.asarray(scale, np.float32).reshape(-1, 3)
+    out = np.empty((xpos.shape[0], len(g), 3, 4), np.float32)
+    out[..., :3] = xmat[:, g] * s[None, :, None, :]
+    out[..., 3] = xpos[:, g]
+    return out
+
+
 # ---------------------------------------------------------------------------- the reference itself --
 
 _ref_libs: dict = {}

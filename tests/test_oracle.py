@@ -258,3 +258,19 @@ def test_pose_matrices_agree_between_torch_and_numpy():
     q = torch.from_numpy(i["quaternions"][0, :2]).double().requires_grad_()
     p = torch.from_numpy(i["positions"][0, :2]).double()
     assert torch.autograd.gradcheck(lambda qq: pose_matrices(p, qq), (q,))
+
+
+def test_geom_matrices_are_the_compose_kernels_products():
+    """O.geom_matrices against a plain loop of the compose kernel's float32 products (mujoco.py:291-302)."""
+    rng = np.random.default_rng(0)
+    xpos = rng.normal(size=(3, 5, 3)).astype(np.float32)
+    xmat = rng.normal(size=(3, 5, 3, 3)).astype(np.float32)
+    goi = np.int32([4, 0, 2])
+    scale = rng.uniform(0.1, 2.0, size=(3, 3)).astype(np.float32)
+    got = O.geom_matrices(xpos, xmat, goi, scale)
+    for w in range(3):
+        for i, g in enumerate(goi):
+            for row in range(3):
+                for c in range(3):
+                    assert got[w, i, row, c] == np.float32(xmat[w, g, row, c] * scale[i, c])
+                assert got[w, i, row, 3] == xpos[w, g, row]
