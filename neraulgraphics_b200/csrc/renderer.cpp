@@ -149,7 +149,7 @@ struct Renderer {
     DevBuf<int32_t> hit_instance, hit_triangle;
     DevBuf<float> hit_u, hit_v;
     DevBuf<int> error_flag;
-    int *host_error = nullptr;  // pinned: the device error flag, copied back after every launch
+    int *host_error = nullptr;  // pinned: the device error flag, copied back where the host waits for the work
 
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_done = nullptr;
@@ -172,6 +172,7 @@ struct Renderer {
     ~Renderer();
 
     void build(const float *matrices_in, int compose, const float *poses, const float *xmat = nullptr);
+    void queue_error_read();
     void finish();
     void read_timing();
     // Whether the stream is being captured into a CUDA graph.
@@ -494,11 +495,18 @@ void Renderer::read_timing() {
     timing_pending = false;
 }
 
-void Renderer::finish() {
+// Queues the copy of the device error flag to host_error, for a wait that follows.
+void Renderer::queue_error_read() {
     CK(cudaMemcpyAsync(host_error, error_flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    if (capturing()) return;  // a graph's replays report through ngb_synchronize
+}
+
+void Renderer::finish() {
+    // Stream-ordered calls and graph captures queue no copy of the flag: a device-to-host copy in the stream
+    // waits behind every such copy the caller has on the copy engine (the last step's images going out while
+    // this step renders) and holds back the launches queued after it. ngb_synchronize reads the flag.
+    if (capturing() || !synchronous) return;
+    queue_error_read();
     CK(cudaEventRecord(ev_done, stream));
-    if (!synchronous) return;
     wait(ev_done, timeout);
     read_timing();
     if (*host_error) throw CudaFailure(-1, device_error_message(*host_error));
@@ -983,6 +991,7 @@ int ngb_render_host(ngb_renderer *h, const float *cams, float fov, int32_t spp, 
         if (ddepth && depth) CK(cudaMemcpyAsync(depth, ddepth, px * sizeof(float), cudaMemcpyDeviceToHost, r.stream));
         if (dnormal && normal) CK(cudaMemcpyAsync(normal, dnormal, 3 * px * sizeof(float), cudaMemcpyDeviceToHost, r.stream));
         if (dids && object_id) CK(cudaMemcpyAsync(object_id, dids, px * sizeof(int32_t), cudaMemcpyDeviceToHost, r.stream));
+        r.queue_error_read();
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, r.timeout);
         if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
@@ -1056,6 +1065,7 @@ int ngb_set_sync(ngb_renderer *h, int32_t synchronous, double timeout_seconds) {
 
 int ngb_synchronize(ngb_renderer *h, double timeout_seconds) {
     return guarded(h, [&](ngb::Renderer &r) {
+        r.queue_error_read();
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, timeout_seconds > 0.0 ? timeout_seconds : r.timeout);
         r.read_timing();
