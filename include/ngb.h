@@ -234,6 +234,23 @@ int ngb_bind_geoms(ngb_renderer *r, int32_t geoms_per_world, const int32_t *geom
  * (python/neraulgraphics/mujoco.py:287-314), without that kernel or the matrices' round trip through memory. */
 int ngb_set_geom_poses(ngb_renderer *r, const float *geom_xpos, const float *geom_xmat, int32_t memory);
 
+/* ---- meshes whose vertices move ----------------------------------------------------------------------- */
+
+/* New vertex positions for mesh `mesh` (the vertex count and triangles it was made with): vertex_count x 3
+ * floats in memory, and optionally new vertex normals (NULL keeps the ones it has; a mesh made without normals
+ * takes none). The mesh's tree is rebuilt on the device -- the binned SAH build ngb_create runs on the host
+ * (src/bvh.cpp:46-174, src/mesh_build.cpp:91-157), node for node -- its triangles re-packed, and every world's
+ * instance tree rebuilt from the current transforms. Host arrays are checked as ngb_create checks meshes.
+ * No counterpart in the reference, where a mesh changes only by making a new renderer. Waits for the rebuild
+ * (it reads each tree level's size back). */
+int ngb_update_mesh(ngb_renderer *r, int32_t mesh, const float *vertices, const float *normals, int32_t memory);
+
+/* Mesh `mesh`'s tree as the renderer holds it, in ngb_build_meshes's format for that one mesh (mesh-local
+ * node and triangle references): call with NULL arrays for the counts, then with node_count x 8 words,
+ * triangle_count x 12 floats, 6 bounds and triangle_count original triangle indices (any may be NULL). */
+int ngb_inspect_mesh(ngb_renderer *r, int32_t mesh, int32_t *node_count, int32_t *triangle_count, int32_t *nodes,
+    float *triangles, float *bounds, int32_t *triangle_index);
+
 /* ---- rendering ------------------------------------------------------------------------------------- */
 
 /* Renders every view into the renderer's own device buffers, described in *out. view_count cameras of

@@ -1,0 +1,490 @@
+// A mesh's bottom-level tree rebuilt on the device from new vertex positions: the binned surface-area-
+// heuristic build of src/bvh.cpp:46-174 (16 bins, leaves of at most 4 triangles, depth at most 60) and the
+// packing of src/mesh_build.cpp:91-157, giving the host build's tree node for node, its triangles in the
+// same leaf order and the same bits.
+//
+// The host builds depth first from a stack; here the nodes of one depth are split together, one CTA per
+// node, level after level, and the host's node numbering is restored at the end:
+//   - a node's box, centroid box and bin boxes are min/max reductions. The host's sequential std::min keeps
+//     the first of equal values, which matters only for -0 and +0; every reduction here carries the range
+//     position of its value and keeps the smallest position among equal values, so the bits are the host's;
+//   - std::partition (libstdc++'s bidirectional form) swaps the k-th element from the left that fails the
+//     test with the k-th element from the right that passes it, until the two meet: the same swaps are made
+//     here from two prefix counts, in parallel;
+//   - the host gives a node's two children the indices 2k + 1 and 2k + 2 when it splits the k-th internal
+//     node in depth-first, left-first order; that order's rank follows from the subtrees' internal-node
+//     counts (bottom-up) and is handed down from the root (top-down).
+// Node and tree sizes: a tree over T triangles has at most 2T - 1 nodes, so the nodes are numbered in
+// scratch arrays of 2T - 1, level after level (the host reads each level's node count back).
+#include <climits>
+#include <cstdint>
+
+#include "kernels.h"
+
+namespace ngb {
+namespace {
+
+constexpr int THREADS = 256;
+constexpr int WARPS = THREADS / 32;
+constexpr int BINS = 16;
+constexpr int MAX_LEAF = 4;
+constexpr int MAX_DEPTH = 60;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr unsigned long long NONE_MIN = ~0ull, NONE_MAX = 0ull;
+
+// Ordering key of a float for min/max with -0 and +0 as one value (the position decides between them).
+__device__ __forceinline__ unsigned long long order_key(float v, unsigned pos, bool is_max) {
+    const float w = v == 0.0f ? 0.0f : v;
+    const unsigned u = __float_as_uint(w);
+    const unsigned k = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return (static_cast<unsigned long long>(k) << 32) | (is_max ? 0xffffffffu - pos : pos);
+}
+
+__device__ __forceinline__ unsigned key_pos(unsigned long long key, bool is_max) {
+    const unsigned low = static_cast<unsigned>(key);
+    return is_max ? 0xffffffffu - low : low;
+}
+
+__device__ __forceinline__ unsigned long long shfl_u64(unsigned long long v, int mask) {
+    const unsigned lo = __shfl_xor_sync(FULL, static_cast<unsigned>(v), mask);
+    const unsigned hi = __shfl_xor_sync(FULL, static_cast<unsigned>(v >> 32), mask);
+    return (static_cast<unsigned long long>(hi) << 32) | lo;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+    for (int m = 16; m > 0; m >>= 1) {
+        const unsigned long long o = shfl_u64(v, m);
+        v = o < v ? o : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+    for (int m = 16; m > 0; m >>= 1) {
+        const unsigned long long o = shfl_u64(v, m);
+        v = o > v ? o : v;
+    }
+    return v;
+}
+
+// The host's box arithmetic (bvh::grow with std::min / std::max, bvh::surface_area).
+struct Box {
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ Box empty_box() {
+    const float inf = __int_as_float(0x7f800000);
+    return Box{{inf, inf, inf}, {-inf, -inf, -inf}};
+}
+
+__device__ __forceinline__ void grow(Box &b, const Box &o) {
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] = o.lo[k] < b.lo[k] ? o.lo[k] : b.lo[k];
+        b.hi[k] = b.hi[k] < o.hi[k] ? o.hi[k] : b.hi[k];
+    }
+}
+
+__device__ __forceinline__ float area(const Box &b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    if (dx < 0.0f || dy < 0.0f || dz < 0.0f) return 0.0f;
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+__device__ __forceinline__ int bin_of(float c, float lo, float scale) {
+    const int b = static_cast<int>((c - lo) * scale);
+    return b < BINS - 1 ? b : BINS - 1;
+}
+
+// Triangle boxes (the vertices' std::fmin / std::fmax in vertex order, src/mesh_build.cpp, as the host build
+// computes them: of two equal values, -0 and +0, the later one) and centroids (0.5 (lo + hi),
+// src/bvh.cpp:55-56); the order starts as the identity and the root spans every triangle.
+__global__ void prepare_kernel(const MeshBuildArgs a, const MeshBuildScratch t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        t.begin[0] = 0;
+        t.end[0] = a.triangles;
+        t.rank[0] = 0;
+        t.index[0] = 0;
+        t.counter[0] = 1;
+    }
+    if (i >= a.triangles) return;
+    Box b = empty_box();
+    for (int k = 0; k < 3; ++k) {
+        const float *v = a.vertices + 3 * static_cast<size_t>(__ldg(a.indices + 3 * static_cast<size_t>(i) + k));
+        for (int c = 0; c < 3; ++c) {
+            const float x = __ldg(v + c);
+            b.lo[c] = b.lo[c] < x ? b.lo[c] : x;
+            b.hi[c] = b.hi[c] > x ? b.hi[c] : x;
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        t.box[6 * static_cast<size_t>(i) + c] = b.lo[c];
+        t.box[6 * static_cast<size_t>(i) + 3 + c] = b.hi[c];
+        t.centre[3 * static_cast<size_t>(i) + c] = 0.5f * (b.lo[c] + b.hi[c]);
+    }
+    t.order[i] = static_cast<uint32_t>(i);
+}
+
+struct SplitSmem {
+    unsigned long long box_key[12];              // node box lo/hi (6), centroid box lo/hi (6)
+    unsigned long long bin_key[3][BINS][6];      // per axis and bin: its box lo/hi
+    int bin_count[3][BINS];
+    int warp_sum[WARPS];
+    int total;
+    float cbox[6];
+    int best_axis, best_bin, leaf, mid;
+};
+
+// Exclusive prefix count of flag over the CTA (thread order), and the CTA's total.
+__device__ __forceinline__ int cta_scan(SplitSmem &sm, bool flag, int &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(FULL, flag);
+    if (lane == 0) sm.warp_sum[warp] = __popc(m);
+    __syncthreads();
+    int before = 0;
+    total = 0;
+    for (int w = 0; w < WARPS; ++w) {
+        before += w < warp ? sm.warp_sum[w] : 0;
+        total += sm.warp_sum[w];
+    }
+    __syncthreads();
+    return before + __popc(m & ((1u << lane) - 1u));
+}
+
+// Splits every node of one depth: [first, last) in level order, one CTA per node.
+__global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int first,
+    int last, int depth) {
+    __shared__ SplitSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int x = first + blockIdx.x; x < last; x += gridDim.x) {
+        const int begin = t.begin[x], end = t.end[x], count = end - begin;
+        for (int k = tid; k < 12; k += THREADS) sm.box_key[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
+        for (int k = tid; k < 3 * BINS * 6; k += THREADS)
+            (&sm.bin_key[0][0][0])[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
+        for (int k = tid; k < 3 * BINS; k += THREADS) (&sm.bin_count[0][0])[k] = 0;
+        __syncthreads();
+
+        // The node's box and centroid box: per thread the first of its smallest / largest values, then the
+        // warp's and the CTA's by (value, position).
+        {
+            float best[12];
+            unsigned pos[12];
+            for (int k = 0; k < 12; ++k) {
+                best[k] = (k % 6) < 3 ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
+                pos[k] = 0xffffffffu;
+            }
+            for (int i = begin + tid; i < end; i += THREADS) {
+                const uint32_t p = t.order[i];
+                float v[12];
+                for (int c = 0; c < 6; ++c) v[c] = t.box[6 * static_cast<size_t>(p) + c];
+                for (int c = 0; c < 3; ++c) v[6 + c] = v[9 + c] = t.centre[3 * static_cast<size_t>(p) + c];
+                for (int k = 0; k < 12; ++k) {
+                    const bool take = (k % 6) < 3 ? v[k] < best[k] : best[k] < v[k];
+                    if (take || pos[k] == 0xffffffffu) {
+                        best[k] = v[k];
+                        pos[k] = static_cast<unsigned>(i);
+                    }
+                }
+            }
+            for (int k = 0; k < 12; ++k) {
+                const bool is_max = (k % 6) >= 3;
+                unsigned long long key = pos[k] == 0xffffffffu ? (is_max ? NONE_MAX : NONE_MIN)
+                                                                : order_key(best[k], pos[k], is_max);
+                key = is_max ? warp_max_u64(key) : warp_min_u64(key);
+                if (lane == 0) {
+                    if (is_max) atomicMax(&sm.box_key[k], key);
+                    else atomicMin(&sm.box_key[k], key);
+                }
+            }
+        }
+        __syncthreads();
+        Box box;
+        float cb[6];
+        for (int k = 0; k < 12; ++k) {
+            const bool is_max = (k % 6) >= 3;
+            const uint32_t p = t.order[key_pos(sm.box_key[k], is_max)];
+            const float v = k < 6 ? t.box[6 * static_cast<size_t>(p) + k] : t.centre[3 * static_cast<size_t>(p) + (k - 6) % 3];
+            if (k < 3) box.lo[k] = v;
+            else if (k < 6) box.hi[k - 3] = v;
+            else cb[k - 6] = v;
+        }
+
+        // Bins on every axis whose centroids spread (src/bvh.cpp:94-107).
+        if (count > 1) {
+            for (int i = begin + tid; i < end; i += THREADS) {
+                const uint32_t p = t.order[i];
+                for (int axis = 0; axis < 3; ++axis) {
+                    const float extent = cb[3 + axis] - cb[axis];
+                    if (!(extent > 0.0f)) continue;
+                    const float scale = static_cast<float>(BINS) / extent;
+                    const int b = bin_of(t.centre[3 * static_cast<size_t>(p) + axis], cb[axis], scale);
+                    atomicAdd(&sm.bin_count[axis][b], 1);
+                    for (int c = 0; c < 6; ++c) {
+                        const bool is_max = c >= 3;
+                        const unsigned long long key = order_key(t.box[6 * static_cast<size_t>(p) + c],
+                            static_cast<unsigned>(i), is_max);
+                        if (is_max) atomicMax(&sm.bin_key[axis][b][c], key);
+                        else atomicMin(&sm.bin_key[axis][b][c], key);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // The split: the cheapest plane over the axes in order, then the leaf test (src/bvh.cpp:108-146).
+        if (tid == 0) {
+            int best_axis = -1, best_bin = 0;
+            float best_cost = __int_as_float(0x7f800000);
+            if (count > 1) {
+                for (int axis = 0; axis < 3; ++axis) {
+                    const float extent = cb[3 + axis] - cb[axis];
+                    if (!(extent > 0.0f)) continue;
+                    Box bins[BINS];
+                    for (int b = 0; b < BINS; ++b) {
+                        bins[b] = empty_box();
+                        if (sm.bin_count[axis][b] == 0) continue;
+                        for (int c = 0; c < 6; ++c) {
+                            const bool is_max = c >= 3;
+                            const uint32_t p = t.order[key_pos(sm.bin_key[axis][b][c], is_max)];
+                            const float v = t.box[6 * static_cast<size_t>(p) + c];
+                            if (c < 3) bins[b].lo[c] = v;
+                            else bins[b].hi[c - 3] = v;
+                        }
+                    }
+                    float right_area[BINS - 1];
+                    int right_count[BINS - 1];
+                    Box acc = empty_box();
+                    int running = 0;
+                    for (int i = BINS - 1; i >= 1; --i) {
+                        grow(acc, bins[i]);
+                        running += sm.bin_count[axis][i];
+                        right_area[i - 1] = area(acc);
+                        right_count[i - 1] = running;
+                    }
+                    acc = empty_box();
+                    running = 0;
+                    for (int i = 0; i < BINS - 1; ++i) {
+                        grow(acc, bins[i]);
+                        running += sm.bin_count[axis][i];
+                        if (running == 0 || right_count[i] == 0) continue;
+                        const float cost = static_cast<float>(running) * area(acc) +
+                            static_cast<float>(right_count[i]) * right_area[i];
+                        if (cost < best_cost) {
+                            best_cost = cost;
+                            best_axis = axis;
+                            best_bin = i;
+                        }
+                    }
+                }
+            }
+            const float leaf_cost = static_cast<float>(count) * area(box);
+            const float split_cost = 1.0f * area(box) + best_cost;
+            const bool small = count <= MAX_LEAF;
+            sm.leaf = (count == 1 || depth >= MAX_DEPTH || (small && (best_axis < 0 || leaf_cost <= split_cost))) ? 1 : 0;
+            sm.best_axis = best_axis;
+            sm.best_bin = best_bin;
+            for (int c = 0; c < 6; ++c) sm.cbox[c] = cb[c];
+        }
+        __syncthreads();
+        const int leaf = sm.leaf, best_axis = sm.best_axis, best_bin = sm.best_bin;
+        if (tid < 6) t.node_box[6 * static_cast<size_t>(x) + tid] = tid < 3 ? box.lo[tid] : box.hi[tid - 3];
+        if (leaf) {
+            if (tid == 0) t.left[x] = -1;
+            __syncthreads();
+            continue;
+        }
+
+        // std::partition over the range by (bin <= best_bin): the k-th failing element from the left swaps
+        // with the k-th passing element from the right, for every k before the two runs meet.
+        int mid = begin + count / 2;
+        if (best_axis >= 0) {
+            const float lo = sm.cbox[best_axis];
+            const float scale = static_cast<float>(BINS) / (sm.cbox[3 + best_axis] - lo);
+            auto passes = [&](int i) {
+                return bin_of(t.centre[3 * static_cast<size_t>(t.order[i]) + best_axis], lo, scale) <= best_bin;
+            };
+            int passing = 0;
+            for (int base = begin; base < end; base += THREADS) {
+                int total;
+                const int i = base + tid;
+                cta_scan(sm, i < end && passes(i), total);
+                passing += total;
+            }
+            const int meet = begin + passing;
+            int swaps = 0;
+            for (int base = begin; base < meet; base += THREADS) {
+                int total;
+                const int i = base + tid;
+                const bool fail = i < meet && !passes(i);
+                const int k = cta_scan(sm, fail, total);
+                if (fail) t.lpos[begin + swaps + k] = i;
+                swaps += total;
+            }
+            int found = 0;
+            for (int base = 0; meet + base < end; base += THREADS) {
+                int total;
+                const int j = end - 1 - (base + tid);
+                const bool pass = j >= meet && passes(j);
+                const int k = cta_scan(sm, pass, total);
+                if (pass) t.rpos[begin + found + k] = j;
+                found += total;
+            }
+            __syncthreads();
+            for (int k = tid; k < swaps; k += THREADS) {
+                const int l = t.lpos[begin + k], r = t.rpos[begin + k];
+                const uint32_t pl = t.order[l];
+                t.order[l] = t.order[r];
+                t.order[r] = pl;
+            }
+            mid = meet;
+            if (mid == begin || mid == end) mid = begin + count / 2;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int c = atomicAdd(t.counter, 2);
+            t.left[x] = c;
+            t.begin[c] = begin;
+            t.end[c] = mid;
+            t.begin[c + 1] = mid;
+            t.end[c + 1] = end;
+        }
+        __syncthreads();
+    }
+}
+
+// Internal nodes per subtree, one depth at a time from the deepest (its children's counts are final).
+__global__ void sizes_kernel(const MeshBuildScratch t, int first, int last) {
+    const int x = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= last) return;
+    const int l = t.left[x];
+    t.size[x] = l < 0 ? 0 : 1 + t.size[l] + t.size[l + 1];
+}
+
+// Depth-first, left-first ranks among the internal nodes and the host's node indices, one depth at a time
+// from the root: the k-th internal node's children are nodes 2k + 1 and 2k + 2.
+__global__ void ranks_kernel(const MeshBuildScratch t, int first, int last) {
+    const int x = first + blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= last) return;
+    const int l = t.left[x];
+    if (l < 0) return;
+    const int r = t.rank[x];
+    t.rank[l] = r + 1;
+    t.rank[l + 1] = r + 1 + t.size[l];
+    t.index[l] = 2 * r + 1;
+    t.index[l + 1] = 2 * r + 2;
+}
+
+// The packed tree (src/mesh_build.cpp:91-157): bvh::Node records with global indices, and the child-pair
+// records of the internal nodes.
+__global__ void nodes_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int nodes) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nodes) return;
+    const int i = t.index[x];
+    const float *b = t.node_box + 6 * static_cast<size_t>(x);
+    const int l = t.left[x];
+    float4 *node = a.blas + 2 * (static_cast<size_t>(a.node_base) + i);
+    float4 *pair = a.pairs + 4 * (static_cast<size_t>(a.node_base) + i);
+    if (l < 0) {
+        node[0] = make_float4(b[0], b[1], b[2], __int_as_float(a.tri_base + t.begin[x]));
+        node[1] = make_float4(b[3], b[4], b[5], __int_as_float(t.end[x] - t.begin[x]));
+        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        pair[0] = pair[1] = pair[2] = pair[3] = z;
+        return;
+    }
+    node[0] = make_float4(b[0], b[1], b[2], __int_as_float(a.node_base + t.index[l]));
+    node[1] = make_float4(b[3], b[4], b[5], __int_as_float(0));
+    const float *lb = t.node_box + 6 * static_cast<size_t>(l), *rb = t.node_box + 6 * static_cast<size_t>(l + 1);
+    int ref[4];
+    for (int c = 0; c < 2; ++c) {
+        const int y = l + c;
+        const bool y_leaf = t.left[y] < 0;
+        ref[2 * c] = y_leaf ? a.tri_base + t.begin[y] : a.node_base + t.index[y];
+        ref[2 * c + 1] = y_leaf ? t.end[y] - t.begin[y] : 0;
+    }
+    pair[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
+    pair[1] = make_float4(lb[4], lb[5], rb[0], rb[1]);
+    pair[2] = make_float4(rb[2], rb[3], rb[4], rb[5]);
+    pair[3] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+}
+
+// Triangles in leaf order (v0, e1 = v1 - v0, e2 = v2 - v0), their mesh indices both ways, and their vertex
+// normals (ATTR_NORMALS, src/mesh_build.h:28) where the scene keeps them.
+__global__ void triangles_kernel(const MeshBuildArgs a, const MeshBuildScratch t) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.triangles) return;
+    const uint32_t tri = t.order[p];
+    const size_t packed = static_cast<size_t>(a.tri_base) + p;
+    float3 v[3];
+    for (int k = 0; k < 3; ++k) {
+        const float *q = a.vertices + 3 * static_cast<size_t>(__ldg(a.indices + 3 * static_cast<size_t>(tri) + k));
+        v[k] = make_float3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+    }
+    a.tris[3 * packed] = make_float4(v[0].x, v[0].y, v[0].z, 0.0f);
+    a.tris[3 * packed + 1] = make_float4(v[1].x - v[0].x, v[1].y - v[0].y, v[1].z - v[0].z, 0.0f);
+    a.tris[3 * packed + 2] = make_float4(v[2].x - v[0].x, v[2].y - v[0].y, v[2].z - v[0].z, 0.0f);
+    a.tri_index[packed] = static_cast<int>(tri);
+    a.tri_of_local[static_cast<size_t>(a.tri_base) + tri] = static_cast<int>(packed);
+    if (!a.attrs) return;
+    float rec[16] = {};
+    if (a.normals)
+        for (int k = 0; k < 3; ++k) {
+            const float *q = a.normals + 3 * static_cast<size_t>(__ldg(a.indices + 3 * static_cast<size_t>(tri) + k));
+            rec[4 * k] = __ldg(q);
+            rec[4 * k + 1] = __ldg(q + 1);
+            rec[4 * k + 2] = __ldg(q + 2);
+        }
+    rec[15] = __int_as_float(a.normals ? 1 : 0);
+    for (int k = 0; k < 4; ++k) a.attrs[4 * packed + k] = make_float4(rec[4 * k], rec[4 * k + 1], rec[4 * k + 2], rec[4 * k + 3]);
+}
+
+// The slots of this mesh: their root reference, their box in mesh space, and no convexity claim (the new
+// shape is not checked).
+__global__ void slots_kernel(const MeshBuildArgs a, const MeshBuildScratch t, const int *slot_mesh, int slots,
+    int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots || slot_mesh[s] != mesh) return;
+    const bool leaf = t.left[0] < 0;
+    slot_root[s] = leaf ? make_int2(a.tri_base, a.triangles) : make_int2(a.node_base, 0);
+    for (int c = 0; c < 6; ++c) slot_bounds[6 * static_cast<size_t>(s) + c] = t.node_box[c];
+    slot_hull[s].w = -1.0f;
+}
+
+int blocks_for(long long n) { return static_cast<int>((n + 255) / 256); }
+
+}  // namespace
+
+cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &t, cudaStream_t s) {
+    prepare_kernel<<<blocks_for(a.triangles), 256, 0, s>>>(a, t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_split(const MeshBuildArgs &a, const MeshBuildScratch &t, int first, int last, int depth,
+    cudaStream_t s) {
+    const int tasks = last - first;
+    if (tasks <= 0) return cudaSuccess;
+    split_kernel<<<tasks < 4096 ? tasks : 4096, THREADS, 0, s>>>(a, t, first, last, depth);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_sizes(const MeshBuildScratch &t, int first, int last, cudaStream_t s) {
+    if (last <= first) return cudaSuccess;
+    sizes_kernel<<<blocks_for(last - first), 256, 0, s>>>(t, first, last);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_ranks(const MeshBuildScratch &t, int first, int last, cudaStream_t s) {
+    if (last <= first) return cudaSuccess;
+    ranks_kernel<<<blocks_for(last - first), 256, 0, s>>>(t, first, last);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_write(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, const int *slot_mesh,
+    int slots, int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t s) {
+    nodes_kernel<<<blocks_for(nodes), 256, 0, s>>>(a, t, nodes);
+    triangles_kernel<<<blocks_for(a.triangles), 256, 0, s>>>(a, t);
+    if (slots > 0)
+        slots_kernel<<<blocks_for(slots), 256, 0, s>>>(a, t, slot_mesh, slots, mesh, slot_root, slot_bounds, slot_hull);
+    return cudaGetLastError();
+}
+
+}  // namespace ngb

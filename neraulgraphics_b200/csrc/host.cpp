@@ -318,7 +318,7 @@ std::vector<Node> sah_build(const std::vector<Box> &bounds, std::vector<uint32_t
 
 }  // namespace
 
-BuiltMeshes build_meshes(const ngb_scene &s) {
+BuiltMeshes build_meshes(const ngb_scene &s, bool node_capacity) {
     BuiltMeshes out;
     bool any_normals = false;
     for (int m = 0; m < s.mesh_count; ++m) any_normals = any_normals || s.meshes[m].normals != nullptr;
@@ -369,6 +369,12 @@ BuiltMeshes build_meshes(const ngb_scene &s) {
         }
         const std::array<int32_t, 2> root = ref_of(tree[0], 0);
         out.root_refs.insert(out.root_refs.end(), root.begin(), root.end());
+        out.node_counts.push_back(static_cast<int32_t>(tree.size()));
+        if (node_capacity) {
+            const size_t cap = 2 * tri_count - 1;
+            out.nodes.resize(out.nodes.size() + 8 * (cap - tree.size()), 0.0f);
+            out.pairs.resize(out.pairs.size() + 16 * (cap - tree.size()), 0.0f);
+        }
         for (const uint32_t t : order) {
             const float *a = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t]);
             const float *b = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t + 1]);

@@ -57,9 +57,13 @@ struct BuiltMeshes {
     // triangle, count) for a leaf. Per mesh, its root's reference.
     std::vector<float> pairs;        // 16 per node
     std::vector<int32_t> root_refs;  // 2 per mesh
+    std::vector<int32_t> node_counts;  // per mesh: its tree's nodes
 };
 
-BuiltMeshes build_meshes(const ngb_scene &s);
+// node_capacity: with it, mesh m's nodes start at the sum of the capacities 2 T_k - 1 of the meshes before it
+// (T_k triangles) and its unused capacity is zero nodes, so a tree rebuilt on the device for new vertex
+// positions (which may have another node count, never above 2 T - 1) fits where the first one was.
+BuiltMeshes build_meshes(const ngb_scene &s, bool node_capacity = false);
 
 // A mesh's hull facts for the shadow rays: the vertices' mean (x, y, z) and, in w, their largest distance from
 // it when the mesh is convex (every vertex on the mean's side of every triangle's plane, within 1e-6 of that

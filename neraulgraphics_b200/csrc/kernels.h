@@ -162,4 +162,40 @@ struct AdjointArgs {
 };
 cudaError_t launch_depth_normal_adjoint(const SceneParams &s, const AdjointArgs &a, cudaStream_t stream);
 
+// A mesh's tree rebuilt on the device from new vertex positions, node for node the host's (see blas_build.cu).
+struct MeshBuildArgs {
+    const float *vertices;      // vertex_count x 3
+    const float *normals;       // vertex_count x 3, or null
+    const uint32_t *indices;    // triangles x 3
+    int triangles;
+    int node_base, tri_base;    // the mesh's first node and first packed triangle
+    float4 *blas;               // bvh::Node records, 2 float4 per node
+    float4 *pairs;              // child-pair records, 4 float4 per node
+    float4 *tris;               // 3 float4 per packed triangle
+    float4 *attrs;              // 4 float4 per packed triangle, or null (the scene keeps no normals)
+    int *tri_index;             // per packed triangle: its index in the mesh
+    int *tri_of_local;          // at tri_base + mesh triangle: its packed index
+};
+struct MeshBuildScratch {
+    float *box;                 // triangles x 6
+    float *centre;              // triangles x 3
+    uint32_t *order;            // triangles: the leaf order under construction
+    int *lpos, *rpos;           // triangles each: a partition's swap positions
+    // The tree's nodes in level order (at most 2 triangles - 1).
+    float *node_box;            // 6 per node
+    int *begin, *end;           // per node: its range of the order
+    int *left;                  // per node: its first child (the second follows), or -1 for a leaf
+    int *size;                  // per node: internal nodes in its subtree
+    int *rank;                  // per node: depth-first rank among the internal nodes
+    int *index;                 // per node: its index in the mesh's tree
+    int *counter;               // the next free node
+};
+cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &t, cudaStream_t s);
+cudaError_t launch_mesh_split(const MeshBuildArgs &a, const MeshBuildScratch &t, int first, int last, int depth,
+    cudaStream_t s);
+cudaError_t launch_mesh_sizes(const MeshBuildScratch &t, int first, int last, cudaStream_t s);
+cudaError_t launch_mesh_ranks(const MeshBuildScratch &t, int first, int last, cudaStream_t s);
+cudaError_t launch_mesh_write(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, const int *slot_mesh,
+    int slots, int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t s);
+
 }  // namespace ngb

@@ -138,6 +138,17 @@ struct Renderer {
     bool geoms_bound = false;
     DevBuf<int> geom_of_instance;
     DevBuf<float> geom_scale, geom_xpos, geom_xmat;
+    // Meshes whose vertices change (update_mesh): per mesh its first node (its node capacity is 2T - 1), first
+    // packed triangle, triangle and vertex counts, current node count, and where its indices and kept vertex
+    // normals are in mesh_indices / mesh_normals (-1: none); per slot its mesh. The device rebuild's scratch.
+    std::vector<int> mesh_node_base, mesh_tri_base, mesh_tris, mesh_verts, mesh_nodes, mesh_index_at, mesh_normal_at;
+    DevBuf<uint32_t> mesh_indices;
+    DevBuf<float> mesh_normals, mesh_stage;
+    DevBuf<int> slot_mesh;
+    DevBuf<float> mb_box, mb_centre, mb_node_box;
+    DevBuf<uint32_t> mb_order;
+    DevBuf<int> mb_lpos, mb_rpos, mb_begin, mb_end, mb_left, mb_size, mb_rank, mb_index, mb_counter;
+    int *host_count = nullptr;  // pinned: a level's node count read back during a mesh rebuild
     // Staging for host inputs and the renderer's own outputs.
     DevBuf<float> cameras, ray_origins, ray_directions;
     DevBuf<uint8_t> out_rgb;
@@ -186,6 +197,7 @@ struct Renderer {
     void bind_bodies(int bpw, const int32_t *boi, const float *lp, const float *sc);
     void set_body_poses(const float *poses, int memory);
     void bind_geoms(int gpw, const int32_t *goi, const float *sc);
+    void update_mesh(int mesh, const float *vertices, const float *normals, int memory);
     void set_geom_poses(const float *xpos, const float *xmat, int memory);
     void check_render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory);
     void render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
@@ -264,6 +276,7 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
     CK(cudaEventCreate(&ev_stage[1]));
     CK(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
     CK(cudaHostAlloc(&host_error, sizeof(int), cudaHostAllocDefault));
+    CK(cudaHostAlloc(&host_count, sizeof(int), cudaHostAllocDefault));
     *host_error = 0;
     error_flag.ensure(1);
     CK(cudaMemsetAsync(error_flag.p, 0, sizeof(int), stream));
@@ -339,7 +352,7 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
     }
 
     // The meshes' trees, built once on the host (src/mesh_build.cpp:91-157), and the slots' tables.
-    const BuiltMeshes built = build_meshes(s);
+    const BuiltMeshes built = build_meshes(s, true);
     auto upload = [&](auto &buf, const auto &vec) {
         using T = std::remove_pointer_t<decltype(buf.p)>;
         const size_t bytes = vec.size() * sizeof(typename std::decay_t<decltype(vec)>::value_type);
@@ -387,6 +400,28 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
         root_ref_of_slot[i] = make_int2(built.root_refs[2 * mesh], built.root_refs[2 * mesh + 1]);
     }
     upload(slot_root, root_ref_of_slot);
+    // What a device rebuild of a mesh's tree needs: its place in the packed arrays, its indices, its normals.
+    {
+        std::vector<uint32_t> all_indices;
+        std::vector<float> all_normals;
+        for (int m = 0; m < s.mesh_count; ++m) {
+            const ngb_mesh &mesh = s.meshes[m];
+            mesh_node_base.push_back(built.roots[m]);
+            mesh_tri_base.push_back(mesh_base[m]);
+            mesh_tris.push_back(mesh.index_count / 3);
+            mesh_verts.push_back(mesh.vertex_count);
+            mesh_nodes.push_back(built.node_counts[m]);
+            mesh_index_at.push_back(static_cast<int>(all_indices.size()));
+            all_indices.insert(all_indices.end(), mesh.indices, mesh.indices + mesh.index_count);
+            mesh_normal_at.push_back(mesh.normals ? static_cast<int>(all_normals.size()) : -1);
+            if (mesh.normals) all_normals.insert(all_normals.end(), mesh.normals, mesh.normals + 3 * static_cast<size_t>(mesh.vertex_count));
+        }
+        if (!all_indices.empty()) upload(mesh_indices, all_indices);
+        if (!all_normals.empty()) upload(mesh_normals, all_normals);
+        std::vector<int> mesh_of_slot(slots);
+        for (int i = 0; i < slots; ++i) mesh_of_slot[i] = s.instances[i].mesh;
+        if (slots > 0) upload(slot_mesh, mesh_of_slot);
+    }
     tlas_pairs.ensure(4 * std::max<long long>(n - 1, 1));
     upload(slot_bounds, bounds_of_slot);
     upload(slot_material, material_of_slot);
@@ -445,6 +480,7 @@ Renderer::~Renderer() {
         if (e) cudaEventDestroy(e);
     if (ev_done) cudaEventDestroy(ev_done);
     if (host_error) cudaFreeHost(host_error);
+    if (host_count) cudaFreeHost(host_count);
     if (own_stream) cudaStreamDestroy(own_stream);
     // The DevBufs free themselves; the device must be current while they do, so release them here.
     blas.release(), tris.release(), attrs.release(), tri_index.release(), slot_blas_root.release();
@@ -453,6 +489,10 @@ Renderer::~Renderer() {
     keys.release(), sorted_ids.release(), roots.release(), parent.release(), arrivals.release();
     body_of_instance.release(), local_pose.release(), local_scale.release(), body_poses.release();
     geom_of_instance.release(), geom_scale.release(), geom_xpos.release(), geom_xmat.release();
+    mesh_indices.release(), mesh_normals.release(), mesh_stage.release(), slot_mesh.release();
+    mb_box.release(), mb_centre.release(), mb_node_box.release(), mb_order.release(), mb_lpos.release();
+    mb_rpos.release(), mb_begin.release(), mb_end.release(), mb_left.release(), mb_size.release();
+    mb_rank.release(), mb_index.release(), mb_counter.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
@@ -685,6 +725,93 @@ void Renderer::set_geom_poses(const float *xpos, const float *xmat, int memory) 
         r = geom_xmat.p;
     }
     build(nullptr, 2, p, r);
+    finish();
+}
+
+// New vertex positions for one mesh: its tree rebuilt on the device as the host builds it at creation
+// (src/bvh.cpp:46-174, src/mesh_build.cpp:91-157), then every world's instance tree from the current
+// transforms, whose boxes hold the mesh's new box.
+void Renderer::update_mesh(int mesh, const float *vertices, const float *normals, int memory) {
+    require(mesh >= 0 && mesh < static_cast<int>(mesh_tris.size()),
+        "mesh " + std::to_string(mesh) + " does not exist: there are " + std::to_string(mesh_tris.size()) + " meshes");
+    require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
+    require(vertices != nullptr, "vertices must not be null");
+    require(normals == nullptr || mesh_normal_at[mesh] >= 0,
+        "mesh " + std::to_string(mesh) + " was made without vertex normals, so update_mesh cannot give it some");
+    const int V = mesh_verts[mesh], T = mesh_tris[mesh];
+    const std::string name = "mesh " + std::to_string(mesh);
+    if (memory == NGB_MEMORY_HOST) {
+        for (int i = 0; i < V; ++i)
+            require(all_finite(vertices + 3 * static_cast<size_t>(i), 3), name + " vertex " + std::to_string(i) +
+                " has a NaN or infinite value");
+        if (normals)
+            for (int i = 0; i < V; ++i)
+                require(all_finite(normals + 3 * static_cast<size_t>(i), 3), name + " normal " + std::to_string(i) +
+                    " has a NaN or infinite value");
+    }
+    const cudaMemcpyKind kind = memory == NGB_MEMORY_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const float *dv = vertices;
+    if (memory == NGB_MEMORY_HOST) {
+        mesh_stage.ensure(3 * static_cast<size_t>(V));
+        CK(cudaMemcpyAsync(mesh_stage.p, vertices, 3 * static_cast<size_t>(V) * sizeof(float), kind, stream));
+        dv = mesh_stage.p;
+    }
+    float *kept_normals = mesh_normal_at[mesh] >= 0 ? mesh_normals.p + mesh_normal_at[mesh] : nullptr;
+    if (normals) CK(cudaMemcpyAsync(kept_normals, normals, 3 * static_cast<size_t>(V) * sizeof(float), kind, stream));
+
+    MeshBuildScratch t{};
+    t.box = mb_box.ensure(6 * static_cast<size_t>(T));
+    t.centre = mb_centre.ensure(3 * static_cast<size_t>(T));
+    t.order = mb_order.ensure(T);
+    t.lpos = mb_lpos.ensure(T);
+    t.rpos = mb_rpos.ensure(T);
+    const size_t cap = 2 * static_cast<size_t>(T) - 1;
+    t.node_box = mb_node_box.ensure(6 * cap);
+    t.begin = mb_begin.ensure(cap);
+    t.end = mb_end.ensure(cap);
+    t.left = mb_left.ensure(cap);
+    t.size = mb_size.ensure(cap);
+    t.rank = mb_rank.ensure(cap);
+    t.index = mb_index.ensure(cap);
+    t.counter = mb_counter.ensure(1);
+    MeshBuildArgs a{};
+    a.vertices = dv;
+    a.normals = kept_normals;
+    a.indices = mesh_indices.p + mesh_index_at[mesh];
+    a.triangles = T;
+    a.node_base = mesh_node_base[mesh];
+    a.tri_base = mesh_tri_base[mesh];
+    a.blas = blas.p;
+    a.pairs = blas_pairs.p;
+    a.tris = tris.p;
+    a.attrs = attrs.p;
+    a.tri_index = tri_index.p;
+    a.tri_of_local = tri_of_local.p;
+    // The mesh's whole node capacity is cleared: nodes past the new tree's last are zero, as at creation.
+    CK(cudaMemsetAsync(blas.p + 2 * static_cast<size_t>(a.node_base), 0, 2 * cap * sizeof(float4), stream));
+    CK(cudaMemsetAsync(blas_pairs.p + 4 * static_cast<size_t>(a.node_base), 0, 4 * cap * sizeof(float4), stream));
+    CK(launch_mesh_prepare(a, t, stream));
+    // One depth at a time; each depth's new nodes are read back to size the next launch.
+    std::vector<std::pair<int, int>> levels;
+    int first = 0, last = 1;
+    for (int depth = 0;; ++depth) {
+        CK(launch_mesh_split(a, t, first, last, depth, stream));
+        levels.emplace_back(first, last);
+        CK(cudaMemcpyAsync(host_count, t.counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaEventRecord(ev_done, stream));
+        wait(ev_done, timeout);
+        const int next = *host_count;
+        require(next >= last && static_cast<size_t>(next) <= cap && depth <= 61, name + ": the tree rebuild went wrong");
+        if (next == last) break;
+        first = last;
+        last = next;
+    }
+    for (size_t l = levels.size(); l-- > 0;) CK(launch_mesh_sizes(t, levels[l].first, levels[l].second, stream));
+    for (const auto &lv : levels) CK(launch_mesh_ranks(t, lv.first, lv.second, stream));
+    CK(launch_mesh_write(a, t, last, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
+        slot_bounds.p, slot_hull.p, stream));
+    mesh_nodes[mesh] = last;
+    if (n > 0) build(matrices.p, 0, nullptr);
     finish();
 }
 
@@ -948,6 +1075,39 @@ int ngb_bind_geoms(ngb_renderer *h, int32_t gpw, const int32_t *goi, const float
 
 int ngb_set_geom_poses(ngb_renderer *h, const float *xpos, const float *xmat, int32_t memory) {
     return guarded(h, [&](ngb::Renderer &r) { r.set_geom_poses(xpos, xmat, memory); });
+}
+
+int ngb_update_mesh(ngb_renderer *h, int32_t mesh, const float *vertices, const float *normals, int32_t memory) {
+    return guarded(h, [&](ngb::Renderer &r) { r.update_mesh(mesh, vertices, normals, memory); });
+}
+
+int ngb_inspect_mesh(ngb_renderer *h, int32_t mesh, int32_t *node_count, int32_t *triangle_count, int32_t *nodes,
+    float *triangles, float *bounds, int32_t *triangle_index) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(mesh >= 0 && mesh < static_cast<int>(r.mesh_tris.size()), "mesh " + std::to_string(mesh) +
+            " does not exist: there are " + std::to_string(r.mesh_tris.size()) + " meshes");
+        ngb::require(node_count != nullptr && triangle_count != nullptr, "node_count and triangle_count must not be null");
+        const int N = r.mesh_nodes[mesh], T = r.mesh_tris[mesh];
+        const int node_base = r.mesh_node_base[mesh], tri_base = r.mesh_tri_base[mesh];
+        *node_count = N;
+        *triangle_count = T;
+        if (!nodes && !triangles && !bounds && !triangle_index) return;
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+        std::vector<int32_t> words(8 * static_cast<size_t>(N));
+        CK(cudaMemcpy(words.data(), r.blas.p + 2 * static_cast<size_t>(node_base), words.size() * 4, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < N; ++i) words[8 * i + 3] -= words[8 * i + 7] > 0 ? tri_base : node_base;  // mesh-local
+        if (nodes) std::memcpy(nodes, words.data(), words.size() * 4);
+        if (bounds) {
+            std::memcpy(bounds, words.data(), 3 * sizeof(float));
+            std::memcpy(bounds + 3, words.data() + 4, 3 * sizeof(float));
+        }
+        if (triangles)
+            CK(cudaMemcpy(triangles, r.tris.p + 3 * static_cast<size_t>(tri_base), 48 * static_cast<size_t>(T),
+                cudaMemcpyDeviceToHost));
+        if (triangle_index)
+            CK(cudaMemcpy(triangle_index, r.tri_index.p + tri_base, 4 * static_cast<size_t>(T), cudaMemcpyDeviceToHost));
+    });
 }
 
 int ngb_render(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint32_t outputs, int32_t frame,

@@ -184,6 +184,41 @@ class BatchRenderer:
         check(self._lib.ngb_set_geom_poses(self._h, p, r, mem_p), self._h)
         self._keep = (keep_p, keep_r)
 
+    def update_mesh(self, mesh, vertices, normals=None):
+        """New vertex positions for mesh `mesh` (the vertex count and triangles it was made with): (V, 3) floats,
+        host or CUDA, and optionally new vertex normals. Its tree is rebuilt on the GPU as the renderer's
+        construction builds it on the host (src/bvh.cpp:46-174), node for node, and every world's instance tree
+        is rebuilt from the current transforms."""
+        p, mem, keep = self._input(vertices, "vertices")
+        pn = None
+        if normals is not None:
+            pn, mem_n, keep_n = self._input(normals, "normals")
+            if mem_n != mem:
+                raise ValueError("vertices and normals must both be CUDA arrays or both host arrays")
+            if _count(normals) != _count(vertices):
+                raise ValueError(f"normals has {_count(normals)} values, but vertices has {_count(vertices)}")
+        m = self._desc.meshes[mesh] if 0 <= mesh < len(self._desc.meshes) else None
+        if m is not None and _count(vertices) != m.vertices.size:
+            raise ValueError(f"mesh {mesh} has {len(m.vertices)} vertices, but {_count(vertices)} values were given "
+                             f"({len(m.vertices)} x 3 are needed)")
+        self._stream()
+        check(self._lib.ngb_update_mesh(self._h, int(mesh), p, pn, mem), self._h)
+        self._keep = keep
+
+    def inspect_mesh(self, mesh) -> dict:
+        """Mesh `mesh`'s tree as the renderer holds it now, in build_meshes's format for that mesh alone."""
+        nn, nt = C.c_int32(), C.c_int32()
+        check(self._lib.ngb_inspect_mesh(self._h, int(mesh), C.byref(nn), C.byref(nt), None, None, None, None), self._h)
+        nodes = np.zeros((nn.value, 8), np.int32)
+        tris = np.zeros((nt.value, 12), np.float32)
+        bounds = np.zeros((1, 6), np.float32)
+        tidx = np.zeros(nt.value, np.int32)
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(self._lib.ngb_inspect_mesh(self._h, int(mesh), C.byref(nn), C.byref(nt), vp(nodes), vp(tris), vp(bounds),
+                                         vp(tidx)), self._h)
+        return {"nodes": nodes, "triangles": tris, "roots": np.zeros(1, np.int32), "bounds": bounds,
+                "triangle_index": tidx}
+
     # ------------------------------------------------------------------------------------------ rendering --
 
     def _buffer(self, key, shape, dtype):
