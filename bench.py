@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--no-reference-cuda", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
     p.add_argument("--config", default="body_worlds",
-                   choices=["body_worlds", "large_world", "differentiable", "uneven"],
+                   choices=["body_worlds", "large_world", "differentiable", "uneven", "mesh_update"],
                    help="body_worlds: the headline (4096 worlds x 64x64); large_world: one world of 100,000 "
                         "instances at 1280x720 with a 64 x 2048 LiDAR sweep, poses redrawn every frame; "
                         "differentiable: 1024 worlds x 128x128 depth+normals, forward+backward against forward; "
@@ -717,6 +717,94 @@ def reference_cuda_large(wl, torch, mats, cams, lo, ld, steps, warmup):
             "what": "neraulgraphics 0.5.0 CudaBackend, same frames on the device, median step"}
 
 
+def run_mesh_update(args, rank, world, local_rank, dist):
+    """Meshes whose vertices move: the five meshes of the large world (12, 320, 512, 1280 and 20,480
+    triangles) get new vertex positions every step (a twist and a stretch that change from step to step), each
+    mesh's tree is rebuilt on the GPU (update_mesh: the host's binned SAH build, node for node) and the instance
+    trees of 64 worlds x 5 instances are rebuilt around the meshes' new boxes. `value`: vertices already on the
+    GPU; `e2e`: vertices from pinned host memory. Timed on the host clock around synchronised steps (the rebuild
+    reads each tree level's size back), with CUDA events beside it. The reference changes a mesh only by
+    building a new renderer, whose host build_meshes (src/mesh_build.cpp:91-157) is timed here on the same
+    vertices (cpu_baseline)."""
+    import torch
+
+    import neraulgraphics_b200 as ng
+    import oracle as O
+    from neraulgraphics_b200 import scene as S
+    from neraulgraphics_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    base = workloads.large_world(instances=5).desc.meshes
+    worlds = 64
+    insts = [S.Instance(i, S.make_transform((2.0 * i - 4.0, 0.0, -6.0), (0, 0, 0, 1), 1.0)) for i in range(5)]
+    r = ng.BatchRenderer(64, 64, worlds, 1, [], [workloads.LIGHT], None, base, insts, device=dev)
+
+    def shape(mesh, step):
+        v = mesh.vertices.astype(np.float64)
+        a = (0.2 + 0.05 * step) * v[:, 1]
+        x = v[:, 0] * np.cos(a) - v[:, 2] * np.sin(a)
+        z = v[:, 0] * np.sin(a) + v[:, 2] * np.cos(a)
+        return np.stack([(1.0 + 0.02 * step) * x, v[:, 1], z], 1).astype(np.float32)
+
+    steps = [[shape(m, s) for m in base] for s in range(W + K)]
+    on_dev = [[torch.from_numpy(v).to(dev) for v in st] for st in steps]
+    pinned = [[torch.from_numpy(v).pin_memory() for v in st] for st in steps]
+
+    def run(arrays):
+        for s in range(W):
+            for m, v in enumerate(arrays[s]):
+                r.update_mesh(m, v)
+        torch.cuda.synchronize()
+        host_ms, dev_ms = [], []
+        for s in range(W, W + K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record()
+            for m, v in enumerate(arrays[s]):
+                r.update_mesh(m, v)
+            e1.record()
+            torch.cuda.synchronize()
+            host_ms.append(1000.0 * (time.perf_counter() - t0))
+            dev_ms.append(e0.elapsed_time(e1))
+        return statistics.median(host_ms), statistics.median(dev_ms)
+
+    with ClockSampler(local_rank) as clocks:
+        host_ms, dev_ms = run(on_dev)
+        e2e_ms, _ = run([[t.numpy() for t in st] for st in pinned])
+    node_ok = all(np.array_equal(r.inspect_mesh(i)["nodes"], ng.build_meshes([S.Mesh(v, m.triangles)])["nodes"])
+                  for i, (v, m) in enumerate(zip(steps[-1], base)))
+    if rank != 0:
+        return None
+    cpu = None
+    if O.reference_available():
+        ref_ms = []
+        for s in range(min(K, 10)):
+            t0 = time.perf_counter()
+            O.ref_build_meshes([S.Mesh(v, m.triangles) for v, m in zip(steps[W + s], base)])
+            ref_ms.append(1000.0 * (time.perf_counter() - t0))
+        cpu = {"value": round(statistics.median(ref_ms), 4), "unit": "ms per step", "cores": 1, "kind": "reference",
+               "sample": "the reference's build_meshes (host, one thread) of the same five moved meshes, "
+                         f"median of {len(ref_ms)} steps"}
+    tris = sum(len(m.triangles) for m in base)
+    return {
+        "metric": f"ms per step: five mesh trees ({tris} triangles, 12 to 20,480 per mesh) rebuilt from new vertex "
+                  "positions, then the instance trees of 64 worlds",
+        "value": round(host_ms, 4), "unit": "ms per step", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(host_ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (the large world's five meshes, twisted and stretched per step)",
+        "config": {"workload": "mesh_update: box 12, icosphere s2 320, cylinder 512, icosphere s3 1280, icosphere s5 "
+                               "20480 triangles; 64 worlds x 5 instances", "l2": "inputs of 0.5 MB: L2 not flushed"},
+        "device_ms_per_step": round(dev_ms, 4),
+        "trees_equal_host_build": bool(node_ok),
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms per step",
+                "h2d_bytes_per_step": int(sum(v.nbytes for v in steps[0])), "d2h_bytes_per_step": 0},
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+    }
+
+
 def run_reference(args, rank):
     """The reference's own CPU implementation, rank 0 only, with every host core."""
     from neraulgraphics_b200 import workloads
@@ -774,7 +862,7 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device(f"cuda:{local_rank}"))
         run = {"body_worlds": run_ours, "large_world": run_large, "differentiable": run_differentiable,
-               "uneven": run_uneven}[args.config]
+               "uneven": run_uneven, "mesh_update": run_mesh_update}[args.config]
         line = run(args, rank, world, local_rank, dist)
         if dist:
             dist.destroy_process_group()

@@ -12,10 +12,13 @@
 //     test with the k-th element from the right that passes it, until the two meet: the same swaps are made
 //     here from two prefix counts, in parallel;
 //   - the host gives a node's two children the indices 2k + 1 and 2k + 2 when it splits the k-th internal
-//     node in depth-first, left-first order; that order's rank follows from the subtrees' internal-node
-//     counts (bottom-up) and is handed down from the root (top-down).
-// Node and tree sizes: a tree over T triangles has at most 2T - 1 nodes, so the nodes are numbered in
-// scratch arrays of 2T - 1, level after level (the host reads each level's node count back).
+//     node in depth-first, left-first order. An internal node X is preceded in that order by every internal
+//     node that starts (in the leaf order) before X does, and by the internal nodes that start where X starts
+//     and lie above it (a chain of left children at consecutive depths), so its rank is a prefix count over
+//     the start positions plus its depth below the chain's top, with no walk over the tree.
+// Node and tree sizes: a tree over T triangles has at most 2T - 1 nodes, numbered in scratch arrays of
+// 2T - 1 in level order. Each depth's launch records the next depth's range on the device, so the host
+// queues several depths before it reads back whether the tree is finished.
 #include <climits>
 #include <cstdint>
 
@@ -103,11 +106,13 @@ __global__ void prepare_kernel(const MeshBuildArgs a, const MeshBuildScratch t) 
     if (i == 0) {
         t.begin[0] = 0;
         t.end[0] = a.triangles;
-        t.rank[0] = 0;
         t.index[0] = 0;
         t.counter[0] = 1;
+        t.range[0] = make_int2(0, 1);
     }
     if (i >= a.triangles) return;
+    t.starts[i] = 0;
+    t.top[i] = INT_MAX;
     Box b = empty_box();
     for (int k = 0; k < 3; ++k) {
         const float *v = a.vertices + 3 * static_cast<size_t>(__ldg(a.indices + 3 * static_cast<size_t>(i) + k));
@@ -129,6 +134,8 @@ struct SplitSmem {
     unsigned long long box_key[12];              // node box lo/hi (6), centroid box lo/hi (6)
     unsigned long long bin_key[3][BINS][6];      // per axis and bin: its box lo/hi
     int bin_count[3][BINS];
+    float node[12];                              // the decoded node box and centroid box
+    float bin_box[3][BINS][6];                   // the decoded bin boxes (empty bins: +inf lo, -inf hi)
     int warp_sum[WARPS];
     int total;
     float cbox[6];
@@ -151,13 +158,14 @@ __device__ __forceinline__ int cta_scan(SplitSmem &sm, bool flag, int &total) {
     return before + __popc(m & ((1u << lane) - 1u));
 }
 
-// Splits every node of one depth: [first, last) in level order, one CTA per node.
-__global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int first,
-    int last, int depth) {
+// Splits every node of one depth (its range recorded by the depth before), one CTA per node.
+__global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int depth) {
     __shared__ SplitSmem sm;
     const int tid = threadIdx.x, lane = tid & 31;
-    for (int x = first + blockIdx.x; x < last; x += gridDim.x) {
+    const int2 level = t.range[depth];
+    for (int x = level.x + blockIdx.x; x < level.y; x += gridDim.x) {
         const int begin = t.begin[x], end = t.end[x], count = end - begin;
+        if (tid == 0) t.depth[x] = depth;
         for (int k = tid; k < 12; k += THREADS) sm.box_key[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
         for (int k = tid; k < 3 * BINS * 6; k += THREADS)
             (&sm.bin_key[0][0][0])[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
@@ -198,16 +206,19 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             }
         }
         __syncthreads();
+        if (tid < 12) {  // the values the keys point at, one per thread
+            const bool is_max = (tid % 6) >= 3;
+            const uint32_t p = t.order[key_pos(sm.box_key[tid], is_max)];
+            sm.node[tid] = tid < 6 ? t.box[6 * static_cast<size_t>(p) + tid] : t.centre[3 * static_cast<size_t>(p) + (tid - 6) % 3];
+        }
+        __syncthreads();
         Box box;
         float cb[6];
-        for (int k = 0; k < 12; ++k) {
-            const bool is_max = (k % 6) >= 3;
-            const uint32_t p = t.order[key_pos(sm.box_key[k], is_max)];
-            const float v = k < 6 ? t.box[6 * static_cast<size_t>(p) + k] : t.centre[3 * static_cast<size_t>(p) + (k - 6) % 3];
-            if (k < 3) box.lo[k] = v;
-            else if (k < 6) box.hi[k - 3] = v;
-            else cb[k - 6] = v;
+        for (int k = 0; k < 3; ++k) {
+            box.lo[k] = sm.node[k];
+            box.hi[k] = sm.node[3 + k];
         }
+        for (int k = 0; k < 6; ++k) cb[k] = sm.node[6 + k];
 
         // Bins on every axis whose centroids spread (src/bvh.cpp:94-107).
         if (count > 1) {
@@ -219,15 +230,31 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
                     const float scale = static_cast<float>(BINS) / extent;
                     const int b = bin_of(t.centre[3 * static_cast<size_t>(p) + axis], cb[axis], scale);
                     atomicAdd(&sm.bin_count[axis][b], 1);
+                    // The shared value only moves one way, so a key that does not beat it now never will:
+                    // most keys are dropped by a plain read instead of a contended atomic.
                     for (int c = 0; c < 6; ++c) {
                         const bool is_max = c >= 3;
                         const unsigned long long key = order_key(t.box[6 * static_cast<size_t>(p) + c],
                             static_cast<unsigned>(i), is_max);
-                        if (is_max) atomicMax(&sm.bin_key[axis][b][c], key);
-                        else atomicMin(&sm.bin_key[axis][b][c], key);
+                        unsigned long long *slot = &sm.bin_key[axis][b][c];
+                        const unsigned long long now = *reinterpret_cast<volatile unsigned long long *>(slot);
+                        if (is_max ? key > now : key < now) {
+                            if (is_max) atomicMax(slot, key);
+                            else atomicMin(slot, key);
+                        }
                     }
                 }
             }
+        }
+        __syncthreads();
+        for (int e = tid; e < 3 * BINS * 6; e += THREADS) {  // the bin boxes' values, in parallel
+            const int axis = e / (BINS * 6), b = (e / 6) % BINS, c = e % 6;
+            float v = c < 3 ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
+            if (count > 1 && sm.bin_count[axis][b] > 0) {
+                const uint32_t p = t.order[key_pos(sm.bin_key[axis][b][c], c >= 3)];
+                v = t.box[6 * static_cast<size_t>(p) + c];
+            }
+            sm.bin_box[axis][b][c] = v;
         }
         __syncthreads();
 
@@ -240,17 +267,11 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
                     const float extent = cb[3 + axis] - cb[axis];
                     if (!(extent > 0.0f)) continue;
                     Box bins[BINS];
-                    for (int b = 0; b < BINS; ++b) {
-                        bins[b] = empty_box();
-                        if (sm.bin_count[axis][b] == 0) continue;
-                        for (int c = 0; c < 6; ++c) {
-                            const bool is_max = c >= 3;
-                            const uint32_t p = t.order[key_pos(sm.bin_key[axis][b][c], is_max)];
-                            const float v = t.box[6 * static_cast<size_t>(p) + c];
-                            if (c < 3) bins[b].lo[c] = v;
-                            else bins[b].hi[c - 3] = v;
+                    for (int b = 0; b < BINS; ++b)
+                        for (int c = 0; c < 3; ++c) {
+                            bins[b].lo[c] = sm.bin_box[axis][b][c];
+                            bins[b].hi[c] = sm.bin_box[axis][b][3 + c];
                         }
-                    }
                     float right_area[BINS - 1];
                     int right_count[BINS - 1];
                     Box acc = empty_box();
@@ -352,26 +373,55 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
     }
 }
 
-// Internal nodes per subtree, one depth at a time from the deepest (its children's counts are final).
-__global__ void sizes_kernel(const MeshBuildScratch t, int first, int last) {
-    const int x = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= last) return;
-    const int l = t.left[x];
-    t.size[x] = l < 0 ? 0 : 1 + t.size[l] + t.size[l + 1];
+// The next depth's nodes: those the splits of this depth appended.
+__global__ void advance_kernel(const MeshBuildScratch t, int depth) {
+    t.range[depth + 1] = make_int2(t.range[depth].y, *t.counter);
 }
 
-// Depth-first, left-first ranks among the internal nodes and the host's node indices, one depth at a time
-// from the root: the k-th internal node's children are nodes 2k + 1 and 2k + 2.
-__global__ void ranks_kernel(const MeshBuildScratch t, int first, int last) {
-    const int x = first + blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= last) return;
+// Per start position: the internal nodes starting there and the least depth among them.
+__global__ void starts_kernel(const MeshBuildScratch t, int nodes) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nodes || t.left[x] < 0) return;
+    atomicAdd(t.starts + t.begin[x], 1);
+    atomicMin(t.top + t.begin[x], t.depth[x]);
+}
+
+// Exclusive prefix sum of the start counts, one CTA.
+__global__ void __launch_bounds__(1024) prefix_kernel(const MeshBuildScratch t, int n) {
+    __shared__ int warp_sum[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? t.starts[i] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) warp_sum[warp] = incl;
+        __syncthreads();
+        int before = carry;
+        for (int w = 0; w < warp; ++w) before += warp_sum[w];
+        if (i < n) t.prefix[i] = before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + incl;
+        __syncthreads();
+    }
+}
+
+// The host's node indices: the k-th internal node in depth-first order has children 2k + 1 and 2k + 2.
+__global__ void index_kernel(const MeshBuildScratch t, int nodes) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= nodes) return;
     const int l = t.left[x];
     if (l < 0) return;
-    const int r = t.rank[x];
-    t.rank[l] = r + 1;
-    t.rank[l + 1] = r + 1 + t.size[l];
-    t.index[l] = 2 * r + 1;
-    t.index[l + 1] = 2 * r + 2;
+    const int b = t.begin[x];
+    const int k = t.prefix[b] + t.depth[x] - t.top[b];
+    t.index[l] = 2 * k + 1;
+    t.index[l + 1] = 2 * k + 2;
 }
 
 // The packed tree (src/mesh_build.cpp:91-157): bvh::Node records with global indices, and the child-pair
@@ -458,23 +508,19 @@ cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &
     return cudaGetLastError();
 }
 
-cudaError_t launch_mesh_split(const MeshBuildArgs &a, const MeshBuildScratch &t, int first, int last, int depth,
-    cudaStream_t s) {
-    const int tasks = last - first;
-    if (tasks <= 0) return cudaSuccess;
-    split_kernel<<<tasks < 4096 ? tasks : 4096, THREADS, 0, s>>>(a, t, first, last, depth);
+cudaError_t launch_mesh_level(const MeshBuildArgs &a, const MeshBuildScratch &t, int depth, cudaStream_t s) {
+    // A depth holds at most 2^depth nodes, and the CTAs stride over whatever it holds.
+    const int most = depth < 12 ? 1 << depth : 4096;
+    const int cap = a.triangles < most ? a.triangles : most;
+    split_kernel<<<cap > 0 ? cap : 1, THREADS, 0, s>>>(a, t, depth);
+    advance_kernel<<<1, 1, 0, s>>>(t, depth);
     return cudaGetLastError();
 }
 
-cudaError_t launch_mesh_sizes(const MeshBuildScratch &t, int first, int last, cudaStream_t s) {
-    if (last <= first) return cudaSuccess;
-    sizes_kernel<<<blocks_for(last - first), 256, 0, s>>>(t, first, last);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mesh_ranks(const MeshBuildScratch &t, int first, int last, cudaStream_t s) {
-    if (last <= first) return cudaSuccess;
-    ranks_kernel<<<blocks_for(last - first), 256, 0, s>>>(t, first, last);
+cudaError_t launch_mesh_number(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, cudaStream_t s) {
+    starts_kernel<<<blocks_for(nodes), 256, 0, s>>>(t, nodes);
+    prefix_kernel<<<1, 1024, 0, s>>>(t, a.triangles);
+    index_kernel<<<blocks_for(nodes), 256, 0, s>>>(t, nodes);
     return cudaGetLastError();
 }
 

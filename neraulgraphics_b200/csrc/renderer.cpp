@@ -147,7 +147,8 @@ struct Renderer {
     DevBuf<int> slot_mesh;
     DevBuf<float> mb_box, mb_centre, mb_node_box;
     DevBuf<uint32_t> mb_order;
-    DevBuf<int> mb_lpos, mb_rpos, mb_begin, mb_end, mb_left, mb_size, mb_rank, mb_index, mb_counter;
+    DevBuf<int> mb_lpos, mb_rpos, mb_begin, mb_end, mb_left, mb_depth, mb_index, mb_counter, mb_starts, mb_top, mb_prefix;
+    DevBuf<int2> mb_range;
     int *host_count = nullptr;  // pinned: a level's node count read back during a mesh rebuild
     // Staging for host inputs and the renderer's own outputs.
     DevBuf<float> cameras, ray_origins, ray_directions;
@@ -491,8 +492,9 @@ Renderer::~Renderer() {
     geom_of_instance.release(), geom_scale.release(), geom_xpos.release(), geom_xmat.release();
     mesh_indices.release(), mesh_normals.release(), mesh_stage.release(), slot_mesh.release();
     mb_box.release(), mb_centre.release(), mb_node_box.release(), mb_order.release(), mb_lpos.release();
-    mb_rpos.release(), mb_begin.release(), mb_end.release(), mb_left.release(), mb_size.release();
-    mb_rank.release(), mb_index.release(), mb_counter.release();
+    mb_rpos.release(), mb_begin.release(), mb_end.release(), mb_left.release(), mb_depth.release();
+    mb_index.release(), mb_counter.release(), mb_starts.release(), mb_top.release(), mb_prefix.release();
+    mb_range.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
@@ -770,10 +772,13 @@ void Renderer::update_mesh(int mesh, const float *vertices, const float *normals
     t.begin = mb_begin.ensure(cap);
     t.end = mb_end.ensure(cap);
     t.left = mb_left.ensure(cap);
-    t.size = mb_size.ensure(cap);
-    t.rank = mb_rank.ensure(cap);
+    t.depth = mb_depth.ensure(cap);
     t.index = mb_index.ensure(cap);
     t.counter = mb_counter.ensure(1);
+    t.range = mb_range.ensure(MESH_LEVELS + 1);
+    t.starts = mb_starts.ensure(T);
+    t.top = mb_top.ensure(T);
+    t.prefix = mb_prefix.ensure(T);
     MeshBuildArgs a{};
     a.vertices = dv;
     a.normals = kept_normals;
@@ -791,26 +796,25 @@ void Renderer::update_mesh(int mesh, const float *vertices, const float *normals
     CK(cudaMemsetAsync(blas.p + 2 * static_cast<size_t>(a.node_base), 0, 2 * cap * sizeof(float4), stream));
     CK(cudaMemsetAsync(blas_pairs.p + 4 * static_cast<size_t>(a.node_base), 0, 4 * cap * sizeof(float4), stream));
     CK(launch_mesh_prepare(a, t, stream));
-    // One depth at a time; each depth's new nodes are read back to size the next launch.
-    std::vector<std::pair<int, int>> levels;
-    int first = 0, last = 1;
-    for (int depth = 0;; ++depth) {
-        CK(launch_mesh_split(a, t, first, last, depth, stream));
-        levels.emplace_back(first, last);
+    // Depth after depth, several queued at a time; the node count read back after each batch says whether the
+    // last depth split anything (a tree over T triangles is about log2 T deep; a node at depth 60 is a leaf).
+    constexpr int BATCH = 6;
+    int nodes = 1;
+    for (int depth = 0; depth < MESH_LEVELS;) {
+        const int stop = std::min(depth + BATCH, MESH_LEVELS);
+        for (; depth < stop; ++depth) CK(launch_mesh_level(a, t, depth, stream));
         CK(cudaMemcpyAsync(host_count, t.counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
         CK(cudaEventRecord(ev_done, stream));
         wait(ev_done, timeout);
-        const int next = *host_count;
-        require(next >= last && static_cast<size_t>(next) <= cap && depth <= 61, name + ": the tree rebuild went wrong");
-        if (next == last) break;
-        first = last;
-        last = next;
+        const int now = *host_count;
+        require(now >= nodes && static_cast<size_t>(now) <= cap, name + ": the tree rebuild went wrong");
+        if (now == nodes) break;
+        nodes = now;
     }
-    for (size_t l = levels.size(); l-- > 0;) CK(launch_mesh_sizes(t, levels[l].first, levels[l].second, stream));
-    for (const auto &lv : levels) CK(launch_mesh_ranks(t, lv.first, lv.second, stream));
-    CK(launch_mesh_write(a, t, last, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
+    CK(launch_mesh_number(a, t, nodes, stream));
+    CK(launch_mesh_write(a, t, nodes, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
         slot_bounds.p, slot_hull.p, stream));
-    mesh_nodes[mesh] = last;
+    mesh_nodes[mesh] = nodes;
     if (n > 0) build(matrices.p, 0, nullptr);
     finish();
 }
