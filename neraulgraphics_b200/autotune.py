@@ -57,7 +57,11 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
     returns {"kernel", "threads", "registers", "refill", "leaf_batch", "ms", "timings"}."""
     import torch
     outputs = dict(rgb=rgb, depth=depth, normals=normals, object_ids=object_ids)
+    # Worlds of at most TILE_MAX_INSTANCES instances: the tile kernels' shapes. Larger worlds: the persistent
+    # kernel's shapes and the tile kernels walking each world's tree as a packet, whichever is faster here.
     kernel = 3 if renderer.instances_per_world <= TILE_MAX_INSTANCES else 2
+    candidates = ([(3,) + c for c in TILE_CANDIDATES] if kernel == 3 else
+                  [(2,) + c for c in CANDIDATES] + [(3,) + c for c in TILE_CANDIDATES + [(128, 80, 0, 0)]])
     key = _key(renderer, tuple(sorted(k for k, v in outputs.items() if v))) + f"|kernel{kernel}"
     cache = _load() if use_cache else {}
     if key in cache:
@@ -66,8 +70,8 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
         return dict(best, cached=True)
     timings = []
     start = time.perf_counter()
-    for threads, regs, refill, batch in (TILE_CANDIDATES if kernel == 3 else CANDIDATES):
-        _apply(renderer, {"kernel": kernel, "threads": threads, "refill": refill, "registers": regs,
+    for kind, threads, regs, refill, batch in candidates:
+        _apply(renderer, {"kernel": kind, "threads": threads, "refill": refill, "registers": regs,
                           "leaf_batch": batch})
         renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         torch.cuda.synchronize()
@@ -77,7 +81,7 @@ def tune(renderer, cameras, fov=1.0, *, rgb=True, depth=False, normals=False, ob
             renderer.render(cameras, fov, 1, zero_copy=True, **outputs)
         e1.record()
         e1.synchronize()
-        timings.append({"kernel": kernel, "threads": threads, "registers": regs, "refill": refill,
+        timings.append({"kernel": kind, "threads": threads, "registers": regs, "refill": refill,
                         "leaf_batch": batch, "ms": e0.elapsed_time(e1) / repeats})
         if time.perf_counter() - start > budget_s:
             break

@@ -863,12 +863,12 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
         a.hit_v = hit_v.ensure(pixels());
     }
     a.error_flag = error_flag.p;
-    // The persistent and tile kernels cover one sample per pixel, at most one light and no bounces, the tile
-    // kernel for worlds of at most TILE_MAX_INSTANCES instances; everything else takes the per-pixel kernel,
-    // which runs trace in full.
+    // The persistent and tile kernels cover one sample per pixel, at most one light and no bounces; everything
+    // else takes the per-pixel kernel, which runs trace in full. Automatic: the tile kernels for worlds of at
+    // most TILE_MAX_INSTANCES instances (candidate lists), the persistent kernel above.
     const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
-    const bool tiles_ok = persistent_ok && (params.instance_count == 0 || params.per_world <= TILE_MAX_INSTANCES);
-    const bool tiles = tiles_ok && (kernel_choice == 0 || kernel_choice == 3 || uneven);
+    const bool small_worlds = params.instance_count == 0 || params.per_world <= TILE_MAX_INSTANCES;
+    const bool tiles = persistent_ok && (uneven || kernel_choice == 3 || (kernel_choice == 0 && small_worlds));
     const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
     require(!uneven || tiles, "worlds of uneven sizes render with one sample per pixel, at most one light and no "
         "reflective material");

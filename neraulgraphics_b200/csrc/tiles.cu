@@ -45,6 +45,16 @@ struct WarpSmem {
     int leaf_in[CAP];        // collected, in leaf order
     float bound_in[CAP];
 };
+// CAP 0: worlds of any size, walked as a packet (packet_walk); the warp's stack of the world tree's nodes.
+template <>
+struct WarpSmem<0> {
+    int ref[TLAS_STACK];
+    int count[TLAS_STACK];
+};
+
+__device__ __forceinline__ float warp_max(float v) { return from_ordered(__reduce_max_sync(FULL, to_ordered(v))); }
+__device__ __forceinline__ float warp_min(float v) { return from_ordered(__reduce_min_sync(FULL, to_ordered(v))); }
+__device__ __forceinline__ float abs_dot(float3 n, float3 h) { return fabsf(n.x) * h.x + fabsf(n.y) * h.y + fabsf(n.z) * h.z; }
 
 // A world's run of sorted leaves: leaf k of world w is node n - 1 + first + k.
 __device__ __forceinline__ const float4 *world_leaves(const SceneParams &s, int world) {
@@ -163,6 +173,100 @@ __device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpS
     }
 }
 
+// A world's tree walked by the whole warp together (a packet), for worlds too large for candidate lists:
+// every internal node that some lane's ray enters before its closest hit so far is visited once for all
+// lanes, from child-pair records, the child the lanes enter first (least entry distance over the lanes) before
+// the other; an instance whose box a lane's ray enters is walked by that lane (instance_walk). Each lane gets
+// the hit its own walk of the tree finds, up to which of two equally distant hits is kept (the instance order
+// differs from a single ray's). ANY: shadow rays, done at their first hit. skip: an instance left out (a
+// shadow ray's own mesh, walked first or unreachable), or -1. The stack lives in the warp's shared memory.
+template <bool ANY>
+__device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &sm, int lane, int world, bool active,
+    float3 o, float3 d, float &tmax, bool &done, int &hit_inst, int &hit_tri, float &hu, float &hv, int skip,
+    int max_steps, int *err) {
+    const int root = s.instance_count > 0 ? __ldg(s.roots + world) : -1;
+    if (root < 0) return;
+    const float3 inv = safe_inverse(d);
+    // The instance whose leaf box the lane's ray entered: walked by that lane.
+    auto walk = [&](int id, bool enters) {
+        if (!enters || id == skip) return;
+        if (ANY) {
+            float tm = tmax, u, v;
+            int t;
+            done = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tm, true, t, u, v,
+                max_steps, err);
+        } else if (instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, false, hit_tri,
+                       hu, hv, max_steps, err)) {
+            hit_inst = id;
+        }
+    };
+    // An instance met on the stack: its leaf box first (leaf k of the sorted leaves is node n - 1 + k).
+    auto leaf_walk = [&](int id) {
+        const float4 *leaf = s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + __ldg(s.leaf_of + id));
+        walk(id, active && !done && box_entry(__ldg(leaf), __ldg(leaf + 1), o, inv, tmax) < NO_HIT);
+    };
+    if (root >= s.tlas_internal) {  // a world of one instance: its leaf is the root
+        leaf_walk(~__float_as_int(__ldg(s.tlas + 2 * root).w));
+        return;
+    }
+    {
+        const float4 lo = __ldg(s.tlas + 2 * root), hi = __ldg(s.tlas + 2 * root + 1);
+        if (!__any_sync(FULL, active && !done && box_entry(lo, hi, o, inv, tmax) < NO_HIT)) return;
+    }
+    const int max_nodes = 2 * s.instance_count + 2;
+    int ref = root, count = 0, sp = 0;
+    for (int steps = 0;; ++steps) {
+        if (steps > max_nodes) {  // a correct walk visits each node once; only a malformed tree gets here
+            if (lane == 0) *err = 2;
+            return;
+        }
+        bool pop = true;
+        if (count < 0) {
+            leaf_walk(ref);
+        } else {
+            const float4 *q = s.tlas_pairs + 4 * static_cast<long long>(ref);
+            const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+            const bool open = active && !done;
+            const float dl = open ? box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o,
+                inv, tmax) : NO_HIT;
+            const float dr = open ? box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), o,
+                inv, tmax) : NO_HIT;
+            const bool hl = __any_sync(FULL, dl < NO_HIT), hr = __any_sync(FULL, dr < NO_HIT);
+            if (hl || hr) {
+                const bool left_first = !hr || (hl && warp_min(dl) <= warp_min(dr));
+                const int near_ref = __float_as_int(left_first ? q3.x : q3.z);
+                const int near_count = __float_as_int(left_first ? q3.y : q3.w);
+                if (hl && hr) {
+                    if (sp >= TLAS_STACK) {
+                        if (lane == 0) *err = 1;
+                        return;
+                    }
+                    if (lane == 0) {
+                        sm.ref[sp] = __float_as_int(left_first ? q3.z : q3.x);
+                        sm.count[sp] = __float_as_int(left_first ? q3.w : q3.y);
+                    }
+                    ++sp;
+                }
+                if (near_count < 0) {
+                    walk(near_ref, (left_first ? dl : dr) < NO_HIT);
+                } else {
+                    ref = near_ref;
+                    count = near_count;
+                    pop = false;
+                }
+            }
+        }
+        if (pop) {
+            __syncwarp();
+            if (sp == 0) return;
+            --sp;
+            ref = sm.ref[sp];
+            count = sm.count[sp];
+            __syncwarp();
+        }
+    }
+}
+
 // Spheres and the floor before the meshes, the meshes with the closest of those as their limit
 // (scene_intersect, src/render_core.h:78-112).
 __device__ __forceinline__ float spheres_and_floor(const SceneParams &s, float3 o, float3 d, int &best_sphere,
@@ -222,9 +326,6 @@ __device__ __forceinline__ void put_rgb(uint8_t *rgb, long long pix, int bytes) 
     o[2] = static_cast<uint8_t>(bytes >> 16);
 }
 
-__device__ __forceinline__ float warp_max(float v) { return from_ordered(__reduce_max_sync(FULL, to_ordered(v))); }
-__device__ __forceinline__ float warp_min(float v) { return from_ordered(__reduce_min_sync(FULL, to_ordered(v))); }
-__device__ __forceinline__ float abs_dot(float3 n, float3 h) { return fabsf(n.x) * h.x + fabsf(n.y) * h.y + fabsf(n.z) * h.z; }
 
 // The tile kernels' common start: which tile of which view, and the pixel of this lane.
 struct TileAt {
@@ -329,6 +430,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             const float3 eye = mk3(c0.x, c0.y, c0.z), right = mk3(c0.w, c1.x, c1.y);
             const float3 up = mk3(c1.z, c1.w, c2.x), fwd = mk3(c2.y, c2.z, c2.w);
 
+            const float4 *leaves = world_leaves(s, T.world);
+            int ncand = 0;
+            if constexpr (CAP > 0) {
             // The tile's pyramid: the tangent-plane offsets of its pixel edges (every jittered and centre ray of
             // the tile lies inside), widened by 1e-3, and the four side planes through the eye, facing inwards.
             const float sxa = (2.0f * static_cast<float>(T.x0) / fw - 1.0f) * fs * asp;
@@ -341,7 +445,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             const float sy_hi = fmaxf(sya, syb) + 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
 
             // Every instance of the world against the pyramid, 32 at a time: the candidates, in leaf order.
-            const float4 *leaves = world_leaves(s, T.world);
             const float3 k00 = right * sx_lo + up * sy_lo + fwd, k10 = right * sx_hi + up * sy_lo + fwd;
             const float3 k11 = right * sx_hi + up * sy_hi + fwd, k01 = right * sx_lo + up * sy_hi + fwd;
             const float3 mid = k00 + k11;
@@ -350,7 +453,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             for (int e = 0; e < 4; ++e)
                 if (dot(planes[e], mid) < 0.0f) planes[e] = -planes[e];
             __syncwarp();
-            int ncand = 0;
             for (int base = 0; base < P; base += 32) {
                 const int j = base + lane;
                 bool cand = false;
@@ -396,6 +498,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                 sm.bound[rank] = bi;
             }
             __syncwarp();
+            }
 
             // The centre ray for depth, normals and IDs (aov_pixel, src/render_core.h:313-327), then the picture
             // ray (trace, src/render_core.h:202-245) up to its closest hit. Spheres and the floor first.
@@ -414,8 +517,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                 float tmax = spheres_and_floor(s, eye, d, best_sphere, hit_floor);
                 int hit_inst = -1, hit_tri = -1;
                 float hu = 0.0f, hv = 0.0f;
-                closest_meshes(s, sm, leaves, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps,
-                    a.error_flag);
+                if constexpr (CAP > 0) {
+                    closest_meshes(s, sm, leaves, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps,
+                        a.error_flag);
+                } else {
+                    bool unused = false;
+                    packet_walk<false>(s, sm, lane, T.world, T.pixel, eye, d, tmax, unused, hit_inst, hit_tri, hu, hv, -1,
+                        max_steps, a.error_flag);
+                }
                 if (!T.pixel) continue;
                 const size_t p = static_cast<size_t>(T.pix);
                 if (pass == 1) {
@@ -610,7 +719,8 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
 template <int THREADS, int MIN_BLOCKS, int CAP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
-    __shared__ int warp_cand[THREADS / 32][CAP];
+    __shared__ int warp_cand[THREADS / 32][CAP > 0 ? CAP : 1];
+    __shared__ WarpSmem<0> warp_stack[CAP > 0 ? 1 : THREADS / 32];
     int *cand_leaf = warp_cand[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -633,6 +743,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
             if (pending) d4 = a.shadow_d[T.pix];
             const float3 so = mk3(o4.x, o4.y, o4.z), sd = mk3(d4.x, d4.y, d4.z);
             const float sdist = o4.w;
+            int ncand = 0;
+            const float4 *leaves = world_leaves(s, T.world);
+            if constexpr (CAP > 0) {
             const float3 se = so + sd * sdist;
             const float mnx = warp_min(pending ? fminf(so.x, se.x) : INF);
             const float mny = warp_min(pending ? fminf(so.y, se.y) : INF);
@@ -666,10 +779,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                     support[k] = warp_max(pending ? fmaxf(dot(axis[k], so), dot(axis[k], se)) : -INF);
             }
             // Every instance of the world against the hull, 32 at a time: the candidates, in leaf order.
-            const float4 *leaves = world_leaves(s, T.world);
             const float light_scale = fabsf(lt.position.x) + fabsf(lt.position.y) + fabsf(lt.position.z) + lt.radius + 1.0f;
             __syncwarp();
-            int ncand = 0;
             for (int base = 0; base < P; base += 32) {
                 const int j = base + lane;
                 bool scand = false;
@@ -692,6 +803,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 ncand += __popc(cmask);
             }
             __syncwarp();
+            }
             // The ray's own mesh first when the shade kernel found it starts on that body's side, or not at all when
             // it cannot meet it; any hit ends the ray whatever the order, so the answer is the same.
             const int self_code = pending ? a.shadow_self[T.pix] : -1;
@@ -706,6 +818,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                     blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd, tm,
                         true, ht, hu, hv, max_steps, a.error_flag);
                 }
+            }
+            if constexpr (CAP == 0) {
+                int ht = -1, hi = -1;
+                float tm = sdist, hu = 0.0f, hv = 0.0f;
+                packet_walk<true>(s, warp_stack[threadIdx.x >> 5], lane, T.world, pending, so, sd, tm, blocked, hi, ht, hu,
+                    hv, self_code >= 0 ? self : -1, max_steps, a.error_flag);
             }
             for (int c = 0; c < ncand; ++c) {
                 const bool open = pending && !blocked;
@@ -788,9 +906,17 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
 
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade) {
-    if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) return cudaErrorInvalidValue;
     // (threads per CTA, register budget) -> the instantiation with that budget, and the candidate lists'
-    // capacity: 32 for worlds of up to 32 instances, else TILE_MAX_INSTANCES.
+    // capacity: 32 for worlds of up to 32 instances, else TILE_MAX_INSTANCES; larger worlds walk their tree
+    // as a packet (capacity 0).
+    if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) {
+        if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8, 0>(s, a, counter, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 56) return launch_variant<128, 9, 0>(s, a, counter, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10, 0>(s, a, counter, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6, 0>(s, a, counter, stream, after_camera, after_shade);
+        if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4, 0>(s, a, counter, stream, after_camera, after_shade);
+        return cudaErrorInvalidValue;
+    }
     const bool small = s.per_world <= 32;
     if (t.threads == 128 && t.registers == 64)
         return small ? launch_variant<128, 8, 32>(s, a, counter, stream, after_camera, after_shade)

@@ -552,3 +552,23 @@ def test_shadows_of_convex_concave_and_open_meshes(torch_cuda, light_y):
         r.set_tuning(kernel=kernel, threads_per_block=128, refill_lanes=8, registers=64)
         r.set_instance_transforms(mats)
         assert_same_images(r.render(cams, 1.0, 1, **ALL), want, ties=want["ties"] if kernel == 3 else None)
+
+
+@pytest.mark.parametrize("tuning", [(128, 56), (256, 64)])
+def test_tile_kernel_walks_large_worlds_as_packets(torch_cuda, tuning):
+    """Worlds above 256 instances on the tile kernels: the world tree walked by the warp as a packet for the
+    camera rays and the shadow rays, against the oracle (one world of 3000 boxes, global build; three worlds of
+    400 icospheres, per-world build)."""
+    desc, mats, cams = scenes.scattered_boxes(1, 3000)
+    cases = [(desc, mats, cams, scenes.FOV)]
+    wl = workloads.icosphere_worlds(worlds=3, per_world=400, width=48, height=40, seed=17)
+    cases.append((wl.desc, wl.matrices, wl.cameras, 1.0))
+    for d, m, c, fov in cases:
+        r, o = product(d), O.Oracle(d)
+        r.set_tuning(kernel=3, threads_per_block=tuning[0], registers=tuning[1])
+        r.set_instance_transforms(m)
+        o.set_instance_transforms(m)
+        want = o.render(c, fov, 1, **ALL, ties=True)
+        got = r.render(c, fov, 1, **ALL)
+        assert (got["object_ids"] >= 34).mean() > 0.1
+        assert_same_images(got, want, ties=want["ties"])
