@@ -87,8 +87,8 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
     if (box_entry(blo, bhi, o, inv, tmax) >= NO_HIT) return false;
     const int2 root = __ldg(slot_root + slot);
     int ref = root.x, count = root.y;
-    int st_ref[WALK_STACK], st_cnt[WALK_STACK];
-    float st_t[WALK_STACK];
+    // One 16-byte entry per pushed node: (reference, count, entry distance), stored and loaded whole.
+    int4 st[WALK_STACK];
     bool found = false;
     int sp = 0, steps = 0;
     // While-while: a lane walks internal nodes until it stands at a leaf (or its walk ends), and the leaf's
@@ -114,19 +114,23 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
                         *err = 1;
                         return found;
                     }
-                    st_ref[sp] = __float_as_int(left_first ? q3.z : q3.x);
-                    st_cnt[sp] = __float_as_int(left_first ? q3.w : q3.y);
-                    st_t[sp] = far_t;
+                    st[sp] = make_int4(__float_as_int(left_first ? q3.z : q3.x), __float_as_int(left_first ? q3.w : q3.y),
+                        __float_as_int(far_t), 0);
                     ++sp;
                 }
                 ref = __float_as_int(left_first ? q3.x : q3.z);
                 count = __float_as_int(left_first ? q3.y : q3.w);
             } else {
-                while (sp > 0 && st_t[sp - 1] >= tmax) --sp;
+                int4 e = make_int4(0, 0, 0, 0);
+                while (sp > 0) {
+                    e = st[sp - 1];
+                    if (__int_as_float(e.z) < tmax) break;
+                    --sp;
+                }
                 if (sp == 0) return found;
                 --sp;
-                ref = st_ref[sp];
-                count = st_cnt[sp];
+                ref = e.x;
+                count = e.y;
             }
         }
         if (++steps > max_steps) {
@@ -144,11 +148,16 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
                 found = true;
             }
         }
-        while (sp > 0 && st_t[sp - 1] >= tmax) --sp;
+        int4 e = make_int4(0, 0, 0, 0);
+        while (sp > 0) {
+            e = st[sp - 1];
+            if (__int_as_float(e.z) < tmax) break;
+            --sp;
+        }
         if (sp == 0) return found;
         --sp;
-        ref = st_ref[sp];
-        count = st_cnt[sp];
+        ref = e.x;
+        count = e.y;
     }
 }
 
