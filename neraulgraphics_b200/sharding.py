@@ -28,6 +28,18 @@ def world_range(world_count: int, rank: int, world_size: int) -> tuple[int, int]
     return start, start + base + (1 if rank < extra else 0)
 
 
+class _Group:
+    """The process group's rank and size (one rank when torch.distributed is not initialised)."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.group = group
+        if dist.is_available() and dist.is_initialized():
+            self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
+        else:
+            self.rank, self.size = 0, 1
+
+
 class ShardedWorlds:
     """This rank's share of world_count worlds in a torch.distributed process group (the default group when
     group is None; one rank when torch.distributed is not initialised)."""
@@ -84,3 +96,45 @@ class ShardedWorlds:
         t = torch.tensor([float(value)], dtype=torch.float64, device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
         return float(t.item())
+
+
+class ShardedRays(_Group):
+    """This rank's share of every world's rays: for one large world (or a few) whose ray queries outnumber its
+    worlds, such as a LiDAR sweep of one scene. Every rank holds the whole scene (the same instance matrices,
+    so the same tree) and casts a contiguous range of each world's rays; gather() puts the results back in
+    ray order. The ray queries are independent, so nothing is exchanged until the gather.
+
+        shard = ShardedRays(rays_per_world=131072)
+        hits = r.cast_rays(shard.take(origins), shard.take(directions), max_distance)
+        everything = {k: shard.gather(v) for k, v in hits.items()}      # (worlds, 131072, ...) on every rank
+    """
+
+    def __init__(self, rays_per_world: int, group=None):
+        super().__init__(group)
+        self.rays_per_world = rays_per_world
+        self.start, self.stop = world_range(rays_per_world, self.rank, self.size)
+        self.ranges = [world_range(rays_per_world, r, self.size) for r in range(self.size)]
+
+    @property
+    def count(self) -> int:
+        return self.stop - self.start
+
+    def take(self, per_ray):
+        """This rank's rays of an array or tensor shaped (worlds, rays_per_world, ...)."""
+        if per_ray.shape[1] != self.rays_per_world:
+            raise ValueError(f"expected {self.rays_per_world} rays per world on the second axis, got {per_ray.shape[1]}")
+        return per_ray[:, self.start:self.stop]
+
+    def gather(self, local):
+        """Every rank's (worlds, its rays, ...) tensor joined along the rays in ray order, on every rank: one
+        all-gather of pieces padded to the largest share."""
+        import torch
+        import torch.distributed as dist
+        if self.size == 1:
+            return local
+        pad = max(b - a for a, b in self.ranges)
+        piece = torch.zeros((local.shape[0], pad) + tuple(local.shape[2:]), dtype=local.dtype, device=local.device)
+        piece[:, :local.shape[1]] = local
+        pieces = [torch.empty_like(piece) for _ in range(self.size)]
+        dist.all_gather(pieces, piece, group=self.group)
+        return torch.cat([p[:, :b - a] for p, (a, b) in zip(pieces, self.ranges)], 1)

@@ -81,3 +81,57 @@ def test_two_ranks_render_their_worlds_and_gather_everything(tmp_path, worlds):
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     ok, slowest, start, stop = np.load(out)
     assert ok and slowest and (start, stop) == (0, (worlds + 1) // 2)
+
+
+def _ray_rank(rank, size, port, out):
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import torch
+    import torch.distributed as dist
+
+    import oracle as O
+    import scenes
+    from neraulgraphics_b200.sharding import ShardedRays
+    dist.init_process_group("gloo", rank=rank, world_size=size, timeout=datetime.timedelta(seconds=120))
+    try:
+        desc, mats, _ = scenes.scattered_boxes(1, 3000)
+        el = np.radians(np.linspace(-15.0, 15.0, 16))
+        az = np.radians(np.linspace(0.0, 360.0, 63, endpoint=False))
+        e, a = np.meshgrid(el, az, indexing="ij")
+        dirs = np.stack([np.cos(e) * np.sin(a), np.sin(e), -np.cos(e) * np.cos(a)], -1).reshape(1, -1, 3).astype(np.float32)
+        dirs = dirs[:, :1001]  # an odd count: shares of 501 and 500
+        origins = np.tile(np.float32([0.0, 0.0, -40.0]), (1, dirs.shape[1], 1))
+        o = O.Oracle(desc)
+        o.set_instance_transforms(mats)  # every rank: the whole scene, the same tree
+        shard = ShardedRays(dirs.shape[1])
+        hits = o.cast_rays(shard.take(origins), shard.take(dirs), 100.0)
+        got = {k: shard.gather(torch.from_numpy(np.ascontiguousarray(v))).numpy() for k, v in hits.items()}
+        if rank == 0:
+            want = o.cast_rays(origins, dirs, 100.0)
+            ok = all(np.array_equal(np.asarray(got[k]).view(np.uint8), np.asarray(want[k]).view(np.uint8)) for k in want)
+            hit = float((want["object_id"] > 0).mean())
+            np.save(out, np.array([ok, hit, shard.start, shard.stop], dtype=np.float64))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_split_one_worlds_rays():
+    """One world's 1001 ray queries split over two gloo ranks (501 + 500), each holding the whole scene, then
+    gathered in ray order: the same distances, normals and IDs as one rank casting them all."""
+    import tempfile
+
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with tempfile.TemporaryDirectory() as tmp:
+        port, out = _free_port(), os.path.join(tmp, "rank0.npy")
+        procs = [ctx.Process(target=_ray_rank, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=180)
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+        assert all(p.exitcode == 0 for p in procs)
+        ok, hit, start, stop = np.load(out)
+    assert ok == 1.0 and hit > 0.2 and (start, stop) == (0, 501)
