@@ -27,8 +27,6 @@
 namespace ngb {
 namespace {
 
-constexpr int THREADS = 256;
-constexpr int WARPS = THREADS / 32;
 constexpr int BINS = 16;
 constexpr int MAX_LEAF = 4;
 constexpr int MAX_DEPTH = 60;
@@ -130,6 +128,7 @@ __global__ void prepare_kernel(const MeshBuildArgs a, const MeshBuildScratch t) 
     t.order[i] = static_cast<uint32_t>(i);
 }
 
+template <int WARPS>
 struct SplitSmem {
     unsigned long long box_key[12];              // node box lo/hi (6), centroid box lo/hi (6)
     unsigned long long bin_key[3][BINS][6];      // per axis and bin: its box lo/hi
@@ -142,25 +141,34 @@ struct SplitSmem {
     int best_axis, best_bin, leaf, mid;
 };
 
-// Exclusive prefix count of flag over the CTA (thread order), and the CTA's total.
-__device__ __forceinline__ int cta_scan(SplitSmem &sm, bool flag, int &total) {
+// Exclusive prefix sum of v over the CTA's threads (in thread order, or from the last thread down when
+// reverse), and the CTA's total.
+template <int WARPS>
+__device__ __forceinline__ int cta_scan(SplitSmem<WARPS> &sm, int v, bool reverse, int &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned m = __ballot_sync(FULL, flag);
-    if (lane == 0) sm.warp_sum[warp] = __popc(m);
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = reverse ? __shfl_down_sync(FULL, incl, o) : __shfl_up_sync(FULL, incl, o);
+        if (reverse ? lane + o < 32 : lane >= o) incl += u;
+    }
+    if (reverse ? lane == 0 : lane == 31) sm.warp_sum[warp] = incl;
     __syncthreads();
     int before = 0;
     total = 0;
     for (int w = 0; w < WARPS; ++w) {
-        before += w < warp ? sm.warp_sum[w] : 0;
+        before += (reverse ? w > warp : w < warp) ? sm.warp_sum[w] : 0;
         total += sm.warp_sum[w];
     }
     __syncthreads();
-    return before + __popc(m & ((1u << lane) - 1u));
+    return before + incl - v;
 }
 
-// Splits every node of one depth (its range recorded by the depth before), one CTA per node.
+// Splits every node of one depth (its range recorded by the depth before), one CTA per node: 256 threads for
+// the upper depths' large nodes, one warp for the lower depths' small ones.
+template <int THREADS>
 __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int depth) {
-    __shared__ SplitSmem sm;
+    constexpr int WARPS = THREADS / 32;
+    __shared__ SplitSmem<WARPS> sm;
     const int tid = threadIdx.x, lane = tid & 31;
     const int2 level = t.range[depth];
     for (int x = level.x + blockIdx.x; x < level.y; x += gridDim.x) {
@@ -324,32 +332,28 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             auto passes = [&](int i) {
                 return bin_of(t.centre[3 * static_cast<size_t>(t.order[i]) + best_axis], lo, scale) <= best_bin;
             };
-            int passing = 0;
-            for (int base = begin; base < end; base += THREADS) {
-                int total;
-                const int i = base + tid;
-                cta_scan(sm, i < end && passes(i), total);
-                passing += total;
-            }
+            // Each thread takes a contiguous run of the range: it counts, the CTA scans the counts, and it
+            // writes its run's positions in order.
+            const int run = (count + THREADS - 1) / THREADS;
+            const int r0 = begin + tid * run < end ? begin + tid * run : end;
+            const int r1 = r0 + run < end ? r0 + run : end;
+            int mine = 0;
+            for (int i = r0; i < r1; ++i) mine += passes(i) ? 1 : 0;
+            int passing;
+            cta_scan(sm, mine, false, passing);
             const int meet = begin + passing;
-            int swaps = 0;
-            for (int base = begin; base < meet; base += THREADS) {
-                int total;
-                const int i = base + tid;
-                const bool fail = i < meet && !passes(i);
-                const int k = cta_scan(sm, fail, total);
-                if (fail) t.lpos[begin + swaps + k] = i;
-                swaps += total;
-            }
-            int found = 0;
-            for (int base = 0; meet + base < end; base += THREADS) {
-                int total;
-                const int j = end - 1 - (base + tid);
-                const bool pass = j >= meet && passes(j);
-                const int k = cta_scan(sm, pass, total);
-                if (pass) t.rpos[begin + found + k] = j;
-                found += total;
-            }
+            // Failing elements left of meet, ranked from the left; passing ones right of it, from the right.
+            const int l1 = r1 < meet ? r1 : meet, q0 = r0 > meet ? r0 : meet;
+            int fails = 0, passes_right = 0;
+            for (int i = r0; i < l1; ++i) fails += passes(i) ? 0 : 1;
+            for (int j = q0; j < r1; ++j) passes_right += passes(j) ? 1 : 0;
+            int swaps, found;
+            const int lbase = cta_scan(sm, fails, false, swaps);
+            const int rbase = cta_scan(sm, passes_right, true, found);
+            for (int i = r0, k = lbase; i < l1; ++i)
+                if (!passes(i)) t.lpos[begin + k++] = i;
+            for (int j = r1 - 1, k = rbase; j >= q0; --j)
+                if (passes(j)) t.rpos[begin + k++] = j;
             __syncthreads();
             for (int k = tid; k < swaps; k += THREADS) {
                 const int l = t.lpos[begin + k], r = t.rpos[begin + k];
@@ -510,9 +514,13 @@ cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &
 
 cudaError_t launch_mesh_level(const MeshBuildArgs &a, const MeshBuildScratch &t, int depth, cudaStream_t s) {
     // A depth holds at most 2^depth nodes, and the CTAs stride over whatever it holds.
-    const int most = depth < 12 ? 1 << depth : 4096;
+    const int most = depth < 16 ? 1 << depth : 65536;
     const int cap = a.triangles < most ? a.triangles : most;
-    split_kernel<<<cap > 0 ? cap : 1, THREADS, 0, s>>>(a, t, depth);
+    // A node at depth d holds about T / 2^d triangles: 256-thread CTAs while that is above a few hundred.
+    if ((static_cast<long long>(a.triangles) >> depth) > 512)
+        split_kernel<256><<<cap > 0 ? cap : 1, 256, 0, s>>>(a, t, depth);
+    else
+        split_kernel<32><<<cap > 0 ? cap : 1, 32, 0, s>>>(a, t, depth);
     advance_kernel<<<1, 1, 0, s>>>(t, depth);
     return cudaGetLastError();
 }
