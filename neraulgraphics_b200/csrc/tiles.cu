@@ -66,12 +66,15 @@ __device__ __forceinline__ const float4 *world_leaves(const SceneParams &s, int 
 // from its child-pair records: the nearer child first (dl <= dr), the farther one pushed with its entry
 // distance and dropped at pop time once a hit is closer (traverse, src/mesh_dev.h:113-159), and a leaf's
 // triangles in order (mesh_intersect / mesh_occluded, src/mesh_dev.h:180-226).
-// any: true at the first hit closer than tmax. Otherwise: lowers tmax to each closer hit and records it, true
-// if there was one. Not inlined, so that the picture, centre and shadow rays share one copy of the walk (the
-// instruction cache holds it once) and its stack lives in this function's own frame.
+// ANY (shadow rays): true at the first hit closer than tmax; tmax never shrinks, so a pushed node is never
+// dropped at pop time and its entry distance is not checked. Otherwise: lowers tmax to each closer hit and
+// records it, true if there was one. Not inlined, so that a kernel's rays share one copy of the walk (the
+// instruction cache holds it once: the camera kernel the closest-hit copy, the shadow kernel the any-hit one)
+// and its stack lives in this function's own frame.
+template <bool ANY>
 __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, const float *__restrict__ slot_bounds,
     const int2 *__restrict__ slot_root, const float4 *__restrict__ pairs, const float4 *__restrict__ tris, int id,
-    float3 o, float3 d, float &tmax, bool any, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
+    float3 o, float3 d, float &tmax, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
     const float4 *rec = inst + 4 * static_cast<long long>(id);
     InstanceRec r;
     r.r0 = __ldg(rec);
@@ -122,13 +125,18 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
                 count = __float_as_int(left_first ? q3.y : q3.w);
             } else {
                 int4 e = make_int4(0, 0, 0, 0);
-                while (sp > 0) {
-                    e = st[sp - 1];
-                    if (__int_as_float(e.z) < tmax) break;
+                if (ANY) {
+                    if (sp == 0) return false;
+                    e = st[--sp];
+                } else {
+                    while (sp > 0) {
+                        e = st[sp - 1];
+                        if (__int_as_float(e.z) < tmax) break;
+                        --sp;
+                    }
+                    if (sp == 0) return found;
                     --sp;
                 }
-                if (sp == 0) return found;
-                --sp;
                 ref = e.x;
                 count = e.y;
             }
@@ -140,7 +148,7 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
         for (int j = ref; j < ref + count; ++j) {
             float t, bu, bv;
             if (triangle_hit(tris, j, o, d, tmax, t, bu, bv)) {
-                if (any) return true;
+                if (ANY) return true;
                 tmax = t;
                 hit_tri = j;
                 hu = bu;
@@ -149,13 +157,18 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
             }
         }
         int4 e = make_int4(0, 0, 0, 0);
-        while (sp > 0) {
-            e = st[sp - 1];
-            if (__int_as_float(e.z) < tmax) break;
+        if (ANY) {
+            if (sp == 0) return false;
+            e = st[--sp];
+        } else {
+            while (sp > 0) {
+                e = st[sp - 1];
+                if (__int_as_float(e.z) < tmax) break;
+                --sp;
+            }
+            if (sp == 0) return found;
             --sp;
         }
-        if (sp == 0) return found;
-        --sp;
         ref = e.x;
         count = e.y;
     }
@@ -175,7 +188,7 @@ __device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpS
         const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
         if (reach && box_entry(lo, hi, o, inv, tmax) < NO_HIT) {
             const int id = ~__float_as_int(lo.w);
-            if (instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, false, hit_tri,
+            if (instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, hit_tri,
                     hu, hv, max_steps, err))
                 hit_inst = id;
         }
@@ -199,14 +212,15 @@ __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &s
     // The instance whose leaf box the lane's ray entered: walked by that lane.
     auto walk = [&](int id, bool enters) {
         if (!enters || id == skip) return;
-        if (ANY) {
+        if constexpr (ANY) {
             float tm = tmax, u, v;
             int t;
-            done = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tm, true, t, u, v,
+            done = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tm, t, u, v,
                 max_steps, err);
-        } else if (instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, false, hit_tri,
-                       hu, hv, max_steps, err)) {
-            hit_inst = id;
+        } else {
+            if (instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, hit_tri,
+                    hu, hv, max_steps, err))
+                hit_inst = id;
         }
     };
     // An instance met on the stack: its leaf box first (leaf k of the sorted leaves is node n - 1 + k).
@@ -824,8 +838,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 if (box_entry(__ldg(leaf), __ldg(leaf + 1), so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd, tm,
-                        true, ht, hu, hv, max_steps, a.error_flag);
+                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd,
+                        tm, ht, hu, hv, max_steps, a.error_flag);
                 }
             }
             if constexpr (CAP == 0) {
@@ -843,8 +857,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 if (open && id != self && box_entry(lo, hi, so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, so, sd, tm,
-                        true, ht, hu, hv, max_steps, a.error_flag);
+                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, so, sd, tm,
+                        ht, hu, hv, max_steps, a.error_flag);
                 }
             }
             if (pending) put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));
