@@ -500,6 +500,9 @@ class UnevenBatchRenderer(BatchRenderer):
     def bind_bodies(self, *args, **kwargs):
         raise ValueError("worlds of uneven sizes take instance matrices (set_instance_transforms), not body poses")
 
+    def bind_geoms(self, *args, **kwargs):
+        raise ValueError("worlds of uneven sizes take instance matrices (set_instance_transforms), not geom poses")
+
     def render(self, cameras, fov=1.0, samples_per_pixel=1, *, rgb=True, depth=False, normals=False,
                object_ids=False, frame=0, zero_copy=False):
         torch = _torch()

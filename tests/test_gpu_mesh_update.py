@@ -154,3 +154,23 @@ def test_update_arguments_are_checked(torch_cuda):
         r.update_mesh(2, bad)
     with pytest.raises(ValueError, match="made without vertex normals"):
         r.update_mesh(0, ms[0].vertices, ms[0].vertices)
+
+
+def test_uneven_worlds_follow_a_mesh_update(torch_cuda):
+    """Worlds of uneven sizes: a moved mesh in every world that uses it (slot tables per instance), against a
+    plain renderer of each world made with the moved mesh, bit for bit."""
+    import test_gpu_parity as P
+    worlds, meshes, floor, lights, mats, cams = P.uneven_scene()
+    u = ng.UnevenBatchRenderer(worlds, lights=lights, floor=floor, meshes=meshes, device="cuda:0")
+    u.set_instance_transforms(mats)
+    new = list(meshes)
+    new[1] = S.Mesh(moved(meshes[1], 12, scale=0.02) * np.float32(1.3), meshes[1].triangles)
+    u.update_mesh(1, new[1].vertices)
+    got = u.render(cams, 1.0, 1, **ALL)
+    first = u.instance_first
+    for w, (width, height, insts) in enumerate(worlds):
+        plain = ng.BatchRenderer(width, height, 1, 1, [], lights, floor, new, insts, device="cuda:0")
+        if insts:
+            plain.set_instance_transforms(mats[first[w]:first[w + 1]].reshape(1, len(insts), 3, 4))
+        mine = {k: u.image(v, w)[None] for k, v in got.items()}
+        P.assert_same_images(mine, plain.render(cams[w:w + 1], 1.0, 1, **ALL), rgb_tol=0)
