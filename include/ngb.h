@@ -389,6 +389,12 @@ int ngb_inspect_tlas(ngb_renderer *r, uint64_t *keys, int32_t *sorted_ids, int32
  * ngb_inspect_hits). Off by default: it writes 16 more bytes per pixel. */
 int ngb_record_hits(ngb_renderer *r, int32_t on);
 
+/* Like ngb_record_hits(r, 1), but later renders write the hit records into the caller's device arrays (each
+ * view_count x height x width: instance, triangle, u, v; all four given) instead of the renderer's own, saving
+ * ngb_copy_hits' copy; ngb_record_hits (either value) goes back to the renderer's own. The arrays must stay
+ * valid while renders may write them. No counterpart in the reference. */
+int ngb_record_hits_into(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *u, float *v);
+
 /* Per pixel of the last render's centre (depth/normal/ID) rays: the instance hit (over all worlds, -1
  * for none), the triangle hit (its index in its mesh's own list, -1 for none) and the barycentrics u, v.
  * Host arrays of view_count * height * width; any may be NULL. Filled by renders made with

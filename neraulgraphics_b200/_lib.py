@@ -48,6 +48,7 @@ def lib():
     L.ngb_bind_geoms.argtypes = [_vp, C.c_int32, _i32p, _f32p]
     L.ngb_set_geom_poses.argtypes = [_vp, _vp, _vp, C.c_int32]
     L.ngb_update_mesh.argtypes = [_vp, C.c_int32, _vp, _vp, C.c_int32]
+    L.ngb_record_hits_into.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.ngb_inspect_mesh.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_render.argtypes = [_vp, _vp, C.c_float, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                              C.POINTER(_abi.BatchFrameC)]

@@ -27,16 +27,20 @@ class _DepthNormals(torch.autograd.Function):
         m = matrices.detach().contiguous()
         c = cameras.detach().contiguous()
         renderer.set_instance_transforms(m)
-        renderer.record_hits(True)
         views, h, w = renderer.view_count, renderer.height, renderer.width
         depth = torch.empty((views, h, w), dtype=torch.float32, device=m.device)
         normals = torch.empty((views, h, w, 3), dtype=torch.float32, device=m.device)
-        renderer.render(c, fov, 1, rgb=False, depth=True, normals=True, into={"depth": depth, "normals": normals})
         hits = (torch.empty(depth.shape, dtype=torch.int32, device=depth.device),
                 torch.empty(depth.shape, dtype=torch.int32, device=depth.device),
                 torch.empty(depth.shape, dtype=torch.float32, device=depth.device),
                 torch.empty(depth.shape, dtype=torch.float32, device=depth.device))
-        renderer.copy_hits(*hits)
+        # The render writes the hit records straight into the tensors saved for the backward; the renderer goes
+        # back to not recording once the render is queued.
+        renderer.record_hits(True, into=hits)
+        try:
+            renderer.render(c, fov, 1, rgb=False, depth=True, normals=True, into={"depth": depth, "normals": normals})
+        finally:
+            renderer.record_hits(False)
         ctx.renderer = renderer
         ctx.fov = float(fov)
         ctx.save_for_backward(m, c, depth, *hits)

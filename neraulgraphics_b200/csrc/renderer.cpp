@@ -160,6 +160,14 @@ struct Renderer {
     bool record_hits = false;
     DevBuf<int32_t> hit_instance, hit_triangle;
     DevBuf<float> hit_u, hit_v;
+    // The caller's hit arrays (ngb_record_hits_into), written instead of the renderer's own while set.
+    int32_t *ext_instance = nullptr, *ext_triangle = nullptr;
+    float *ext_u = nullptr, *ext_v = nullptr;
+    // The arrays the last render's hits went to (the caller's or the renderer's own).
+    const int32_t *hits_instance() const { return ext_instance ? ext_instance : hit_instance.p; }
+    const int32_t *hits_triangle() const { return ext_instance ? ext_triangle : hit_triangle.p; }
+    const float *hits_u() const { return ext_instance ? ext_u : hit_u.p; }
+    const float *hits_v() const { return ext_instance ? ext_v : hit_v.p; }
     DevBuf<int> error_flag;
     int *host_error = nullptr;  // pinned: the device error flag, copied back where the host waits for the work
 
@@ -857,10 +865,17 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     a.normal = (outputs & NGB_OUTPUT_NORMAL) ? normal : nullptr;
     a.object_id = (outputs & NGB_OUTPUT_OBJECT_ID) ? ids : nullptr;
     if (record_hits && (outputs & (NGB_OUTPUT_DEPTH | NGB_OUTPUT_NORMAL | NGB_OUTPUT_OBJECT_ID))) {
-        a.hit_instance = hit_instance.ensure(pixels());
-        a.hit_triangle = hit_triangle.ensure(pixels());
-        a.hit_u = hit_u.ensure(pixels());
-        a.hit_v = hit_v.ensure(pixels());
+        if (ext_instance) {
+            a.hit_instance = ext_instance;
+            a.hit_triangle = ext_triangle;
+            a.hit_u = ext_u;
+            a.hit_v = ext_v;
+        } else {
+            a.hit_instance = hit_instance.ensure(pixels());
+            a.hit_triangle = hit_triangle.ensure(pixels());
+            a.hit_u = hit_u.ensure(pixels());
+            a.hit_v = hit_v.ensure(pixels());
+        }
     }
     a.error_flag = error_flag.p;
     // The persistent and tile kernels cover one sample per pixel, at most one light and no bounces; everything
@@ -1334,7 +1349,22 @@ int ngb_srgb_thresholds(float *thresholds) {
 }
 
 int ngb_record_hits(ngb_renderer *h, int32_t on) {
-    return guarded(h, [&](ngb::Renderer &r) { r.record_hits = on != 0; });
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.record_hits = on != 0;
+        r.ext_instance = r.ext_triangle = nullptr;
+        r.ext_u = r.ext_v = nullptr;
+    });
+}
+
+int ngb_record_hits_into(ngb_renderer *h, int32_t *instance, int32_t *triangle, float *u, float *v) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(instance && triangle && u && v, "instance, triangle, u and v must all be given");
+        r.record_hits = true;
+        r.ext_instance = instance;
+        r.ext_triangle = triangle;
+        r.ext_u = u;
+        r.ext_v = v;
+    });
 }
 
 int ngb_inspect_tlas(ngb_renderer *h, uint64_t *keys, int32_t *sorted_ids, int32_t *nodes, int32_t *roots,
@@ -1354,12 +1384,12 @@ int ngb_inspect_tlas(ngb_renderer *h, uint64_t *keys, int32_t *sorted_ids, int32
 
 int ngb_copy_hits(ngb_renderer *h, int32_t *instance, int32_t *triangle, float *u, float *v) {
     return guarded(h, [&](ngb::Renderer &r) {
-        ngb::require(r.hit_instance.p != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
+        ngb::require(r.hits_instance() != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
         const size_t px = r.pixels() * 4;
-        if (instance) CK(cudaMemcpyAsync(instance, r.hit_instance.p, px, cudaMemcpyDeviceToDevice, r.stream));
-        if (triangle) CK(cudaMemcpyAsync(triangle, r.hit_triangle.p, px, cudaMemcpyDeviceToDevice, r.stream));
-        if (u) CK(cudaMemcpyAsync(u, r.hit_u.p, px, cudaMemcpyDeviceToDevice, r.stream));
-        if (v) CK(cudaMemcpyAsync(v, r.hit_v.p, px, cudaMemcpyDeviceToDevice, r.stream));
+        if (instance) CK(cudaMemcpyAsync(instance, r.hits_instance(), px, cudaMemcpyDeviceToDevice, r.stream));
+        if (triangle) CK(cudaMemcpyAsync(triangle, r.hits_triangle(), px, cudaMemcpyDeviceToDevice, r.stream));
+        if (u) CK(cudaMemcpyAsync(u, r.hits_u(), px, cudaMemcpyDeviceToDevice, r.stream));
+        if (v) CK(cudaMemcpyAsync(v, r.hits_v(), px, cudaMemcpyDeviceToDevice, r.stream));
         r.finish();
     });
 }
@@ -1403,14 +1433,14 @@ int ngb_depth_normal_adjoint(ngb_renderer *h, const float *matrices, const float
 
 int ngb_inspect_hits(ngb_renderer *h, int32_t *instance, int32_t *triangle, float *u, float *v) {
     return guarded(h, [&](ngb::Renderer &r) {
-        ngb::require(r.hit_instance.p != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
+        ngb::require(r.hits_instance() != nullptr, "no hit records: call ngb_record_hits(r, 1) before rendering");
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, r.timeout);
         const size_t px = r.pixels();
-        if (instance) CK(cudaMemcpy(instance, r.hit_instance.p, px * 4, cudaMemcpyDeviceToHost));
-        if (triangle) CK(cudaMemcpy(triangle, r.hit_triangle.p, px * 4, cudaMemcpyDeviceToHost));
-        if (u) CK(cudaMemcpy(u, r.hit_u.p, px * 4, cudaMemcpyDeviceToHost));
-        if (v) CK(cudaMemcpy(v, r.hit_v.p, px * 4, cudaMemcpyDeviceToHost));
+        if (instance) CK(cudaMemcpy(instance, r.hits_instance(), px * 4, cudaMemcpyDeviceToHost));
+        if (triangle) CK(cudaMemcpy(triangle, r.hits_triangle(), px * 4, cudaMemcpyDeviceToHost));
+        if (u) CK(cudaMemcpy(u, r.hits_u(), px * 4, cudaMemcpyDeviceToHost));
+        if (v) CK(cudaMemcpy(v, r.hits_v(), px * 4, cudaMemcpyDeviceToHost));
     });
 }
 

@@ -407,8 +407,22 @@ class BatchRenderer:
         1 per-world, 2 global. Both make the same tree."""
         check(self._lib.ngb_set_build(self._h, int(mode)), self._h)
 
-    def record_hits(self, on=True):
-        check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
+    def record_hits(self, on=True, into=None):
+        """Later renders that ask for depth, normals or IDs also record each centre ray's hit. into: the
+        caller's CUDA tensors (instance int32, triangle int32, u float32, v float32; each (views, H, W),
+        contiguous) to write them to instead of the renderer's own buffers (no copy_hits needed); they must
+        stay alive while renders may write them, until the next record_hits call."""
+        if into is None:
+            check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
+            return
+        torch = _torch()
+        shape = (self.view_count, self.height, self.width)
+        for t, dt in zip(into, (torch.int32, torch.int32, torch.float32, torch.float32)):
+            if (not _is_cuda_tensor(t) or tuple(t.shape) != shape or t.dtype != dt or not t.is_contiguous() or
+                    t.device.index != self._device):
+                raise ValueError(f"record_hits(into=...) takes four contiguous CUDA tensors of shape {shape}: "
+                                 "instance and triangle int32, u and v float32")
+        check(self._lib.ngb_record_hits_into(self._h, *[C.c_void_p(t.data_ptr()) for t in into]), self._h)
 
     def inspect_tlas(self) -> dict:
         """The last tree build: keys (instance order), sorted ids, nodes (8 words), roots, matrices."""

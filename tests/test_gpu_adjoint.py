@@ -121,9 +121,12 @@ def test_adjoint_is_the_float64_reference(torch_cuda):
     finite = torch.isfinite(depth)
     loss = (torch.where(finite, depth, 0.0) * gd).sum() + (normals * gn).sum()
     loss.backward()
-    # The same pixels and triangles in float64.
+    # The same pixels and triangles in float64: the forward's hits, recorded again by the same render.
     hits = [torch.empty(depth.shape, dtype=dt, device="cuda") for dt in (torch.int32, torch.int32, torch.float32, torch.float32)]
+    r.record_hits(True)
+    r.render(cams.detach(), wl.fov, 1, rgb=False, depth=True, normals=True, zero_copy=True)
     r.copy_hits(*hits)
+    r.record_hits(False)
     m64 = torch.from_numpy(wl.matrices).cuda().double().requires_grad_()
     c64 = torch.from_numpy(wl.cameras).cuda().double().requires_grad_()
     d64, n64 = reference_depth_normals(torch, wl, m64, c64, hits, depth.detach(), wl.fov)
