@@ -372,6 +372,16 @@ int ngb_copy_hits(ngb_renderer *r, int32_t *instance, int32_t *triangle, float *
  * with hit records on) moves with its instance, and the camera rays move with the cameras. matrices, cameras,
  * fov and depth must be those of that render. Every pointer is device memory. No counterpart in the
  * reference, which has no derivatives. */
+/* Instance matrices [R(q) diag(s) | p] (12 floats each, q normalised first) of count poses: positions (3
+ * floats), quaternions (x, y, z, w) and scales (3 floats, or NULL for 1), all in device memory, queued on
+ * `stream` (a cudaStream_t). The matrices of ngb_depth_normal_adjoint's gradient go back to the poses through
+ * ngb_pose_matrices_grad: d(loss)/d(positions, quaternions, scales) from d(loss)/d(matrices) (grad_scales may be
+ * NULL). No counterpart in the reference; errors: ngb_last_error(NULL). */
+int ngb_pose_matrices(const float *positions, const float *quaternions, const float *scales, int64_t count,
+    float *matrices, void *stream);
+int ngb_pose_matrices_grad(const float *quaternions, const float *scales, int64_t count, const float *grad_matrices,
+    float *grad_positions, float *grad_quaternions, float *grad_scales, void *stream);
+
 int ngb_depth_normal_adjoint(ngb_renderer *r, const float *matrices, const float *cameras, float fov,
     const int32_t *hit_instance, const int32_t *hit_triangle, const float *hit_u, const float *hit_v, const float *depth,
     const float *grad_depth, const float *grad_normal, float *grad_matrices, float *grad_cameras);

@@ -49,6 +49,8 @@ def lib():
     L.ngb_set_geom_poses.argtypes = [_vp, _vp, _vp, C.c_int32]
     L.ngb_update_mesh.argtypes = [_vp, C.c_int32, _vp, _vp, C.c_int32]
     L.ngb_record_hits_into.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.ngb_pose_matrices.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
+    L.ngb_pose_matrices_grad.argtypes = [_vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]
     L.ngb_inspect_mesh.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_render.argtypes = [_vp, _vp, C.c_float, C.c_int32, C.c_uint32, C.c_int32, C.c_int32,
                              C.POINTER(_abi.BatchFrameC)]

@@ -62,6 +62,43 @@ def render_depth_normals(renderer, matrices, cameras, fov=1.0):
     return _DepthNormals.apply(renderer, matrices, cameras, fov)
 
 
+class _PoseMatrices(torch.autograd.Function):
+    """pose_matrices on float32 CUDA tensors of one shape: one kernel each way (ngb_pose_matrices and
+    ngb_pose_matrices_grad) instead of the dozens of small element-wise kernels of the PyTorch form."""
+
+    @staticmethod
+    def forward(ctx, positions, quaternions, scales):
+        import ctypes as C
+        from ._lib import check, lib
+        L = lib()
+        out = torch.empty(positions.shape[:-1] + (3, 4), dtype=torch.float32, device=positions.device)
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        with torch.cuda.device(positions.device):
+            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            check(L.ngb_pose_matrices(ptr(positions), ptr(quaternions), ptr(scales), out.numel() // 12, ptr(out), stream))
+        ctx.save_for_backward(quaternions, scales)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        import ctypes as C
+        from ._lib import check, lib
+        L = lib()
+        quaternions, scales = ctx.saved_tensors
+        grad = grad.contiguous()
+        lead = quaternions.shape[:-1]
+        gp = torch.empty(lead + (3,), dtype=torch.float32, device=grad.device)
+        gq = torch.empty(lead + (4,), dtype=torch.float32, device=grad.device)
+        gs = torch.empty(lead + (3,), dtype=torch.float32, device=grad.device) if (
+            scales is not None and ctx.needs_input_grad[2]) else None
+        ptr = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        with torch.cuda.device(grad.device):
+            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            check(L.ngb_pose_matrices_grad(ptr(quaternions), ptr(scales), grad.numel() // 12, ptr(grad), ptr(gp), ptr(gq),
+                                           ptr(gs), stream))
+        return gp, gq, gs
+
+
 def quaternion_matrix(q):
     """Rotation matrices (..., 3, 3) of quaternions (..., 4) stored (x, y, z, w), normalised first."""
     q = q / torch.linalg.norm(q, dim=-1, keepdim=True)
@@ -72,7 +109,16 @@ def quaternion_matrix(q):
 
 
 def pose_matrices(positions, quaternions, scales=None):
-    """3 x 4 matrices [R(q) diag(s) | p] of positions (..., 3), quaternions (..., 4) and scales (..., 3)."""
+    """3 x 4 matrices [R(q) diag(s) | p] of positions (..., 3), quaternions (..., 4) and scales (..., 3).
+    Float32 CUDA tensors take the fused kernels (broadcast to one leading shape first); other tensors (CPU,
+    float64 references) the PyTorch form below."""
+    tensors = [t for t in (positions, quaternions, scales) if t is not None]
+    if all(t.is_cuda and t.dtype == torch.float32 for t in tensors):
+        lead = torch.broadcast_shapes(*[t.shape[:-1] for t in tensors])
+        p = positions.expand(lead + (3,)).contiguous()
+        q = quaternions.expand(lead + (4,)).contiguous()
+        s = None if scales is None else scales.expand(lead + (3,)).contiguous()
+        return _PoseMatrices.apply(p, q, s)
     r = quaternion_matrix(quaternions)
     if scales is not None:
         r = r * scales.unsqueeze(-2)

@@ -21,7 +21,7 @@ OBJ = os.path.join(HERE, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
               "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = ["lbvh.cu", "trace.cu", "persistent.cu", "tiles.cu", "adjoint.cu", "noalloc.cu", "blas_build.cu", "host.cpp", "renderer.cpp"]
+SOURCES = ["lbvh.cu", "trace.cu", "persistent.cu", "tiles.cu", "adjoint.cu", "noalloc.cu", "blas_build.cu", "pose.cu", "host.cpp", "renderer.cpp"]
 
 
 def nvcc() -> str:
