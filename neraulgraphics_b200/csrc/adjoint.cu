@@ -80,9 +80,26 @@ __device__ __forceinline__ void camera_adjoint(float *gcam, float3 gdir, float3 
 }
 
 // The sum of v over the warp (every lane takes part), in every lane.
-__device__ __forceinline__ float warp_sum(float v) {
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    return v;
+// Twelve sums over the warp at once (recursive halving): each exchange sends half of the values a lane still
+// carries and keeps the other half, so 12 sums (padded to 16) take 8 + 4 + 2 + 1 + 1 shuffles instead of 12 x 5.
+// Lane l ends with the total of entry l >> 1 (entries 12 to 15 are padding).
+__device__ __forceinline__ float warp_sums12(const float *in, int lane) {
+    float v[8];
+    const bool b16 = lane & 16;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float lo = in[k], hi = k + 8 < 12 ? in[k + 8] : 0.0f;
+        v[k] = (b16 ? hi : lo) + __shfl_xor_sync(0xffffffffu, b16 ? lo : hi, 16);
+    }
+    const bool b8 = lane & 8;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = (b8 ? v[k + 4] : v[k]) + __shfl_xor_sync(0xffffffffu, b8 ? v[k] : v[k + 4], 8);
+    const bool b4 = lane & 4;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) v[k] = (b4 ? v[k + 2] : v[k]) + __shfl_xor_sync(0xffffffffu, b4 ? v[k] : v[k + 2], 4);
+    const bool b2 = lane & 2;
+    v[0] = (b2 ? v[1] : v[0]) + __shfl_xor_sync(0xffffffffu, b2 ? v[0] : v[1], 2);
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 __global__ void __launch_bounds__(ADJ_THREADS, 4) depth_normal_adjoint_kernel(const __grid_constant__ SceneParams s,
@@ -223,19 +240,21 @@ __global__ void __launch_bounds__(ADJ_THREADS, 4) depth_normal_adjoint_kernel(co
     // Sums over the warp before any atomic: the camera's in one tree (a warp's pixels share the view), the
     // instances' one distinct instance at a time (a tile's warp sees few of them).
     const int lane = threadIdx.x & 31;
-    for (int e = 0; e < 12; ++e) {
-        const float v = warp_sum(gcam[e]);
-        if (lane == 0 && v != 0.0f) atomicAdd(cam_sum + e, v);
+    const int entry = lane >> 1;  // the sum this lane holds after warp_sums12
+    const bool adds = (lane & 1) == 0 && entry < 12;
+    {
+        const float v = warp_sums12(gcam, lane);
+        if (adds && v != 0.0f) atomicAdd(cam_sum + entry, v);
     }
     for (unsigned pending = __ballot_sync(0xffffffffu, owner >= 0); pending != 0;) {
         const int inst_k = __shfl_sync(0xffffffffu, owner, __ffs(pending) - 1);
         const bool mine = owner == inst_k;
         pending &= ~__ballot_sync(0xffffffffu, mine);
         float *dst = shared_sums ? sums + 12 * (inst_k - world * P) : a.grad_matrices + 12LL * inst_k;
-        for (int e = 0; e < 12; ++e) {
-            const float v = warp_sum(mine ? ginst[e] : 0.0f);
-            if (lane == 0 && v != 0.0f) atomicAdd(dst + e, v);
-        }
+        float part[12];
+        for (int e = 0; e < 12; ++e) part[e] = mine ? ginst[e] : 0.0f;
+        const float v = warp_sums12(part, lane);
+        if (adds && v != 0.0f) atomicAdd(dst + entry, v);
     }
     __syncthreads();
     if (shared_sums)
