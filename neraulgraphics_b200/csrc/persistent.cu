@@ -114,16 +114,20 @@ __device__ __forceinline__ void start_walk(const SceneParams &s, Lane &L) {
 
 // The walk's pop (traverse's dead end, src/mesh_dev.h:154-157): resume from the stack, dropping what a closer
 // hit has put out of reach; a marker hands the walk back to the world's tree.
-__device__ __forceinline__ void walk_pop(Lane &L, const ColdRef &cold, const int *st_ref, const int *st_cnt,
-    const float *st_t) {
+__device__ __forceinline__ void walk_pop(Lane &L, const ColdRef &cold, const int4 *st) {
     for (;;) {
-        while (L.sp > 0 && st_t[L.sp - 1] >= L.tmax) --L.sp;
+        int4 e = make_int4(0, 0, 0, 0);
+        while (L.sp > 0) {
+            e = st[L.sp - 1];
+            if (__int_as_float(e.z) < L.tmax) break;
+            --L.sp;
+        }
         if (L.sp == 0) {
             L.state = ST_DONE;
             return;
         }
         --L.sp;
-        const int c = st_cnt[L.sp];
+        const int c = e.y;
         if (c == MARKER) {
             L.o = cold.get3(C_WO);
             L.d = cold.get3(C_WD);
@@ -131,7 +135,7 @@ __device__ __forceinline__ void walk_pop(Lane &L, const ColdRef &cold, const int
             L.in_blas = false;
             continue;
         }
-        L.ref = st_ref[L.sp];
+        L.ref = e.x;
         L.count = c;
         return;
     }
@@ -139,8 +143,7 @@ __device__ __forceinline__ void walk_pop(Lane &L, const ColdRef &cold, const int
 
 // A walk step at an internal node of either tree: both children's boxes, the nearer one next, the farther one
 // pushed with its entry distance (traverse, src/mesh_dev.h:133-151).
-__device__ __forceinline__ void walk_inner(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
-    float *st_t, int *err) {
+__device__ __forceinline__ void walk_inner(const SceneParams &s, Lane &L, const ColdRef &cold, int4 *st, int *err) {
     const float4 *rec = (L.in_blas ? s.blas_pairs : s.tlas_pairs) + 4 * static_cast<long long>(L.ref);
     const float4 q0 = __ldg(rec), q1 = __ldg(rec + 1), q2 = __ldg(rec + 2), q3 = __ldg(rec + 3);
     const float dl = box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), L.o, L.inv, L.tmax);
@@ -154,23 +157,21 @@ __device__ __forceinline__ void walk_inner(const SceneParams &s, Lane &L, const 
                 L.state = ST_DONE;
                 return;
             }
-            st_ref[L.sp] = __float_as_int(left_first ? q3.z : q3.x);
-            st_cnt[L.sp] = __float_as_int(left_first ? q3.w : q3.y);
-            st_t[L.sp] = far_t;
+            st[L.sp] = make_int4(__float_as_int(left_first ? q3.z : q3.x), __float_as_int(left_first ? q3.w : q3.y),
+                __float_as_int(far_t), 0);
             ++L.sp;
         }
         L.ref = __float_as_int(left_first ? q3.x : q3.z);
         L.count = __float_as_int(left_first ? q3.y : q3.w);
         return;
     }
-    walk_pop(L, cold, st_ref, st_cnt, st_t);
+    walk_pop(L, cold, st);
 }
 
 // A walk step at a leaf: an instance (into its mesh's space, and its mesh root's box test: blas_walk's first
 // line) or one triangle of a mesh leaf, in the leaf's order (mesh_intersect / mesh_occluded's leaves,
 // src/mesh_dev.h:180-226).
-__device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const ColdRef &cold, int *st_ref, int *st_cnt,
-    float *st_t, int *err) {
+__device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const ColdRef &cold, int4 *st, int *err) {
     if (L.count < 0) {
         const InstanceRec r = load_instance(s.inst, L.ref);
         const int slot = __float_as_int(__ldg(s.inst + 4 * L.ref + 3).y);
@@ -186,9 +187,7 @@ __device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const C
                 L.state = ST_DONE;
                 return;
             }
-            st_ref[L.sp] = MARKER;
-            st_cnt[L.sp] = MARKER;
-            st_t[L.sp] = -INFINITY;  // never dropped by the tmax test
+            st[L.sp] = make_int4(MARKER, MARKER, __float_as_int(-INFINITY), 0);  // never dropped by the tmax test
             ++L.sp;
             const int2 root = __ldg(s.slot_root + slot);
             // The world-space ray waits in shared memory while the walk is in mesh space.
@@ -225,7 +224,7 @@ __device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const C
             return;
         }
     }
-    walk_pop(L, cold, st_ref, st_cnt, st_t);
+    walk_pop(L, cold, st);
 }
 
 // A new job from its item number. Items run over views, then 4 x 4 pixel tiles, then the pixels of a tile,
@@ -471,8 +470,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
     const RenderArgs a, const RayArgs ra, int *counter, long long total, int kinds, int tiles_x, int tiles_per_view,
     int refill, int leaf_batch) {
     extern __shared__ float cold_smem[];
-    int st_ref[STACK], st_cnt[STACK];
-    float st_t[STACK];
+    int4 st[STACK];  // (reference, count, entry distance) per pushed node, stored and loaded whole
     const int lane = threadIdx.x & 31;
     const unsigned lanes_below = (1u << lane) - 1u;
     const ColdRef cold{cold_smem + threadIdx.x, THREADS};
@@ -520,9 +518,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
                     *(kinds == KINDS_RAYS ? ra.error_flag : a.error_flag) = 2;
                     L.state = ST_DONE;
                 } else if (leaf_phase) {
-                    walk_leaf(s, L, cold, st_ref, st_cnt, st_t, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
+                    walk_leaf(s, L, cold, st, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
                 } else {
-                    walk_inner(s, L, cold, st_ref, st_cnt, st_t, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
+                    walk_inner(s, L, cold, st, kinds == KINDS_RAYS ? ra.error_flag : a.error_flag);
                 }
             }
         }
