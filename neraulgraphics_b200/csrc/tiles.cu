@@ -195,38 +195,27 @@ __device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpS
     }
 }
 
-// A world's tree walked by the whole warp together (a packet), for worlds too large for candidate lists:
-// every internal node that some lane's ray enters before its closest hit so far is visited once for all
-// lanes, from child-pair records, the child the lanes enter first (least entry distance over the lanes) before
-// the other; an instance whose box a lane's ray enters is walked by that lane (instance_walk). Each lane gets
-// the hit its own walk of the tree finds, up to which of two equally distant hits is kept (the instance order
-// differs from a single ray's). ANY: shadow rays, done at their first hit. skip: an instance left out (a
-// shadow ray's own mesh, walked first or unreachable), or -1. The stack lives in the warp's shared memory.
-template <bool ANY>
+// A world's tree walked by the whole warp together (a packet), for the camera rays of worlds too large for
+// candidate lists: every internal node that some lane's ray enters before its closest hit so far is visited
+// once for all lanes, from child-pair records, the child the lanes enter first (least entry distance over the
+// lanes) before the other; an instance whose box a lane's ray enters is walked by that lane (instance_walk).
+// Each lane gets the hit its own walk of the tree finds, up to which of two equally distant hits is kept (the
+// instance order differs from a single ray's). The stack lives in the warp's shared memory.
 __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &sm, int lane, int world, bool active,
-    float3 o, float3 d, float &tmax, bool &done, int &hit_inst, int &hit_tri, float &hu, float &hv, int skip,
-    int max_steps, int *err) {
+    float3 o, float3 d, float &tmax, int &hit_inst, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
     const int root = s.instance_count > 0 ? __ldg(s.roots + world) : -1;
     if (root < 0) return;
     const float3 inv = safe_inverse(d);
     // The instance whose leaf box the lane's ray entered: walked by that lane.
     auto walk = [&](int id, bool enters) {
-        if (!enters || id == skip) return;
-        if constexpr (ANY) {
-            float tm = tmax, u, v;
-            int t;
-            done = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tm, t, u, v,
-                max_steps, err);
-        } else {
-            if (instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, hit_tri,
-                    hu, hv, max_steps, err))
-                hit_inst = id;
-        }
+        if (enters && instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax,
+                          hit_tri, hu, hv, max_steps, err))
+            hit_inst = id;
     };
     // An instance met on the stack: its leaf box first (leaf k of the sorted leaves is node n - 1 + k).
     auto leaf_walk = [&](int id) {
         const float4 *leaf = s.tlas + 2 * (static_cast<long long>(s.tlas_internal) + __ldg(s.leaf_of + id));
-        walk(id, active && !done && box_entry(__ldg(leaf), __ldg(leaf + 1), o, inv, tmax) < NO_HIT);
+        walk(id, active && box_entry(__ldg(leaf), __ldg(leaf + 1), o, inv, tmax) < NO_HIT);
     };
     if (root >= s.tlas_internal) {  // a world of one instance: its leaf is the root
         leaf_walk(~__float_as_int(__ldg(s.tlas + 2 * root).w));
@@ -234,7 +223,7 @@ __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &s
     }
     {
         const float4 lo = __ldg(s.tlas + 2 * root), hi = __ldg(s.tlas + 2 * root + 1);
-        if (!__any_sync(FULL, active && !done && box_entry(lo, hi, o, inv, tmax) < NO_HIT)) return;
+        if (!__any_sync(FULL, active && box_entry(lo, hi, o, inv, tmax) < NO_HIT)) return;
     }
     const int max_nodes = 2 * s.instance_count + 2;
     int ref = root, count = 0, sp = 0;
@@ -249,7 +238,7 @@ __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &s
         } else {
             const float4 *q = s.tlas_pairs + 4 * static_cast<long long>(ref);
             const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
-            const bool open = active && !done;
+            const bool open = active;
             const float dl = open ? box_entry(make_float4(q0.x, q0.y, q0.z, 0.0f), make_float4(q0.w, q1.x, q1.y, 0.0f), o,
                 inv, tmax) : NO_HIT;
             const float dr = open ? box_entry(make_float4(q1.z, q1.w, q2.x, 0.0f), make_float4(q2.y, q2.z, q2.w, 0.0f), o,
@@ -544,9 +533,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                     closest_meshes(s, sm, leaves, ncand, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps,
                         a.error_flag);
                 } else {
-                    bool unused = false;
-                    packet_walk<false>(s, sm, lane, T.world, T.pixel, eye, d, tmax, unused, hit_inst, hit_tri, hu, hv, -1,
-                        max_steps, a.error_flag);
+                    packet_walk(s, sm, lane, T.world, T.pixel, eye, d, tmax, hit_inst, hit_tri, hu, hv, max_steps,
+                        a.error_flag);
                 }
                 if (!T.pixel) continue;
                 const size_t p = static_cast<size_t>(T.pix);
@@ -742,8 +730,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
 template <int THREADS, int MIN_BLOCKS, int CAP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
-    __shared__ int warp_cand[THREADS / 32][CAP > 0 ? CAP : 1];
-    __shared__ WarpSmem<0> warp_stack[CAP > 0 ? 1 : THREADS / 32];
+    __shared__ int warp_cand[THREADS / 32][CAP];
     int *cand_leaf = warp_cand[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -768,7 +755,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
             const float sdist = o4.w;
             int ncand = 0;
             const float4 *leaves = world_leaves(s, T.world);
-            if constexpr (CAP > 0) {
             const float3 se = so + sd * sdist;
             const float mnx = warp_min(pending ? fminf(so.x, se.x) : INF);
             const float mny = warp_min(pending ? fminf(so.y, se.y) : INF);
@@ -826,7 +812,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 ncand += __popc(cmask);
             }
             __syncwarp();
-            }
             // The ray's own mesh first when the shade kernel found it starts on that body's side, or not at all when
             // it cannot meet it; any hit ends the ray whatever the order, so the answer is the same.
             const int self_code = pending ? a.shadow_self[T.pix] : -1;
@@ -841,12 +826,6 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                     blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd,
                         tm, ht, hu, hv, max_steps, a.error_flag);
                 }
-            }
-            if constexpr (CAP == 0) {
-                int ht = -1, hi = -1;
-                float tm = sdist, hu = 0.0f, hv = 0.0f;
-                packet_walk<true>(s, warp_stack[threadIdx.x >> 5], lane, T.world, pending, so, sd, tm, blocked, hi, ht, hu,
-                    hv, self_code >= 0 ? self : -1, max_steps, a.error_flag);
             }
             for (int c = 0; c < ncand; ++c) {
                 const bool open = pending && !blocked;
@@ -921,8 +900,14 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     e = cudaGetLastError();
     mark(after_shade);
     if (e != cudaSuccess || s.light_count != 1) return e;
-    return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
-        stream);
+    // Worlds too large for candidate lists: the shadow rays as persistent-kernel jobs, whose lanes refill as
+    // rays end (the packet walk keeps a tile's warp until its last ray ends).
+    if constexpr (CAP == 0) {
+        return launch_shadows_persistent(s, a, counter, stream);
+    } else {
+        return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x,
+            tiles_per_view, stream);
+    }
 }
 
 }  // namespace
