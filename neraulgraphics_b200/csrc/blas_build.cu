@@ -17,10 +17,13 @@
 //     and lie above it (a chain of left children at consecutive depths), so its rank is a prefix count over
 //     the start positions plus its depth below the chain's top, with no walk over the tree.
 // Node and tree sizes: a tree over T triangles has at most 2T - 1 nodes, numbered in scratch arrays of
-// 2T - 1 in level order. Each depth's launch records the next depth's range on the device, so the host
-// queues several depths before it reads back whether the tree is finished.
+// 2T - 1 in level order. The whole build is one cooperative launch: the CTAs (a CTA per large node, a warp per
+// small one) split one depth, meet at a grid-wide barrier, and go on to the next depth, whose nodes the splits
+// appended after the depth's last node; then the numbering and the packing, between further barriers.
 #include <climits>
 #include <cstdint>
+
+#include <cooperative_groups.h>
 
 #include "kernels.h"
 
@@ -99,16 +102,7 @@ __device__ __forceinline__ int bin_of(float c, float lo, float scale) {
 // Triangle boxes (the vertices' std::fmin / std::fmax in vertex order, src/mesh_build.cpp, as the host build
 // computes them: of two equal values, -0 and +0, the later one) and centroids (0.5 (lo + hi),
 // src/bvh.cpp:55-56); the order starts as the identity and the root spans every triangle.
-__global__ void prepare_kernel(const MeshBuildArgs a, const MeshBuildScratch t) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0) {
-        t.begin[0] = 0;
-        t.end[0] = a.triangles;
-        t.index[0] = 0;
-        t.counter[0] = 1;
-        t.range[0] = make_int2(0, 1);
-    }
-    if (i >= a.triangles) return;
+__device__ void prepare_item(const MeshBuildArgs &a, const MeshBuildScratch &t, int i) {
     t.starts[i] = 0;
     t.top[i] = INT_MAX;
     Box b = empty_box();
@@ -141,44 +135,51 @@ struct SplitSmem {
     int best_axis, best_bin, leaf, mid;
 };
 
-// Exclusive prefix sum of v over the CTA's threads (in thread order, or from the last thread down when
-// reverse), and the CTA's total.
+// A barrier over the threads that split one node: the CTA, or one warp.
 template <int WARPS>
-__device__ __forceinline__ int cta_scan(SplitSmem<WARPS> &sm, int v, bool reverse, int &total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+__device__ __forceinline__ void group_sync() {
+    if constexpr (WARPS == 1) __syncwarp();
+    else __syncthreads();
+}
+
+// Exclusive prefix sum of v over the group's threads (gtid: the thread's place in the group; in thread order,
+// or from the last thread down when reverse), and the group's total.
+template <int WARPS>
+__device__ __forceinline__ int cta_scan(SplitSmem<WARPS> &sm, int v, bool reverse, int &total, int gtid) {
+    const int lane = gtid & 31, warp = gtid >> 5;
     int incl = v;
     for (int o = 1; o < 32; o <<= 1) {
         const int u = reverse ? __shfl_down_sync(FULL, incl, o) : __shfl_up_sync(FULL, incl, o);
         if (reverse ? lane + o < 32 : lane >= o) incl += u;
     }
     if (reverse ? lane == 0 : lane == 31) sm.warp_sum[warp] = incl;
-    __syncthreads();
+    group_sync<WARPS>();
     int before = 0;
     total = 0;
     for (int w = 0; w < WARPS; ++w) {
         before += (reverse ? w > warp : w < warp) ? sm.warp_sum[w] : 0;
         total += sm.warp_sum[w];
     }
-    __syncthreads();
+    group_sync<WARPS>();
     return before + incl - v;
 }
 
-// Splits every node of one depth (its range recorded by the depth before), one CTA per node: 256 threads for
-// the upper depths' large nodes, one warp for the lower depths' small ones.
+// Splits node x at this depth with a group of THREADS threads (tid: the thread's place in the group): 256 for
+// the upper depths' large nodes, one warp for the lower depths' small ones. Its children, if any, take the
+// next two places after next_first (the next depth's first node) counted by next_count.
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int depth) {
+__device__ void split_node(const MeshBuildArgs &a, const MeshBuildScratch &t, int x, int depth, SplitSmem<THREADS / 32> &sm,
+    int tid, int next_first, int *next_count) {
     constexpr int WARPS = THREADS / 32;
-    __shared__ SplitSmem<WARPS> sm;
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int2 level = t.range[depth];
-    for (int x = level.x + blockIdx.x; x < level.y; x += gridDim.x) {
+    const int lane = tid & 31;
+    {
         const int begin = t.begin[x], end = t.end[x], count = end - begin;
         if (tid == 0) t.depth[x] = depth;
         for (int k = tid; k < 12; k += THREADS) sm.box_key[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
         for (int k = tid; k < 3 * BINS * 6; k += THREADS)
             (&sm.bin_key[0][0][0])[k] = (k % 6) < 3 ? NONE_MIN : NONE_MAX;
         for (int k = tid; k < 3 * BINS; k += THREADS) (&sm.bin_count[0][0])[k] = 0;
-        __syncthreads();
+        group_sync<WARPS>();
 
         // The node's box and centroid box: per thread the first of its smallest / largest values, then the
         // warp's and the CTA's by (value, position).
@@ -213,13 +214,13 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
                 }
             }
         }
-        __syncthreads();
+        group_sync<WARPS>();
         if (tid < 12) {  // the values the keys point at, one per thread
             const bool is_max = (tid % 6) >= 3;
             const uint32_t p = t.order[key_pos(sm.box_key[tid], is_max)];
             sm.node[tid] = tid < 6 ? t.box[6 * static_cast<size_t>(p) + tid] : t.centre[3 * static_cast<size_t>(p) + (tid - 6) % 3];
         }
-        __syncthreads();
+        group_sync<WARPS>();
         Box box;
         float cb[6];
         for (int k = 0; k < 3; ++k) {
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
                 }
             }
         }
-        __syncthreads();
+        group_sync<WARPS>();
         for (int e = tid; e < 3 * BINS * 6; e += THREADS) {  // the bin boxes' values, in parallel
             const int axis = e / (BINS * 6), b = (e / 6) % BINS, c = e % 6;
             float v = c < 3 ? __int_as_float(0x7f800000) : -__int_as_float(0x7f800000);
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             }
             sm.bin_box[axis][b][c] = v;
         }
-        __syncthreads();
+        group_sync<WARPS>();
 
         // The split: the cheapest plane over the axes in order, then the leaf test (src/bvh.cpp:108-146).
         if (tid == 0) {
@@ -314,13 +315,13 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             sm.best_bin = best_bin;
             for (int c = 0; c < 6; ++c) sm.cbox[c] = cb[c];
         }
-        __syncthreads();
+        group_sync<WARPS>();
         const int leaf = sm.leaf, best_axis = sm.best_axis, best_bin = sm.best_bin;
         if (tid < 6) t.node_box[6 * static_cast<size_t>(x) + tid] = tid < 3 ? box.lo[tid] : box.hi[tid - 3];
         if (leaf) {
             if (tid == 0) t.left[x] = -1;
-            __syncthreads();
-            continue;
+            group_sync<WARPS>();
+            return;
         }
 
         // std::partition over the range by (bin <= best_bin): the k-th failing element from the left swaps
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             int mine = 0;
             for (int i = r0; i < r1; ++i) mine += passes(i) ? 1 : 0;
             int passing;
-            cta_scan(sm, mine, false, passing);
+            cta_scan(sm, mine, false, passing, tid);
             const int meet = begin + passing;
             // Failing elements left of meet, ranked from the left; passing ones right of it, from the right.
             const int l1 = r1 < meet ? r1 : meet, q0 = r0 > meet ? r0 : meet;
@@ -348,13 +349,13 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             for (int i = r0; i < l1; ++i) fails += passes(i) ? 0 : 1;
             for (int j = q0; j < r1; ++j) passes_right += passes(j) ? 1 : 0;
             int swaps, found;
-            const int lbase = cta_scan(sm, fails, false, swaps);
-            const int rbase = cta_scan(sm, passes_right, true, found);
+            const int lbase = cta_scan(sm, fails, false, swaps, tid);
+            const int rbase = cta_scan(sm, passes_right, true, found, tid);
             for (int i = r0, k = lbase; i < l1; ++i)
                 if (!passes(i)) t.lpos[begin + k++] = i;
             for (int j = r1 - 1, k = rbase; j >= q0; --j)
                 if (passes(j)) t.rpos[begin + k++] = j;
-            __syncthreads();
+            group_sync<WARPS>();
             for (int k = tid; k < swaps; k += THREADS) {
                 const int l = t.lpos[begin + k], r = t.rpos[begin + k];
                 const uint32_t pl = t.order[l];
@@ -364,75 +365,22 @@ __global__ void __launch_bounds__(THREADS) split_kernel(const MeshBuildArgs a, c
             mid = meet;
             if (mid == begin || mid == end) mid = begin + count / 2;
         }
-        __syncthreads();
+        group_sync<WARPS>();
         if (tid == 0) {
-            const int c = atomicAdd(t.counter, 2);
+            const int c = next_first + atomicAdd(next_count, 2);
             t.left[x] = c;
             t.begin[c] = begin;
             t.end[c] = mid;
             t.begin[c + 1] = mid;
             t.end[c + 1] = end;
         }
-        __syncthreads();
+        group_sync<WARPS>();
     }
-}
-
-// The next depth's nodes: those the splits of this depth appended.
-__global__ void advance_kernel(const MeshBuildScratch t, int depth) {
-    t.range[depth + 1] = make_int2(t.range[depth].y, *t.counter);
-}
-
-// Per start position: the internal nodes starting there and the least depth among them.
-__global__ void starts_kernel(const MeshBuildScratch t, int nodes) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= nodes || t.left[x] < 0) return;
-    atomicAdd(t.starts + t.begin[x], 1);
-    atomicMin(t.top + t.begin[x], t.depth[x]);
-}
-
-// Exclusive prefix sum of the start counts, one CTA.
-__global__ void __launch_bounds__(1024) prefix_kernel(const MeshBuildScratch t, int n) {
-    __shared__ int warp_sum[32];
-    __shared__ int carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += 1024) {
-        const int i = base + threadIdx.x;
-        const int v = i < n ? t.starts[i] : 0;
-        int incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(FULL, incl, o);
-            if (lane >= o) incl += u;
-        }
-        if (lane == 31) warp_sum[warp] = incl;
-        __syncthreads();
-        int before = carry;
-        for (int w = 0; w < warp; ++w) before += warp_sum[w];
-        if (i < n) t.prefix[i] = before + incl - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = before + incl;
-        __syncthreads();
-    }
-}
-
-// The host's node indices: the k-th internal node in depth-first order has children 2k + 1 and 2k + 2.
-__global__ void index_kernel(const MeshBuildScratch t, int nodes) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= nodes) return;
-    const int l = t.left[x];
-    if (l < 0) return;
-    const int b = t.begin[x];
-    const int k = t.prefix[b] + t.depth[x] - t.top[b];
-    t.index[l] = 2 * k + 1;
-    t.index[l + 1] = 2 * k + 2;
 }
 
 // The packed tree (src/mesh_build.cpp:91-157): bvh::Node records with global indices, and the child-pair
 // records of the internal nodes.
-__global__ void nodes_kernel(const MeshBuildArgs a, const MeshBuildScratch t, int nodes) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= nodes) return;
+__device__ void write_node(const MeshBuildArgs &a, const MeshBuildScratch &t, int x) {
     const int i = t.index[x];
     const float *b = t.node_box + 6 * static_cast<size_t>(x);
     const int l = t.left[x];
@@ -463,9 +411,7 @@ __global__ void nodes_kernel(const MeshBuildArgs a, const MeshBuildScratch t, in
 
 // Triangles in leaf order (v0, e1 = v1 - v0, e2 = v2 - v0), their mesh indices both ways, and their vertex
 // normals (ATTR_NORMALS, src/mesh_build.h:28) where the scene keeps them.
-__global__ void triangles_kernel(const MeshBuildArgs a, const MeshBuildScratch t) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.triangles) return;
+__device__ void write_triangle(const MeshBuildArgs &a, const MeshBuildScratch &t, int p) {
     const uint32_t tri = t.order[p];
     const size_t packed = static_cast<size_t>(a.tri_base) + p;
     float3 v[3];
@@ -493,52 +439,129 @@ __global__ void triangles_kernel(const MeshBuildArgs a, const MeshBuildScratch t
 
 // The slots of this mesh: their root reference, their box in mesh space, and no convexity claim (the new
 // shape is not checked).
-__global__ void slots_kernel(const MeshBuildArgs a, const MeshBuildScratch t, const int *slot_mesh, int slots,
-    int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= slots || slot_mesh[s] != mesh) return;
+__device__ void write_slot(const MeshBuildArgs &a, const MeshBuildScratch &t, const int *slot_mesh, int mesh,
+    int2 *slot_root, float *slot_bounds, float4 *slot_hull, int s) {
+    if (slot_mesh[s] != mesh) return;
     const bool leaf = t.left[0] < 0;
     slot_root[s] = leaf ? make_int2(a.tri_base, a.triangles) : make_int2(a.node_base, 0);
     for (int c = 0; c < 6; ++c) slot_bounds[6 * static_cast<size_t>(s) + c] = t.node_box[c];
     slot_hull[s].w = -1.0f;
 }
 
-int blocks_for(long long n) { return static_cast<int>((n + 255) / 256); }
+// The whole build, one cooperative launch of CTAs of 256 threads; grid-wide barriers between its phases.
+__global__ void __launch_bounds__(256) build_mesh_kernel(const MeshBuildArgs a, const MeshBuildScratch t,
+    const int *slot_mesh, int slots, int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    __shared__ SplitSmem<8> cta_smem;
+    __shared__ SplitSmem<1> warp_smem[8];
+    __shared__ int prefix_warp[8];
+    __shared__ int prefix_carry;
+    const long long rank = grid.thread_rank(), size = grid.size();
+    const int T = a.triangles;
+    const long long cap = 2LL * T - 1;
+
+    // The mesh's whole node run cleared, the triangles' boxes, the root spanning every triangle.
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (long long k = rank; k < 2 * cap; k += size) a.blas[2LL * a.node_base + k] = zero;
+    for (long long k = rank; k < 4 * cap; k += size) a.pairs[4LL * a.node_base + k] = zero;
+    for (long long i = rank; i < T; i += size) prepare_item(a, t, static_cast<int>(i));
+    for (long long d = rank; d <= MESH_LEVELS; d += size) t.level_count[d] = 0;
+    if (rank == 0) {
+        t.begin[0] = 0;
+        t.end[0] = T;
+        t.index[0] = 0;
+    }
+    grid.sync();
+
+    // Depth after depth: the splits of depth d append depth d + 1's nodes after depth d's last.
+    int first = 0, last = 1;
+    for (int depth = 0; depth < MESH_LEVELS && first < last; ++depth) {
+        int *next_count = t.level_count + depth + 1;
+        if ((static_cast<long long>(T) >> depth) > 512) {
+            for (int x = first + blockIdx.x; x < last; x += gridDim.x)
+                split_node<256>(a, t, x, depth, cta_smem, threadIdx.x, last, next_count);
+        } else {
+            const int w = threadIdx.x >> 5;
+            for (int x = first + blockIdx.x * 8 + w; x < last; x += gridDim.x * 8)
+                split_node<32>(a, t, x, depth, warp_smem[w], threadIdx.x & 31, last, next_count);
+        }
+        grid.sync();
+        const int next = last + __ldcg(next_count);
+        first = last;
+        last = next;
+    }
+    const int nodes = last;
+
+    // Per start position: the internal nodes starting there and the least depth among them; their prefix sum
+    // (one CTA); then the host's node indices: the k-th internal node in depth-first order has children 2k + 1
+    // and 2k + 2.
+    for (long long x = rank; x < nodes; x += size)
+        if (t.left[x] >= 0) {
+            atomicAdd(t.starts + t.begin[x], 1);
+            atomicMin(t.top + t.begin[x], t.depth[x]);
+        }
+    grid.sync();
+    if (blockIdx.x == 0) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (threadIdx.x == 0) prefix_carry = 0;
+        __syncthreads();
+        for (int base = 0; base < T; base += 256) {
+            const int i = base + threadIdx.x;
+            const int v = i < T ? __ldcg(t.starts + i) : 0;
+            int incl = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += u;
+            }
+            if (lane == 31) prefix_warp[warp] = incl;
+            __syncthreads();
+            int before = prefix_carry;
+            for (int k = 0; k < warp; ++k) before += prefix_warp[k];
+            if (i < T) t.prefix[i] = before + incl - v;
+            __syncthreads();
+            if (threadIdx.x == 255) prefix_carry = before + incl;
+            __syncthreads();
+        }
+    }
+    grid.sync();
+    for (long long x = rank; x < nodes; x += size) {
+        const int l = t.left[x];
+        if (l < 0) continue;
+        const int b = t.begin[x];
+        const int k = t.prefix[b] + t.depth[x] - __ldcg(t.top + b);
+        t.index[l] = 2 * k + 1;
+        t.index[l + 1] = 2 * k + 2;
+    }
+    if (rank == 0) *t.counter = nodes;
+    grid.sync();
+
+    // The packed tree, its triangles, and the slots of this mesh.
+    for (long long x = rank; x < nodes; x += size) write_node(a, t, static_cast<int>(x));
+    for (long long p = rank; p < T; p += size) write_triangle(a, t, static_cast<int>(p));
+    for (long long k = rank; k < slots; k += size)
+        write_slot(a, t, slot_mesh, mesh, slot_root, slot_bounds, slot_hull, static_cast<int>(k));
+}
 
 }  // namespace
 
-cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &t, cudaStream_t s) {
-    prepare_kernel<<<blocks_for(a.triangles), 256, 0, s>>>(a, t);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mesh_level(const MeshBuildArgs &a, const MeshBuildScratch &t, int depth, cudaStream_t s) {
-    // A depth holds at most 2^depth nodes, and the CTAs stride over whatever it holds.
-    const int most = depth < 16 ? 1 << depth : 65536;
-    const int cap = a.triangles < most ? a.triangles : most;
-    // A node at depth d holds about T / 2^d triangles: 256-thread CTAs while that is above a few hundred.
-    if ((static_cast<long long>(a.triangles) >> depth) > 512)
-        split_kernel<256><<<cap > 0 ? cap : 1, 256, 0, s>>>(a, t, depth);
-    else
-        split_kernel<32><<<cap > 0 ? cap : 1, 32, 0, s>>>(a, t, depth);
-    advance_kernel<<<1, 1, 0, s>>>(t, depth);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mesh_number(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, cudaStream_t s) {
-    starts_kernel<<<blocks_for(nodes), 256, 0, s>>>(t, nodes);
-    prefix_kernel<<<1, 1024, 0, s>>>(t, a.triangles);
-    index_kernel<<<blocks_for(nodes), 256, 0, s>>>(t, nodes);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mesh_write(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, const int *slot_mesh,
-    int slots, int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t s) {
-    nodes_kernel<<<blocks_for(nodes), 256, 0, s>>>(a, t, nodes);
-    triangles_kernel<<<blocks_for(a.triangles), 256, 0, s>>>(a, t);
-    if (slots > 0)
-        slots_kernel<<<blocks_for(slots), 256, 0, s>>>(a, t, slot_mesh, slots, mesh, slot_root, slot_bounds, slot_hull);
-    return cudaGetLastError();
+cudaError_t launch_mesh_build(const MeshBuildArgs &a, const MeshBuildScratch &t, const int *slot_mesh, int slots,
+    int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t stream) {
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, build_mesh_kernel, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    // Every CTA resident at once (the barriers need it); no more CTAs than about one per 8 triangles.
+    long long blocks = static_cast<long long>(sms) * per_sm;
+    const long long want = (static_cast<long long>(a.triangles) + 7) / 8;
+    if (blocks > want) blocks = want;
+    if (blocks < 1) blocks = 1;
+    void *args[] = {const_cast<MeshBuildArgs *>(&a), const_cast<MeshBuildScratch *>(&t), &slot_mesh, &slots, &mesh,
+        &slot_root, &slot_bounds, &slot_hull};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(build_mesh_kernel), dim3(static_cast<unsigned>(blocks)),
+        dim3(256), args, 0, stream);
 }
 
 }  // namespace ngb

@@ -190,18 +190,15 @@ struct MeshBuildScratch {
     int *left;                  // per node: its first child (the second follows), or -1 for a leaf
     int *depth;                 // per node
     int *index;                 // per node: its index in the mesh's tree
-    int *counter;               // the next free node
-    int2 *range;                // per depth (MESH_LEVELS + 1): its nodes [x, y)
+    int *counter;               // out: the tree's node count
+    int *level_count;           // per depth (MESH_LEVELS + 1): the nodes its parents' splits appended
     int *starts, *top, *prefix; // per order position: internal nodes starting there, the least depth of those,
                                 // and the internal nodes starting before it
 };
 constexpr int MESH_LEVELS = 61;  // depths 0..60: a node at depth 60 is a leaf
-cudaError_t launch_mesh_prepare(const MeshBuildArgs &a, const MeshBuildScratch &t, cudaStream_t s);
-// Splits the nodes of one depth and records the next depth's range (no host round trip).
-cudaError_t launch_mesh_level(const MeshBuildArgs &a, const MeshBuildScratch &t, int depth, cudaStream_t s);
-// The host's node indices of the finished tree of `nodes` nodes.
-cudaError_t launch_mesh_number(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, cudaStream_t s);
-cudaError_t launch_mesh_write(const MeshBuildArgs &a, const MeshBuildScratch &t, int nodes, const int *slot_mesh,
-    int slots, int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t s);
+// The whole rebuild in one cooperative launch: the tree, its packing, and the slots of this mesh (their root
+// reference, box and convexity claim); the node count lands in t.counter.
+cudaError_t launch_mesh_build(const MeshBuildArgs &a, const MeshBuildScratch &t, const int *slot_mesh, int slots,
+    int mesh, int2 *slot_root, float *slot_bounds, float4 *slot_hull, cudaStream_t stream);
 
 }  // namespace ngb

@@ -148,7 +148,7 @@ struct Renderer {
     DevBuf<float> mb_box, mb_centre, mb_node_box;
     DevBuf<uint32_t> mb_order;
     DevBuf<int> mb_lpos, mb_rpos, mb_begin, mb_end, mb_left, mb_depth, mb_index, mb_counter, mb_starts, mb_top, mb_prefix;
-    DevBuf<int2> mb_range;
+    DevBuf<int> mb_level_count;
     int *host_count = nullptr;  // pinned: a level's node count read back during a mesh rebuild
     // Staging for host inputs and the renderer's own outputs.
     DevBuf<float> cameras, ray_origins, ray_directions;
@@ -502,7 +502,7 @@ Renderer::~Renderer() {
     mb_box.release(), mb_centre.release(), mb_node_box.release(), mb_order.release(), mb_lpos.release();
     mb_rpos.release(), mb_begin.release(), mb_end.release(), mb_left.release(), mb_depth.release();
     mb_index.release(), mb_counter.release(), mb_starts.release(), mb_top.release(), mb_prefix.release();
-    mb_range.release();
+    mb_level_count.release();
     blas_pairs.release(), tlas_pairs.release(), slot_root.release(), work_counter.release();
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
@@ -783,7 +783,7 @@ void Renderer::update_mesh(int mesh, const float *vertices, const float *normals
     t.depth = mb_depth.ensure(cap);
     t.index = mb_index.ensure(cap);
     t.counter = mb_counter.ensure(1);
-    t.range = mb_range.ensure(MESH_LEVELS + 1);
+    t.level_count = mb_level_count.ensure(MESH_LEVELS + 1);
     t.starts = mb_starts.ensure(T);
     t.top = mb_top.ensure(T);
     t.prefix = mb_prefix.ensure(T);
@@ -800,29 +800,15 @@ void Renderer::update_mesh(int mesh, const float *vertices, const float *normals
     a.attrs = attrs.p;
     a.tri_index = tri_index.p;
     a.tri_of_local = tri_of_local.p;
-    // The mesh's whole node capacity is cleared: nodes past the new tree's last are zero, as at creation.
-    CK(cudaMemsetAsync(blas.p + 2 * static_cast<size_t>(a.node_base), 0, 2 * cap * sizeof(float4), stream));
-    CK(cudaMemsetAsync(blas_pairs.p + 4 * static_cast<size_t>(a.node_base), 0, 4 * cap * sizeof(float4), stream));
-    CK(launch_mesh_prepare(a, t, stream));
-    // Depth after depth, several queued at a time; the node count read back after each batch says whether the
-    // last depth split anything (a tree over T triangles is about log2 T deep; a node at depth 60 is a leaf).
-    constexpr int BATCH = 6;
-    int nodes = 1;
-    for (int depth = 0; depth < MESH_LEVELS;) {
-        const int stop = std::min(depth + BATCH, MESH_LEVELS);
-        for (; depth < stop; ++depth) CK(launch_mesh_level(a, t, depth, stream));
-        CK(cudaMemcpyAsync(host_count, t.counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CK(cudaEventRecord(ev_done, stream));
-        wait(ev_done, timeout);
-        const int now = *host_count;
-        require(now >= nodes && static_cast<size_t>(now) <= cap, name + ": the tree rebuild went wrong");
-        if (now == nodes) break;
-        nodes = now;
-    }
-    CK(launch_mesh_number(a, t, nodes, stream));
-    CK(launch_mesh_write(a, t, nodes, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
+    // One cooperative launch builds and packs the tree (clearing the mesh's whole node run first, so nodes past
+    // the new tree's last are zero, as at creation); its node count comes back for inspection.
+    CK(launch_mesh_build(a, t, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
         slot_bounds.p, slot_hull.p, stream));
-    mesh_nodes[mesh] = nodes;
+    CK(cudaMemcpyAsync(host_count, t.counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaEventRecord(ev_done, stream));
+    wait(ev_done, timeout);
+    require(*host_count >= 1 && static_cast<size_t>(*host_count) <= cap, name + ": the tree rebuild went wrong");
+    mesh_nodes[mesh] = *host_count;
     if (n > 0) build(matrices.p, 0, nullptr);
     finish();
 }
