@@ -197,6 +197,24 @@ def test_library_exports_every_declared_entry_point():
     assert not missing, missing
 
 
+def test_stream_entry_points_check_their_arguments_before_any_launch():
+    """The handle-free entry points (pose matrices, their gradient) reject bad arguments on the host, with a
+    message in ngb_last_error(NULL), and do nothing for zero poses; no GPU is touched."""
+    import ctypes
+    from neraulgraphics_b200._lib import lib
+    L = lib()
+    L.ngb_last_error.restype = ctypes.c_char_p
+    assert L.ngb_pose_matrices(None, None, None, 0, None, None) == 0
+    assert L.ngb_pose_matrices(None, None, None, 5, None, None) == 1
+    assert b"positions, quaternions and matrices must not be null" in L.ngb_last_error(None)
+    assert L.ngb_pose_matrices(None, None, None, -1, None, None) == 1
+    assert L.ngb_pose_matrices_grad(None, None, 0, None, None, None, None, None) == 0
+    assert L.ngb_pose_matrices_grad(None, None, 3, None, None, None, None, None) == 1
+    dummy = ctypes.c_void_p(16)
+    assert L.ngb_pose_matrices_grad(dummy, None, 3, dummy, dummy, dummy, dummy, None) == 1
+    assert b"grad_scales needs scales" in L.ngb_last_error(None)
+
+
 def test_construction_rejects_bad_scenes_with_the_reference_messages():
     import neraulgraphics_b200 as ng
     with pytest.raises(ValueError, match="world_count must be 1 or more, got 0"):
