@@ -33,7 +33,7 @@ using namespace tr;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int TILE_W = 8, TILE_H = 4;
 constexpr int WALK_STACK = 64;      // a mesh's tree is at most 60 deep
-constexpr int TILES_PER_FETCH = 4;  // tiles a warp takes with one atomic
+constexpr int TILES_PER_FETCH = 1;  // tiles a warp takes with one atomic (1: the finest balance, measured fastest)
 
 // A tile's candidate instances as its warp holds them: each one's position in its world's run of sorted
 // leaves and the distance below which no camera ray of the tile can enter its box, collected in leaf order,
