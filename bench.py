@@ -473,6 +473,7 @@ def run_large(args, rank, world, local_rank, dist):
         "stages_ms": {"set_instance_transforms": round(statistics.median(stage[0]), 4),
                       "render": round(statistics.median(stage[1]), 4),
                       "lidar": round(statistics.median(stage[2]), 4)},
+        "step_ms": [round(stage[0][k] + stage[1][k] + stage[2][k], 3) for k in range(K)],
         "lidar_rays_per_s": round(rays / (statistics.median(stage[2]) / 1000.0), 1),
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
                                                                             "leaf_batch", "ms")},

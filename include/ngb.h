@@ -297,11 +297,12 @@ int ngb_set_stream(ngb_renderer *r, void *cuda_stream);
 /* synchronous 1: calls wait for their work, at most timeout_seconds (NGB_TIMEOUT after that).
  * synchronous 0: calls return once the work is queued. */
 int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
-/* How renders run. kernel: 0 automatic (the tile kernel where it applies: one sample per pixel, at most one
- * light, no material with reflectivity >= 1e-3, at most 256 instances per world; else the persistent kernel
- * where it applies: the same without the instance limit; else the per-pixel kernel), 1 the per-pixel kernel,
+/* How renders run. kernel: 0 automatic (the tile kernels where they apply: one sample per pixel, at most one
+ * light, no material with reflectivity >= 1e-3; else the per-pixel kernel), 1 the per-pixel kernel,
  * 2 the persistent kernel where it applies, 3 the tile kernels where the persistent kernel applies (worlds of
  * at most 256 instances through per-tile candidate lists, larger ones walking their tree as a warp packet).
+ * Ray queries (ngb_cast_rays) take the persistent kernel in a shape of their own (256/64, refill 28, no leaf
+ * batching) unless kernel 2 is chosen, whose shape they then take, or kernel 1 (the per-thread ray kernel).
  * With kernel 3 the call sets the tile kernel's shape: threads_per_block and registers as one of 128/48,
  * 128/56, 128/64, 128/80, 256/64 (default 128/56); refill_lanes and leaf_batch are not read.
  * Otherwise it sets the persistent kernel's shape: threads_per_block and registers (the register budget per

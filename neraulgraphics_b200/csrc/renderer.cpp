@@ -128,6 +128,9 @@ struct Renderer {
     int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
     PersistentTuning tuning{128, 28, 72, 16};
     PersistentTuning tile_tuning{128, 0, 56, 0};
+    // Ray queries: the persistent kernel's shape measured best for them (no leaf batching), unless the caller
+    // chose the persistent kernel and its shape.
+    PersistentTuning ray_tuning{256, 28, 64, 1};
     // Bodies.
     bool bound = false;
     int bodies_per_world = 0;
@@ -865,11 +868,10 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     }
     a.error_flag = error_flag.p;
     // The persistent and tile kernels cover one sample per pixel, at most one light and no bounces; everything
-    // else takes the per-pixel kernel, which runs trace in full. Automatic: the tile kernels for worlds of at
-    // most TILE_MAX_INSTANCES instances (candidate lists), the persistent kernel above.
+    // else takes the per-pixel kernel, which runs trace in full. Automatic: the tile kernels (candidate lists
+    // for worlds of at most TILE_MAX_INSTANCES instances, a packet walk of the world tree above).
     const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
-    const bool small_worlds = params.instance_count == 0 || params.per_world <= TILE_MAX_INSTANCES;
-    const bool tiles = persistent_ok && (uneven || kernel_choice == 3 || (kernel_choice == 0 && small_worlds));
+    const bool tiles = persistent_ok && (uneven || kernel_choice == 3 || kernel_choice == 0);
     const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
     require(!uneven || tiles, "worlds of uneven sizes render with one sample per pixel, at most one light and no "
         "reflective material");
@@ -944,7 +946,8 @@ void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, flo
     if (timed) CK(cudaEventRecord(ev_start, stream));
     // The persistent kernel's lane-refilling walk; the per-thread kernel when the per-pixel kernel is chosen.
     if (kernel_choice == 1) CK(launch_rays(params, a, stream));
-    else CK(launch_rays_persistent(params, a, reinterpret_cast<int *>(work_counter.p), tuning, stream));
+    else CK(launch_rays_persistent(params, a, reinterpret_cast<int *>(work_counter.p),
+        kernel_choice == 2 ? tuning : ray_tuning, stream));
     if (timed) {
         stages = 1;
         CK(cudaEventRecord(ev_stop, stream));

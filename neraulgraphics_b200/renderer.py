@@ -394,9 +394,10 @@ class BatchRenderer:
     # ----------------------------------------------------------------------------------------- inspection --
 
     def set_tuning(self, kernel=0, threads_per_block=128, refill_lanes=28, registers=72, leaf_batch=16):
-        """kernel: 0 automatic, 1 the per-pixel kernel, 2 the persistent kernel (where it applies: one sample per
-        pixel, at most one light, no reflective material), 3 the tile kernels (where the persistent kernel applies:
-        per-tile candidate lists for worlds of at most 256 instances, a warp-packet walk of the world tree above). With kernel 3, threads_per_block and registers set the tile
+        """kernel: 0 automatic (the tile kernels where they apply), 1 the per-pixel kernel, 2 the persistent kernel
+        (where it applies: one sample per pixel, at most one light, no reflective material), 3 the tile kernels
+        (where the persistent kernel applies: per-tile candidate lists for worlds of at most 256 instances, a
+        warp-packet walk of the world tree above). Ray queries keep a shape of their own unless kernel 2 is set. With kernel 3, threads_per_block and registers set the tile
         kernel's shape; otherwise they, refill_lanes and leaf_batch set the persistent kernel's (see
         ngb_set_tuning)."""
         check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes), int(registers),
