@@ -572,3 +572,25 @@ def test_tile_kernel_walks_large_worlds_as_packets(torch_cuda, tuning):
         got = r.render(c, fov, 1, **ALL)
         assert (got["object_ids"] >= 34).mean() > 0.1
         assert_same_images(got, want, ties=want["ties"])
+
+
+def test_packet_tiles_with_partial_tiles_two_cameras_spheres_and_floor(torch_cuda):
+    """The large-world tile path with everything around it: 300 instances per world (packet walk), two cameras
+    per world, 37x29 images (partial tiles), spheres and a checker floor, shadow rays as persistent-kernel
+    pixel jobs: against the oracle."""
+    wl = workloads.icosphere_worlds(worlds=3, per_world=300, width=37, height=29, seed=23)
+    d = wl.desc
+    spheres = [ng.Sphere((0.5, -1.0, -7.0), 0.7), ng.Sphere((-1.5, 0.0, -8.0), 0.5)]
+    floor = ng.Plane(y=-2.0, half_extent_x=12.0, z_min=-30.0, z_max=-2.0, checker_scale=1.0)
+    desc = ng.SceneDesc(d.width, d.height, 3, 2, spheres, d.lights, floor, d.meshes, d.instances)
+    cams = np.repeat(wl.cameras, 2, axis=0)
+    cams[1::2, :, 3] += np.float32([0.4, 0.1, 0.0])
+    r, o = product(desc), O.Oracle(desc)
+    r.set_instance_transforms(wl.matrices)
+    o.set_instance_transforms(wl.matrices)
+    r.ambient = 0.05
+    o.set_ambient(0.05)
+    want = o.render(cams, 1.0, 1, **ALL, frame=2, ties=True)
+    got = r.render(cams, 1.0, 1, **ALL, frame=2)
+    assert (got["object_ids"] >= 34).mean() > 0.1 and (got["object_ids"] == 33).mean() > 0.01
+    assert_same_images(got, want, ties=want["ties"])
