@@ -243,7 +243,9 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
         const float4 d4 = a.shadow_d[item];
         L.job = JOB_SHADOW_PIXEL;
         cold.put_pix(item);
-        L.world = static_cast<int>(item / (static_cast<long long>(a.width) * a.height)) / a.cameras_per_world;
+        const int view = a.view_info ? view_of(a.view_info, a.views, item, false)
+                                     : static_cast<int>(item / (static_cast<long long>(a.width) * a.height));
+        L.world = view / a.cameras_per_world;
         L.o = mk3(o4.x, o4.y, o4.z);
         L.d = mk3(d4.x, d4.y, d4.z);
         L.tmax = o4.w;
@@ -564,7 +566,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayA
     const int kinds = shadows ? KINDS_SHADOWS : rays ? KINDS_RAYS
         : (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
     if (kinds == 0) return cudaSuccess;
-    const long long total = shadows ? static_cast<long long>(a.views) * a.width * a.height
+    const long long total = shadows ? (a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.height)
         : rays ? rays->count : 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
     if (total == 0) return cudaSuccess;
     const RayArgs ra = rays ? *rays : RayArgs{};

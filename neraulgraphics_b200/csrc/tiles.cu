@@ -348,18 +348,6 @@ struct TileAt {
     long long pix;
 };
 
-// The last view whose first tile (uneven views: view_info[v].w) or first pixel (.z) is at most at.
-__device__ __forceinline__ int view_of(const int4 *info, int views, long long at, bool by_tile) {
-    int lo = 0, hi = views - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        const int4 v = __ldg(info + mid);
-        if ((by_tile ? v.w : v.z) <= at) lo = mid;
-        else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view, int lane) {
     TileAt t;
     int q;

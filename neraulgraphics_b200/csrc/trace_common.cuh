@@ -426,6 +426,19 @@ __device__ __forceinline__ void write_rgb(const float *table, uint8_t *rgb, long
     o[2] = srgb_byte(table, sum.z);
 }
 
+// Views of uneven sizes (view_info: per view width, height, first pixel, first tile): the last view whose
+// first tile (by_tile) or first pixel is at most at.
+__device__ __forceinline__ int view_of(const int4 *info, int views, long long at, bool by_tile) {
+    int lo = 0, hi = views - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int4 v = __ldg(info + mid);
+        if ((by_tile ? v.w : v.z) <= at) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 }  // namespace
 }  // namespace tr
 }  // namespace ngb
