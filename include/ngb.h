@@ -172,7 +172,7 @@ typedef struct {
     int32_t device_id;
     int32_t views;
     int32_t width;
-    int32_t height;
+    int32_t height;           /* the rows drawn: the image's height unless ngb_set_rows chose fewer */
     const uint8_t *rgb;
     const float *depth;
     const float *normal;
@@ -319,6 +319,16 @@ int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, i
  * reference, which always runs its global build. */
 int ngb_set_build(ngb_renderer *r, int32_t mode);
 
+/* The rows every later render draws: image rows [first, first + count) of every view, count >= 1 and
+ * first + count <= height; (0, height) is the whole image again (the default). The rays, their random streams
+ * and so every pixel are the whole image's; the outputs (and ngb_pixel_count, the hit records and the
+ * adjoint's per-pixel inputs) hold views x count x width pixels, the band's rows in order. For splitting one
+ * large picture across GPUs by rows. Not for worlds of uneven sizes. No counterpart in the reference, which
+ * renders whole images. */
+int ngb_set_rows(ngb_renderer *r, int32_t first, int32_t count);
+/* The rows set by ngb_set_rows: *first and *count (the whole image: 0 and height). */
+int ngb_rows(const ngb_renderer *r, int32_t *first, int32_t *count);
+
 /* Waits for every call queued so far, at most timeout_seconds, and reports a kernel's error flag (a
  * traversal stack or walk that ran past what a valid tree allows) as NGB_CUDA_ERROR. */
 int ngb_synchronize(ngb_renderer *r, double timeout_seconds);
@@ -356,7 +366,8 @@ typedef struct ngb_uneven_world {
  * each world's width x height pixels row-major (ngb_pixel_count in all). Body bindings are not supported.
  * No counterpart in the reference, whose worlds all hold the same instances at one image size. */
 int ngb_create_uneven(const ngb_scene *scene, const ngb_uneven_world *worlds, int32_t world_count, ngb_renderer **out);
-/* Pixels of one image of every view: views x width x height, or the uneven worlds' sum. */
+/* Pixels of one image of every view: views x width x height (height: the rows drawn, ngb_set_rows), or the
+ * uneven worlds' sum. */
 int64_t ngb_pixel_count(const ngb_renderer *r);
 
 /* ---- differentiation ------------------------------------------------------------------------------- */

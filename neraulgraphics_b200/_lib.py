@@ -77,6 +77,8 @@ def lib():
     L.ngb_build_tlas_noalloc.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
+    L.ngb_set_rows.argtypes = [_vp, C.c_int32, C.c_int32]
+    L.ngb_rows.argtypes = [_vp, _i32p, _i32p]
     L.ngb_copy_hits.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.ngb_depth_normal_adjoint.argtypes = [_vp, _vp, _vp, C.c_float] + [_vp] * 9
     L.ngb_srgb_thresholds.argtypes = [_vp]

@@ -27,7 +27,7 @@ class _DepthNormals(torch.autograd.Function):
         m = matrices.detach().contiguous()
         c = cameras.detach().contiguous()
         renderer.set_instance_transforms(m)
-        views, h, w = renderer.view_count, renderer.height, renderer.width
+        views, h, w = renderer.view_count, renderer.rows[1], renderer.width
         depth = torch.empty((views, h, w), dtype=torch.float32, device=m.device)
         normals = torch.empty((views, h, w, 3), dtype=torch.float32, device=m.device)
         hits = (torch.empty(depth.shape, dtype=torch.int32, device=depth.device),

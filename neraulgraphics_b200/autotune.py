@@ -31,7 +31,7 @@ def cache_path() -> str:
 def _key(renderer, outputs) -> str:
     import torch
     name = torch.cuda.get_device_name(renderer._device)
-    return (f"{name}|{renderer.world_count}x{renderer.cameras_per_world}|{renderer.width}x{renderer.height}|"
+    return (f"{name}|{renderer.world_count}x{renderer.cameras_per_world}|{renderer.width}x{renderer.rows[1]}|"
             f"{renderer.instances_per_world}|{outputs}")
 
 

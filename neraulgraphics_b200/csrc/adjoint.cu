@@ -108,15 +108,15 @@ __global__ void __launch_bounds__(ADJ_THREADS, 4) depth_normal_adjoint_kernel(co
     const int view = blockIdx.x / tiles_per_view;
     const int q = blockIdx.x % tiles_per_view;
     const int x = (q % tiles_x) * ADJ_TILE + threadIdx.x % ADJ_TILE;
-    const int y = (q / tiles_x) * ADJ_TILE + threadIdx.x / ADJ_TILE;
+    const int y = a.row_first + (q / tiles_x) * ADJ_TILE + threadIdx.x / ADJ_TILE;
     const int world = view / a.cameras_per_world;
     const int P = s.per_world;
     float *cam_sum = sums + (shared_sums ? 12 * P : 0);
     for (int k = threadIdx.x; k < (shared_sums ? 12 * P : 0) + 12; k += ADJ_THREADS) sums[k] = 0.0f;
     __syncthreads();
 
-    const long long pix = (static_cast<long long>(view) * a.height + y) * a.width + x;
-    const bool inside = x < a.width && y < a.height;
+    const long long pix = (static_cast<long long>(view) * a.rows + (y - a.row_first)) * a.width + x;
+    const bool inside = x < a.width && y < a.row_first + a.rows;
     const int inst = inside ? a.hit_instance[pix] : -1;
     const float depth = inside ? a.depth[pix] : __int_as_float(0x7f800000);
     const bool hit = inside && isfinite(depth);
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 4) depth_normal_adjoint_kernel(co
 }  // namespace
 
 cudaError_t launch_depth_normal_adjoint(const SceneParams &s, const AdjointArgs &a, cudaStream_t stream) {
-    const int tiles_x = (a.width + ADJ_TILE - 1) / ADJ_TILE, tiles_y = (a.height + ADJ_TILE - 1) / ADJ_TILE;
+    const int tiles_x = (a.width + ADJ_TILE - 1) / ADJ_TILE, tiles_y = (a.rows + ADJ_TILE - 1) / ADJ_TILE;
     const long long blocks = static_cast<long long>(tiles_x) * tiles_y * a.views;
     if (blocks == 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

@@ -70,15 +70,17 @@ struct RenderArgs {
     float fov_scale;               // tanf(fov / 2), computed on the host
     float aspect;                  // width / height
     int width;
-    int height;
+    int height;                    // the image's height: rays and random streams follow the whole image
+    int row_first;                 // the rows rendered, [row_first, row_first + rows) of every view's image;
+    int rows;                      // the outputs hold views x rows x W pixels (rows = height: the whole image)
     int cameras_per_world;
     int views;
     int frame;
     int spp;
-    uint8_t *rgb;                  // views x H x W x 3, or null
-    float *depth;                  // views x H x W, or null
-    float *normal;                 // views x H x W x 3, or null
-    int32_t *object_id;            // views x H x W, or null
+    uint8_t *rgb;                  // views x rows x W x 3, or null
+    float *depth;                  // views x rows x W, or null
+    float *normal;                 // views x rows x W x 3, or null
+    int32_t *object_id;            // views x rows x W, or null
     int32_t *hit_instance;         // centre ray's hit record, or null
     int32_t *hit_triangle;
     float *hit_u;
@@ -149,6 +151,8 @@ struct AdjointArgs {
     float aspect;
     int width;
     int height;
+    int row_first;                 // the rows the forward rendered (RenderArgs)
+    int rows;
     int cameras_per_world;
     int views;
     const int32_t *hit_instance;   // per pixel: the centre ray's hit, -1 for none or not a mesh

@@ -244,7 +244,7 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
         L.job = JOB_SHADOW_PIXEL;
         cold.put_pix(item);
         const int view = a.view_info ? view_of(a.view_info, a.views, item, false)
-                                     : static_cast<int>(item / (static_cast<long long>(a.width) * a.height));
+                                     : static_cast<int>(item / (static_cast<long long>(a.width) * a.rows));
         L.world = view / a.cameras_per_world;
         L.o = mk3(o4.x, o4.y, o4.z);
         L.d = mk3(d4.x, d4.y, d4.z);
@@ -307,13 +307,13 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
     const int q = static_cast<int>(item % per_view);
     const int tile = q >> 4, within = q & 15;
     const int x = (tile % tiles_x) * 4 + (within & 3);
-    const int y = (tile / tiles_x) * 4 + (within >> 2);
-    if (x >= a.width || y >= a.height) {
+    const int y = a.row_first + (tile / tiles_x) * 4 + (within >> 2);
+    if (x >= a.width || y >= a.row_first + a.rows) {
         L.state = ST_IDLE;
         return;
     }
     L.job = job;
-    cold.put_pix((static_cast<long long>(view) * a.height + y) * a.width + x);
+    cold.put_pix((static_cast<long long>(view) * a.rows + (y - a.row_first)) * a.width + x);
     L.world = view / a.cameras_per_world;
     // The view's camera (camera_from_matrix, src/render_core.h:264-273), made once per view by
     // prepare_cameras: (position.xyz, right.x) (right.yz, up.xy) (up.z, forward.xyz).
@@ -561,12 +561,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
 template <int THREADS, int MIN_BLOCKS>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayArgs *rays, int *counter, int refill,
     int leaf_batch, cudaStream_t stream, bool shadows = false) {
-    const int tiles_x = (a.width + 3) / 4, tiles_y = (a.height + 3) / 4;
+    const int tiles_x = (a.width + 3) / 4, tiles_y = (a.rows + 3) / 4;
     const int tiles_per_view = tiles_x * tiles_y;
     const int kinds = shadows ? KINDS_SHADOWS : rays ? KINDS_RAYS
         : (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
     if (kinds == 0) return cudaSuccess;
-    const long long total = shadows ? (a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.height)
+    const long long total = shadows ? (a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.rows)
         : rays ? rays->count : 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
     if (total == 0) return cudaSuccess;
     const RayArgs ra = rays ? *rays : RayArgs{};

@@ -98,6 +98,9 @@ struct Renderer {
     int width = 0, height = 0, worlds = 0, cpw = 0, per_world = 0, device = 0;
     long long n = 0;
     SceneParams params{};
+    // The rows every render draws, [band_first, band_first + band_rows) of each view's image (ngb_set_rows):
+    // the whole image by default.
+    int band_first = 0, band_rows = 0;
 
     // The scene: shared meshes and what each slot of a world holds.
     DevBuf<float4> blas, tris, attrs;
@@ -216,8 +219,9 @@ struct Renderer {
         float *depth, float *normal, int32_t *ids);
     void cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory, ngb_ray_hits *out,
         float *distance, float *normal, int32_t *ids);
+    int rows() const { return band_rows > 0 ? band_rows : height; }
     size_t pixels() const {
-        return uneven ? static_cast<size_t>(total_pixels) : static_cast<size_t>(worlds) * cpw * height * width;
+        return uneven ? static_cast<size_t>(total_pixels) : static_cast<size_t>(worlds) * cpw * rows() * width;
     }
     int world_of_instance(long long g) const {
         if (!uneven) return static_cast<int>(g / per_world);
@@ -845,6 +849,8 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     a.aspect = uneven ? 1.0f : static_cast<float>(width) / static_cast<float>(height);
     a.width = width;
     a.height = height;
+    a.row_first = band_first;
+    a.rows = rows();
     a.cameras_per_world = cpw;
     a.views = views;
     a.frame = frame;
@@ -1129,7 +1135,7 @@ int ngb_render(ngb_renderer *h, const float *cams, float fov, int32_t spp, uint3
         float *normal = (outputs & NGB_OUTPUT_NORMAL) ? r.out_normal.ensure(3 * px) : nullptr;
         int32_t *ids = (outputs & NGB_OUTPUT_OBJECT_ID) ? r.out_id.ensure(px) : nullptr;
         r.render(cams, fov, spp, outputs, frame, camera_memory, rgb, depth, normal, ids);
-        *out = ngb_batch_frame{NGB_MEMORY_DEVICE, r.device, r.worlds * r.cpw, r.width, r.height, rgb, depth, normal, ids};
+        *out = ngb_batch_frame{NGB_MEMORY_DEVICE, r.device, r.worlds * r.cpw, r.width, r.rows(), rgb, depth, normal, ids};
     });
 }
 
@@ -1331,6 +1337,24 @@ int ngb_set_build(ngb_renderer *h, int32_t mode) {
     });
 }
 
+int ngb_set_rows(ngb_renderer *h, int32_t first, int32_t count) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(!r.uneven, "worlds of uneven sizes render whole images");
+        ngb::require(first >= 0 && count >= 1 && static_cast<long long>(first) + count <= r.height,
+            "rows [" + std::to_string(first) + ", " + std::to_string(static_cast<long long>(first) + count) +
+            ") are not a non-empty range of the image's " + std::to_string(r.height) + " rows");
+        r.band_first = first;
+        r.band_rows = count == r.height ? 0 : count;
+    });
+}
+
+int ngb_rows(const ngb_renderer *h, int32_t *first, int32_t *count) {
+    if (!h || !first || !count) return NGB_INVALID_ARGUMENT;
+    *first = h->r.band_first;
+    *count = h->r.rows();
+    return NGB_OK;
+}
+
 int ngb_srgb_thresholds(float *thresholds) {
     if (!thresholds) return NGB_INVALID_ARGUMENT;
     ngb::srgb_thresholds(thresholds);
@@ -1398,6 +1422,8 @@ int ngb_depth_normal_adjoint(ngb_renderer *h, const float *matrices, const float
         a.aspect = static_cast<float>(r.width) / static_cast<float>(r.height);
         a.width = r.width;
         a.height = r.height;
+        a.row_first = r.band_first;
+        a.rows = r.rows();
         a.cameras_per_world = r.cpw;
         a.views = r.worlds * r.cpw;
         a.hit_instance = hit_instance;

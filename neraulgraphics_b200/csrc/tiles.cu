@@ -350,7 +350,7 @@ struct TileAt {
 
 __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view, int lane) {
     TileAt t;
-    int q;
+    int q, row0, row_end;  // the view's rendered rows [row0, row_end)
     long long first_pixel;
     if (a.view_info) {
         t.view = view_of(a.view_info, a.views, tile, true);
@@ -361,21 +361,25 @@ __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, i
         tiles_x = (v.x + TILE_W - 1) / TILE_W;
         q = static_cast<int>(tile - v.w);
         first_pixel = v.z;
+        row0 = 0;
+        row_end = v.y;
     } else {
         t.view = static_cast<int>(tile / tiles_per_view);
         t.width = a.width;
         t.height = a.height;
         t.aspect = a.aspect;
         q = static_cast<int>(tile % tiles_per_view);
-        first_pixel = static_cast<long long>(t.view) * a.height * a.width;
+        first_pixel = static_cast<long long>(t.view) * a.rows * a.width;
+        row0 = a.row_first;
+        row_end = a.row_first + a.rows;
     }
     t.x0 = (q % tiles_x) * TILE_W;
-    t.y0 = (q / tiles_x) * TILE_H;
+    t.y0 = row0 + (q / tiles_x) * TILE_H;
     t.x = t.x0 + (lane % TILE_W);
     t.y = t.y0 + lane / TILE_W;
-    t.pixel = t.x < t.width && t.y < t.height;
+    t.pixel = t.x < t.width && t.y < row_end;
     t.world = t.view / a.cameras_per_world;
-    t.pix = first_pixel + static_cast<long long>(t.y) * t.width + t.x;
+    t.pix = first_pixel + static_cast<long long>(t.y - row0) * t.width + t.x;
     return t;
 }
 
@@ -599,11 +603,11 @@ __device__ __forceinline__ bool shadow_misses_own_mesh(const SceneParams &s, int
 // the hit's code) for the shadow kernel. shadow_o.w = 0 marks a pixel without a shadow ray.
 __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ SceneParams s, const RenderArgs a,
     long long pixels) {
-    const long long per_view = static_cast<long long>(a.width) * a.height;
+    const long long per_view = static_cast<long long>(a.width) * a.rows;
     const float3 zero = mk3(0.0f, 0.0f, 0.0f);
     for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < pixels;
          p += static_cast<long long>(gridDim.x) * blockDim.x) {
-        int view, rem, width = a.width, height = a.height;
+        int view, rem, row0 = 0, width = a.width, height = a.height;
         float aspect = a.aspect;
         if (a.view_info) {
             view = view_of(a.view_info, a.views, p, false);
@@ -615,8 +619,9 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
         } else {
             view = static_cast<int>(p / per_view);
             rem = static_cast<int>(p % per_view);
+            row0 = a.row_first;
         }
-        const int y = rem / width, x = rem % width;
+        const int y = row0 + rem / width, x = rem % width;
         const int world = view / a.cameras_per_world;
         const float4 c0 = __ldg(a.camera_basis + 3 * view), c1 = __ldg(a.camera_basis + 3 * view + 1);
         const float4 c2 = __ldg(a.camera_basis + 3 * view + 2);
@@ -855,7 +860,7 @@ cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const
 template <int THREADS, int MIN_BLOCKS, int CAP>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream,
     cudaEvent_t after_camera, cudaEvent_t after_shade) {
-    const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
+    const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.rows + TILE_H - 1) / TILE_H;
     const int tiles_per_view = tiles_x * tiles_y;
     const long long tiles = a.view_info ? a.total_tiles : static_cast<long long>(tiles_per_view) * a.views;
     const bool aov = a.depth || a.normal || a.object_id || a.hit_instance;
@@ -877,7 +882,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         mark(after_shade);
         return e;
     }
-    const long long pixels = a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.height;
+    const long long pixels = a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.rows;
     int device = 0, sms = 0;
     e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);

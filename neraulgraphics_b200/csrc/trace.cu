@@ -21,13 +21,13 @@ using namespace tr;
 constexpr int TILE_W = 16, TILE_H = 8;
 
 __global__ void __launch_bounds__(128) render_kernel(const __grid_constant__ SceneParams s, const RenderArgs a) {
-    const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.height + TILE_H - 1) / TILE_H;
+    const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.rows + TILE_H - 1) / TILE_H;
     const int tiles = tiles_x * tiles_y;
     const int view = blockIdx.x / tiles, tile = blockIdx.x % tiles;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int x = (tile % tiles_x) * TILE_W + (warp & 1) * 8 + (lane & 7);
-    const int y = (tile / tiles_x) * TILE_H + (warp >> 1) * 4 + (lane >> 3);
-    if (view >= a.views || x >= a.width || y >= a.height) return;
+    const int y = a.row_first + (tile / tiles_x) * TILE_H + (warp >> 1) * 4 + (lane >> 3);
+    if (view >= a.views || x >= a.width || y >= a.row_first + a.rows) return;
     // camera_from_matrix (src/render_core.h:264-273); tan(fov / 2) and the aspect come from the host.
     const float *m = a.cameras + 12 * static_cast<size_t>(view);
     float cm[12];
@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(128) render_kernel(const __grid_constant__ Sce
     const float3 up = normalize(mk3(cm[1], cm[5], cm[9]));
     const float3 forward = normalize(mk3(-cm[2], -cm[6], -cm[10]));
     const int world = view / a.cameras_per_world;
-    const size_t pix = (static_cast<size_t>(view) * a.height + y) * a.width + x;
+    const size_t pix = (static_cast<size_t>(view) * a.rows + (y - a.row_first)) * a.width + x;
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
     // camera_ray (src/device_scene.h:114-119).
     auto camera_ray = [&](float px, float py) {
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *camer
 }  // namespace
 
 cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream) {
-    const long long tiles = static_cast<long long>((a.width + TILE_W - 1) / TILE_W) * ((a.height + TILE_H - 1) / TILE_H);
+    const long long tiles = static_cast<long long>((a.width + TILE_W - 1) / TILE_W) * ((a.rows + TILE_H - 1) / TILE_H);
     const long long blocks = tiles * a.views;
     if (blocks <= 0) return cudaSuccess;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

@@ -232,7 +232,7 @@ class BatchRenderer:
     def render(self, cameras, fov=1.0, samples_per_pixel=1, *, rgb=True, depth=False, normals=False,
                object_ids=False, frame=0, zero_copy=False, out=None, into=None):
         """Render every view; returns a dict of 'rgb' (V,H,W,3) uint8, 'depth' (V,H,W) float32, 'normals'
-        (V,H,W,3) float32, 'object_ids' (V,H,W) int32, for the images asked for.
+        (V,H,W,3) float32, 'object_ids' (V,H,W) int32, for the images asked for (H: the rows drawn, set_rows).
 
         out: optional dict of preallocated host (NumPy) arrays, pinned or not, to copy the images into
         (BatchRenderer::render_host, src/batch.cpp:164-178); cameras must then be on the host.
@@ -240,7 +240,7 @@ class BatchRenderer:
         device) to render into instead of the renderer's own buffers, queued on PyTorch's current stream (as
         zero_copy): the caller may then copy them out while the next render runs."""
         torch = _torch()
-        views, h, w = self.view_count, self.height, self.width
+        views, h, w = self.view_count, self.rows[1], self.width
         if out is not None:
             return self._render_host(cameras, fov, samples_per_pixel, rgb, depth, normals, object_ids, frame, out)
         _require_count(cameras, views * 12, "cameras", f"{views} cameras of 3 x 4 numbers (camera-to-world)")
@@ -279,7 +279,7 @@ class BatchRenderer:
         return host
 
     def _render_host(self, cameras, fov, spp, rgb, depth, normals, object_ids, frame, out):
-        views, h, w = self.view_count, self.height, self.width
+        views, h, w = self.view_count, self.rows[1], self.width
         _require_count(cameras, views * 12, "cameras", f"{views} cameras of 3 x 4 numbers (camera-to-world)")
         if _is_cuda_tensor(cameras):
             raise ValueError("render(out=...) copies to host memory and takes cameras in host memory")
@@ -355,6 +355,27 @@ class BatchRenderer:
         return int(self._lib.ngb_height(self._h))
 
     @property
+    def pixel_count(self) -> int:
+        """Pixels of one output image of every view: views x rows drawn x width (uneven worlds: their sum)."""
+        return int(self._lib.ngb_pixel_count(self._h))
+
+    @property
+    def rows(self) -> tuple:
+        """(first, count): the image rows every render draws (set_rows); (0, height) for the whole image."""
+        first, count = C.c_int32(0), C.c_int32(0)
+        check(self._lib.ngb_rows(self._h, C.byref(first), C.byref(count)), self._h)
+        return int(first.value), int(count.value)
+
+    def set_rows(self, first=0, count=None):
+        """Later renders draw image rows [first, first + count) of every view (count None: to the last row;
+        set_rows() is the whole image again). Every pixel is the whole image's (the same rays and random
+        streams); the outputs, hit records and the adjoint's per-pixel inputs hold (views, count, width). For
+        splitting one large picture across GPUs by rows (sharding.ShardedFrame)."""
+        if count is None:
+            count = self.height - int(first)
+        check(self._lib.ngb_set_rows(self._h, int(first), int(count)), self._h)
+
+    @property
     def world_count(self) -> int:
         return int(self._lib.ngb_world_count(self._h))
 
@@ -417,7 +438,7 @@ class BatchRenderer:
             check(self._lib.ngb_record_hits(self._h, 1 if on else 0), self._h)
             return
         torch = _torch()
-        shape = (self.view_count, self.height, self.width)
+        shape = (self.view_count, self.rows[1], self.width)
         for t, dt in zip(into, (torch.int32, torch.int32, torch.float32, torch.float32)):
             if (not _is_cuda_tensor(t) or tuple(t.shape) != shape or t.dtype != dt or not t.is_contiguous() or
                     t.device.index != self._device):
@@ -456,7 +477,7 @@ class BatchRenderer:
                                                  ptr(grad_cameras)), self._h)
 
     def inspect_hits(self) -> dict:
-        shape = (self.view_count, self.height, self.width)
+        shape = (self.view_count, self.rows[1], self.width)
         inst, tri = np.zeros(shape, np.int32), np.zeros(shape, np.int32)
         u, v = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
         vp = lambda a: a.ctypes.data_as(C.c_void_p)
@@ -493,10 +514,6 @@ class UnevenBatchRenderer(BatchRenderer):
         self._rays = {}
         self.pixel_first = np.concatenate([[0], np.cumsum([w * hh for w, hh in self._sizes])]).astype(np.int64)
         self.instance_first = np.concatenate([[0], np.cumsum(self._counts)]).astype(np.int64)
-
-    @property
-    def pixel_count(self) -> int:
-        return int(self._lib.ngb_pixel_count(self._h))
 
     @property
     def instance_count(self) -> int:

@@ -28,6 +28,20 @@ def world_range(world_count: int, rank: int, world_size: int) -> tuple[int, int]
     return start, start + base + (1 if rank < extra else 0)
 
 
+def row_range(height: int, rank: int, world_size: int, tile: int = 4) -> tuple[int, int]:
+    """(first, count) of rank's rows of an image height rows tall: contiguous bands of whole tiles of `tile`
+    rows (the render kernels' tile height), in rank order, whose tile counts differ by at most one; the last
+    band ends at the image's last row. Every rank gets at least one row."""
+    if height < 1:
+        raise ValueError(f"height must be 1 or more, got {height}")
+    tiles = (height + tile - 1) // tile
+    if tiles < world_size:
+        raise ValueError(f"{world_size} ranks cannot share {tiles} tiles of {tile} rows ({height} rows)")
+    start, stop = world_range(tiles, rank, world_size)
+    first = start * tile
+    return first, min(stop * tile, height) - first
+
+
 class _Group:
     """The process group's rank and size (one rank when torch.distributed is not initialised)."""
 
@@ -38,6 +52,14 @@ class _Group:
             self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
         else:
             self.rank, self.size = 0, 1
+
+    def broadcast(self, tensor, src: int = 0):
+        """tensor as rank src holds it, on every rank, in place (the scene's inputs replicated from one rank:
+        every rank then builds the same tree). Returns tensor."""
+        import torch.distributed as dist
+        if self.size > 1:
+            dist.broadcast(tensor, src, group=self.group)
+        return tensor
 
 
 class ShardedWorlds:
@@ -138,3 +160,61 @@ class ShardedRays(_Group):
         pieces = [torch.empty_like(piece) for _ in range(self.size)]
         dist.all_gather(pieces, piece, group=self.group)
         return torch.cat([p[:, :b - a] for p, (a, b) in zip(pieces, self.ranges)], 1)
+
+
+class ShardedFrame(_Group):
+    """This rank's band of rows of every view's image: for one large picture (or a few) split across GPUs.
+    Every rank holds the whole scene (the same instance matrices, so the same tree; broadcast() replicates
+    them from one rank) and renders rows [first, first + count) of each view (BatchRenderer.set_rows), with
+    the whole image's rays and random streams, so the joined bands are the whole image's pixels exactly.
+    Bands are whole tiles of 4 rows; nothing is exchanged until the gather.
+
+        shard = ShardedFrame(height=720)
+        shard.apply(r)                                                   # r.set_rows(shard.first, shard.count)
+        images = r.render(cams, zero_copy=True, rgb=True, depth=True)    # (views, shard.count, 1280, ...)
+        everything = {k: shard.gather(v) for k, v in images.items()}     # (views, 720, 1280, ...) on every rank
+    """
+
+    def __init__(self, height: int, group=None):
+        super().__init__(group)
+        self.height = height
+        self.ranges = [row_range(height, r, self.size) for r in range(self.size)]
+        self.first, self.count = self.ranges[self.rank]
+
+    def apply(self, renderer) -> None:
+        """Sets renderer to draw this rank's rows."""
+        if renderer.height != self.height:
+            raise ValueError(f"the renderer's images are {renderer.height} rows tall, the frame {self.height}")
+        renderer.set_rows(self.first, self.count)
+
+    def take(self, per_pixel):
+        """This rank's rows of an array or tensor shaped (views, height, ...)."""
+        if per_pixel.shape[1] != self.height:
+            raise ValueError(f"expected {self.height} rows on the second axis, got {per_pixel.shape[1]}")
+        return per_pixel[:, self.first:self.first + self.count]
+
+    def gather(self, local):
+        """Every rank's (views, its rows, ...) tensor joined along the rows in image order, on every rank: one
+        all-gather of pieces padded to the largest band."""
+        import torch
+        import torch.distributed as dist
+        if local.shape[1] != self.count:
+            raise ValueError(f"expected this rank's {self.count} rows on the second axis, got {local.shape[1]}")
+        if self.size == 1:
+            return local
+        pad = max(c for _, c in self.ranges)
+        piece = torch.zeros((local.shape[0], pad) + tuple(local.shape[2:]), dtype=local.dtype, device=local.device)
+        piece[:, :local.shape[1]] = local
+        pieces = [torch.empty_like(piece) for _ in range(self.size)]
+        dist.all_gather(pieces, piece, group=self.group)
+        return torch.cat([p[:, :c] for p, (_, c) in zip(pieces, self.ranges)], 1)
+
+    def max_over_ranks(self, value: float, device=None) -> float:
+        """The largest value over the ranks (a time: the frame takes as long as its slowest band)."""
+        import torch
+        import torch.distributed as dist
+        if self.size == 1:
+            return float(value)
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+        return float(t.item())
