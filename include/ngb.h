@@ -319,6 +319,16 @@ int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, i
  * reference, which always runs its global build. */
 int ngb_set_build(ngb_renderer *r, int32_t mode);
 
+/* Bytes of device memory held by every renderer of the process (their device arrays; not the caller's). */
+int64_t ngb_device_bytes(void);
+/* Testing: host-side fault injection. The after-th device allocation from now on, by any renderer (0: the next
+ * one), fails as cudaMalloc does for lack of memory: the call that made it returns NGB_CUDA_ERROR ("out of
+ * memory"). A renderer under construction is not made and frees all it made; a renderer stays usable (a failed
+ * set_* call leaves the previous tree in place, a failed render leaves its outputs unwritten) and keeps the
+ * arrays it made before the failure for its next call. after < 0 cancels. No GPU fault is involved. No
+ * counterpart in the reference. */
+int ngb_inject_allocation_failure(int32_t after);
+
 /* The rows every later render draws: image rows [first, first + count) of every view, count >= 1 and
  * first + count <= height; (0, height) is the whole image again (the default). The rays, their random streams
  * and so every pixel are the whole image's; the outputs (and ngb_pixel_count, the hit records and the

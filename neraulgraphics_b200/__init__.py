@@ -22,6 +22,19 @@ from .scene import (Camera, Environment, Instance, Light, Material, Mesh, Plane,
 __version__ = "0.1.0"
 
 
+def device_bytes() -> int:
+    """Bytes of device memory held by every renderer of the process (ngb_device_bytes)."""
+    from ._lib import lib
+    return int(lib().ngb_device_bytes())
+
+
+def inject_allocation_failure(after: int = 0) -> None:
+    """Testing: the after-th device allocation from now on fails as an out-of-memory cudaMalloc would (the call
+    raises CudaError and the renderer stays usable); after < 0 cancels (ngb_inject_allocation_failure)."""
+    from ._lib import lib
+    lib().ngb_inject_allocation_failure(int(after))
+
+
 def cuda_available() -> bool:
     """True when a CUDA GPU is present (there is no CPU backend)."""
     try:

@@ -78,6 +78,9 @@ def lib():
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
     L.ngb_set_rows.argtypes = [_vp, C.c_int32, C.c_int32]
+    L.ngb_device_bytes.argtypes = []
+    L.ngb_device_bytes.restype = C.c_int64
+    L.ngb_inject_allocation_failure.argtypes = [C.c_int32]
     L.ngb_rows.argtypes = [_vp, _i32p, _i32p]
     L.ngb_copy_hits.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.ngb_depth_normal_adjoint.argtypes = [_vp, _vp, _vp, C.c_float] + [_vp] * 9

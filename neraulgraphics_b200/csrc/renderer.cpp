@@ -1,6 +1,7 @@
 // The renderer behind the C ABI (include/ngb.h): validation, device buffers, the stream, launches and
 // bounded waits. Replaces BatchRenderer (src/batch.cpp) over CudaBackend (src/cuda_backend.cu:325-793).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
@@ -13,6 +14,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "host.h"
 #include "kernels.h"
@@ -42,6 +44,26 @@ std::string device_error_message(int code) {
 
 namespace {
 
+// A named range around a call's host work and launches on Nsight timelines (nothing without a tool attached).
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+
+// Bytes held by every renderer's device arrays, and the host-side allocation-failure injection for tests:
+// the value-th device allocation from now on fails (0: the next one), -1 none.
+std::atomic<long long> g_device_bytes{0};
+std::atomic<long long> g_fail_allocation{-1};
+
+bool injected_allocation_failure() {
+    long long v = g_fail_allocation.load();
+    while (v >= 0)
+        if (g_fail_allocation.compare_exchange_weak(v, v - 1)) return v == 0;
+    return false;
+}
+
 // A device array, grown on demand and freed with its owner.
 template <class T>
 struct DevBuf {
@@ -52,16 +74,24 @@ struct DevBuf {
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            g_device_bytes -= static_cast<long long>(n * sizeof(T));
+        }
         p = nullptr;
         n = 0;
     }
+    // At least count elements; the old contents are not kept when it grows.
     T *ensure(size_t count) {
         if (count == 0) return p;
         if (p && count <= n) return p;
         release();
+        if (injected_allocation_failure())
+            cuda_fail(cudaErrorMemoryAllocation, "cudaMalloc (a failure injected by ngb_inject_allocation_failure)",
+                __FILE__, __LINE__);
         CK(cudaMalloc(&p, count * sizeof(T)));
         n = count;
+        g_device_bytes += static_cast<long long>(n * sizeof(T));
         return p;
     }
 };
@@ -177,6 +207,7 @@ struct Renderer {
     DevBuf<int> error_flag;
     int *host_error = nullptr;  // pinned: the device error flag, copied back where the host waits for the work
 
+    bool cuda_touched = false;  // set before the first CUDA call of the constructor
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr, ev_done = nullptr;
     cudaEvent_t ev_stage[2] = {nullptr, nullptr};  // between the tile render's camera, shade and shadow kernels
@@ -196,6 +227,8 @@ struct Renderer {
 
     explicit Renderer(const ngb_scene &s, const UnevenLayout *layout = nullptr);
     ~Renderer();
+    void init(const ngb_scene &s, const UnevenLayout *layout);
+    void teardown();
 
     void build(const float *matrices_in, int compose, const float *poses, const float *xmat = nullptr);
     void queue_error_read();
@@ -230,7 +263,19 @@ struct Renderer {
     }
 };
 
+// A constructor that fails part way frees what it made (src/cuda_backend.cu:210-323 does the same).
 Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
+    try {
+        init(s, layout);
+    } catch (...) {
+        teardown();
+        throw;
+    }
+}
+
+Renderer::~Renderer() { teardown(); }
+
+void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
     if (layout) {
         // The shared scene is checked as it is; each world's image and instance range on their own.
         uneven = true;
@@ -284,6 +329,7 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
         n = static_cast<long long>(worlds) * per_world;
     }
     DeviceGuard guard(device);
+    cuda_touched = true;
     CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
     CK(cudaEventCreate(&ev_start));
@@ -484,20 +530,27 @@ Renderer::Renderer(const ngb_scene &s, const UnevenLayout *layout) {
     wait(ev_done, timeout);
 }
 
-Renderer::~Renderer() {
-    // Destructors must not throw; errors after a sticky fault are ignored.
+// Frees everything; safe on a renderer whose construction stopped part way, and twice.
+void Renderer::teardown() {
+    // Must not throw; errors after a sticky fault are ignored. Nothing to free before the first CUDA call.
+    if (!cuda_touched) return;
     int previous = -1;
     cudaGetDevice(&previous);
     if (previous != device) cudaSetDevice(device);
     if (own_stream) cudaStreamSynchronize(own_stream);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
-    for (cudaEvent_t e : ev_stage)
+    for (cudaEvent_t &e : ev_stage) {
         if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
     if (ev_done) cudaEventDestroy(ev_done);
     if (host_error) cudaFreeHost(host_error);
     if (host_count) cudaFreeHost(host_count);
     if (own_stream) cudaStreamDestroy(own_stream);
+    ev_start = ev_stop = ev_done = nullptr;
+    host_error = host_count = nullptr;
+    own_stream = nullptr;
     // The DevBufs free themselves; the device must be current while they do, so release them here.
     blas.release(), tris.release(), attrs.release(), tri_index.release(), slot_blas_root.release();
     tri_of_local.release(), slot_tri_base.release();
@@ -519,6 +572,7 @@ Renderer::~Renderer() {
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
     hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
+    world_first.release(), view_info.release();
     if (previous >= 0 && previous != device) cudaSetDevice(previous);
 }
 
@@ -620,6 +674,7 @@ void Renderer::build(const float *matrices_in, int compose, const float *poses, 
 
 // src/batch.cpp:91-109 and src/cuda_backend.cu:457-469.
 void Renderer::set_instance_transforms(const float *m, int memory) {
+    Range range("ngb set_instance_transforms");
     require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
     if (n == 0) return;
     require(m != nullptr, "matrices must not be null");
@@ -674,6 +729,7 @@ void Renderer::bind_bodies(int bpw, const int32_t *boi, const float *lp, const f
 
 // src/batch.cpp:131-144 and src/cuda_backend.cu:493-507.
 void Renderer::set_body_poses(const float *poses, int memory) {
+    Range range("ngb set_body_poses");
     require(bound, "set_body_poses needs bind_bodies to be called first");
     require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
     const size_t bodies = static_cast<size_t>(worlds) * bodies_per_world;
@@ -725,6 +781,7 @@ void Renderer::bind_geoms(int gpw, const int32_t *goi, const float *sc) {
 
 // MJWarpBatchRenderer.update (python/neraulgraphics/mujoco.py:304-314): compose and build in one launch.
 void Renderer::set_geom_poses(const float *xpos, const float *xmat, int memory) {
+    Range range("ngb set_geom_poses");
     require(geoms_bound, "set_geom_poses needs bind_geoms to be called first");
     require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
     const size_t geoms = static_cast<size_t>(worlds) * geoms_per_world;
@@ -749,6 +806,7 @@ void Renderer::set_geom_poses(const float *xpos, const float *xmat, int memory) 
 // (src/bvh.cpp:46-174, src/mesh_build.cpp:91-157), then every world's instance tree from the current
 // transforms, whose boxes hold the mesh's new box.
 void Renderer::update_mesh(int mesh, const float *vertices, const float *normals, int memory) {
+    Range range("ngb update_mesh");
     require(mesh >= 0 && mesh < static_cast<int>(mesh_tris.size()),
         "mesh " + std::to_string(mesh) + " does not exist: there are " + std::to_string(mesh_tris.size()) + " meshes");
     require(memory == NGB_MEMORY_HOST || memory == NGB_MEMORY_DEVICE, "memory must be NGB_MEMORY_HOST or NGB_MEMORY_DEVICE");
@@ -836,6 +894,7 @@ void Renderer::check_render(const float *cams, float fov, int spp, unsigned outp
 
 void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
     float *depth, float *normal, int32_t *ids) {
+    Range range("ngb render");
     const int views = worlds * cpw;
     const float *cam = cams;
     if (memory == NGB_MEMORY_HOST) {
@@ -920,6 +979,7 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
 // src/batch.cpp:180-192 and src/cuda_backend.cu:547-585.
 void Renderer::cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory,
     ngb_ray_hits *out, float *distance, float *normal, int32_t *ids) {
+    Range range("ngb cast_rays");
     require(rays_per_world >= 0, "rays_per_world must be 0 or more, got " + std::to_string(rays_per_world));
     const long long count = static_cast<long long>(rays_per_world) * worlds;
     require(count <= INT32_MAX / 3, "too many rays: " + std::to_string(count));
@@ -1337,6 +1397,13 @@ int ngb_set_build(ngb_renderer *h, int32_t mode) {
     });
 }
 
+int ngb_inject_allocation_failure(int32_t after) {
+    ngb::g_fail_allocation = after < 0 ? -1 : after;
+    return NGB_OK;
+}
+
+int64_t ngb_device_bytes(void) { return ngb::g_device_bytes.load(); }
+
 int ngb_set_rows(ngb_renderer *h, int32_t first, int32_t count) {
     return guarded(h, [&](ngb::Renderer &r) {
         ngb::require(!r.uneven, "worlds of uneven sizes render whole images");
@@ -1437,6 +1504,7 @@ int ngb_depth_normal_adjoint(ngb_renderer *h, const float *matrices, const float
         a.grad_cameras = grad_cameras;
         a.tri_of_local = r.tri_of_local.p;
         a.slot_tri_base = r.slot_tri_base.p;
+        ngb::Range range("ngb depth_normal_adjoint");
         CK(cudaEventRecord(r.ev_start, r.stream));
         CK(ngb::launch_depth_normal_adjoint(r.params, a, r.stream));
         CK(cudaEventRecord(r.ev_stop, r.stream));
