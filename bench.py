@@ -396,6 +396,8 @@ def run_ours(args, rank, world, local_rank, dist):
         "gpu_launches": (2 + (4 if len(stage_ms) == 3 else 2)) * K,
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
                                                                             "leaf_batch", "ms")},
+        # The renderers' own device arrays (scene, trees, per-pixel scratch; ngb_device_bytes), not the images.
+        "device_mb": round(ng.device_bytes() / 1e6, 1),
         "clocks": clk,
     }
 
