@@ -43,7 +43,8 @@ def row_range(height: int, rank: int, world_size: int, tile: int = 4) -> tuple[i
 
 
 class _Group:
-    """The process group's rank and size (one rank when torch.distributed is not initialised)."""
+    """The process group's rank and size (one rank when torch.distributed is not initialised), and the
+    collectives every split uses."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
@@ -61,18 +62,23 @@ class _Group:
             dist.broadcast(tensor, src, group=self.group)
         return tensor
 
+    def max_over_ranks(self, value: float, device=None) -> float:
+        """The largest value over the ranks (a time: the job takes as long as its slowest rank)."""
+        import torch
+        import torch.distributed as dist
+        if self.size == 1:
+            return float(value)
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
+        return float(t.item())
 
-class ShardedWorlds:
+
+class ShardedWorlds(_Group):
     """This rank's share of world_count worlds in a torch.distributed process group (the default group when
     group is None; one rank when torch.distributed is not initialised)."""
 
     def __init__(self, world_count: int, group=None):
-        import torch.distributed as dist
-        self.group = group
-        if dist.is_available() and dist.is_initialized():
-            self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
-        else:
-            self.rank, self.size = 0, 1
+        super().__init__(group)
         self.world_count = world_count
         self.start, self.stop = world_range(world_count, self.rank, self.size)
         self.ranges = [world_range(world_count, r, self.size) for r in range(self.size)]
@@ -108,16 +114,6 @@ class ShardedWorlds:
         pieces = [torch.empty_like(piece) for _ in range(self.size)]
         dist.all_gather(pieces, piece, group=self.group)
         return torch.cat([p[:int(r[0])] for p, r in zip(pieces, all_rows)], 0)
-
-    def max_over_ranks(self, value: float, device=None) -> float:
-        """The largest value over the ranks (a time: the job takes as long as its slowest rank)."""
-        import torch
-        import torch.distributed as dist
-        if self.size == 1:
-            return float(value)
-        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
-        return float(t.item())
 
 
 class ShardedRays(_Group):
@@ -208,13 +204,3 @@ class ShardedFrame(_Group):
         pieces = [torch.empty_like(piece) for _ in range(self.size)]
         dist.all_gather(pieces, piece, group=self.group)
         return torch.cat([p[:, :c] for p, (_, c) in zip(pieces, self.ranges)], 1)
-
-    def max_over_ranks(self, value: float, device=None) -> float:
-        """The largest value over the ranks (a time: the frame takes as long as its slowest band)."""
-        import torch
-        import torch.distributed as dist
-        if self.size == 1:
-            return float(value)
-        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=self.group)
-        return float(t.item())
