@@ -14,7 +14,8 @@ collective on the data path); the time is the max over ranks.
 value: device-resident inputs (poses and cameras already on the GPU), CUDA events per step, L2 flushed
 between steps. e2e: the public API with host buffers: pinned host poses in, images copied back to pinned
 host memory, every step. --impl reference times the reference's own CPU backend (compiled from its sources
-into oracle/_ref/) on a bounded sample of worlds per step, with every host core.
+into oracle/_ref/) on a bounded sample of worlds per step, with every host core, and reports beside it the
+reference's CUDA backend (built the same way) on the whole workload on the GPU ("reference_cuda").
 """
 
 from __future__ import annotations
@@ -46,7 +47,8 @@ def parse():
     p.add_argument("--worlds", type=int, default=4096)
     p.add_argument("--e2e-steps", type=int, default=10)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
-    p.add_argument("--no-reference-cuda", action="store_true")
+    p.add_argument("--no-reference-cuda", action="store_true",
+                   help="--impl reference: skip timing the reference's CUDA backend on the GPU")
     p.add_argument("--no-autotune", action="store_true", help="use the library's default kernel shape")
     p.add_argument("--config", default="body_worlds",
                    choices=["body_worlds", "large_world", "differentiable", "uneven", "mesh_update"],
@@ -158,29 +160,25 @@ def camera_kernel_algorithmic_bytes(wl, per_world, blas_bytes):
     return out + cams + trees + blas_bytes
 
 
-def rays_per_image(wl, sample=16):
-    """Rays the path traces per image (a centre ray and a picture ray per pixel, and a shadow ray per lit
-    picture hit), counted by the oracle on the first sample worlds."""
+def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64, count_worlds=16):
+    """The reference's own CPU backend (oracle/_ref/libngref.so) on the first sample_worlds worlds of the
+    workload, every host core: images/s. The CPU leg also renders the first count_worlds worlds with the
+    instrumented port (oracle/), which counts the rays the path traces per image (a centre ray and a picture
+    ray per pixel, a shadow ray per lit picture hit) and the bytes their walks fetch (32 per node, 64 per
+    child-box pair, 48 per instance inverse, 48 per triangle): returned beside the timing as "counts"."""
     import oracle as O
     from neraulgraphics_b200.scene import SceneDesc
     d = wl.desc
-    desc = SceneDesc(d.width, d.height, sample, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    desc = SceneDesc(d.width, d.height, count_worlds, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
     o = O.Oracle(desc)
     o.bind_bodies(**wl.binding)
-    o.set_body_poses(wl.poses[:sample])
-    o.render(wl.cameras[:sample], wl.fov, 1, rgb=True, depth=True, object_ids=True)
-    _, rays = o.traversal_bytes()
-    return rays / sample
-
-
-def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64):
-    """The reference's own CPU backend (oracle/_ref/libngref.so) on the first sample_worlds worlds of the
-    workload, every host core: images/s."""
-    import oracle as O
-    from neraulgraphics_b200.scene import SceneDesc
+    o.set_body_poses(wl.poses[:count_worlds])
+    o.render(wl.cameras[:count_worlds], wl.fov, 1, rgb=True, depth=True, object_ids=True)
+    walked, rays = o.traversal_bytes()
+    counts = {"rays_per_image": rays / count_worlds, "traversal_bytes_per_image": walked / count_worlds,
+              "sample": f"the first {count_worlds} worlds, step 0 poses"}
     if not O.reference_available():
-        return None
-    d = wl.desc
+        return {"unavailable": "oracle/_ref was not built", "counts": counts}
     desc = SceneDesc(d.width, d.height, sample_worlds, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
     cores = os.cpu_count() or 1
     ref = O.Reference(desc, threads=cores)
@@ -198,7 +196,7 @@ def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64):
             break
     return {"value": sample_worlds * n / el, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"{n} steps of {sample_worlds} of the {d.world_count} worlds (set_body_poses + render_host, "
-                      f"RGB+depth+ID), NERAULGRAPHICS_THREADS={cores}, {el:.1f} s"}
+                      f"RGB+depth+ID), NERAULGRAPHICS_THREADS={cores}, {el:.1f} s", "counts": counts}
 
 
 def reference_cuda(wl, torch, poses_dev, cams_dev, steps, warmup):
@@ -348,12 +346,7 @@ def run_ours(args, rank, world, local_rank, dist):
     h2d = pinned_poses[0].numel() * 4 + wl.cameras.nbytes
     d2h = sum(a.numel() * a.element_size() for a in out.values())
 
-    ref_cuda = cpu = None
-    if rank == 0 and not args.no_reference_cuda:
-        try:
-            ref_cuda = reference_cuda(wl, torch, poses_dev, cams_dev, min(K, 10), min(W, 3))
-        except Exception as e:  # reported, not fatal: the comparison arm is optional
-            ref_cuda = {"unavailable": f"{type(e).__name__}: {e}"}
+    cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(wl, steps_np, args.cpu_seconds)
 
@@ -366,7 +359,8 @@ def run_ours(args, rank, world, local_rank, dist):
     rmed = statistics.median(render_ms)
     cam_ms = stage_ms[0]
     achieved = alg / (cam_ms / 1000.0) / 1e9
-    rpi = rays_per_image(wl)
+    counts = (cpu or {}).get("counts")
+    rpi = counts["rays_per_image"] if counts else None
     tr = traffic_per_image()
     clk = clocks.summary()
     return {
@@ -379,8 +373,14 @@ def run_ours(args, rank, world, local_rank, dist):
                       "render": round(rmed, 4),
                       **({"camera_rays": round(stage_ms[0], 4), "shading": round(stage_ms[1], 4),
                           "shadow_rays": round(stage_ms[2], 4)} if len(stage_ms) == 3 else {})},
-        "rays_per_s": round(value * rpi, 1),
-        "rays_per_image": round(rpi, 1),
+        "rays_per_s": None if rpi is None else round(value * rpi, 1),
+        "rays_per_image": None if rpi is None else round(rpi, 1),
+        # The bytes the walks fetch (nodes, child-box pairs, instance inverses, triangles), almost all from L1/L2:
+        # per image as counted on the same walks, and that rate over the measured HBM peak (above 1 shows reuse).
+        "traversal": None if not counts else {
+            "bytes_per_image": round(counts["traversal_bytes_per_image"], 1),
+            "achieved_gbs": round(counts["traversal_bytes_per_image"] * value / 1e9, 1),
+            "frac_of_hbm_peak": round(counts["traversal_bytes_per_image"] * value / 1e9 / peak, 3)},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": KE, "path": "pinned host poses and cameras -> device (copy) -> BatchRenderer.set_body_poses + render(into= one of "
                         "two device image sets) -> pinned host images on a copy stream, overlapping the next step"},
@@ -390,7 +390,6 @@ def run_ours(args, rank, world, local_rank, dist):
                      "kernel": "camera_tiles_kernel", "kernel_ms": round(cam_ms, 4),
                      "algorithmic_bytes_per_launch": int(alg)},
         "cpu_baseline": cpu,
-        "reference_cuda": ref_cuda,
         # Per step: the tree build (compose + per-world build, inter-world links) and the render: the camera-basis
         # kernel and the camera, shade and shadow kernels (tile path), or the camera-basis and one render kernel.
         "gpu_launches": (2 + (4 if len(stage_ms) == 3 else 2)) * K,
@@ -463,12 +462,6 @@ def run_large(args, rank, world, local_rank, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     hit_frac = float((hits["object_id"] > 0).float().mean())
-    ref = None
-    if rank == 0 and not args.no_reference_cuda:
-        try:
-            ref = reference_cuda_large(wl, torch, mats, cams, lo_all, ld_all, min(K, 5), min(W, 2))
-        except Exception as e:  # reported, not fatal
-            ref = {"unavailable": f"{type(e).__name__}: {e}"}
     if rank != 0:
         return None
     rays = lo.shape[1]  # this rank's share (all of them on one GPU)
@@ -491,7 +484,6 @@ def run_large(args, rank, world, local_rank, dist):
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
                                                                             "leaf_batch", "ms")},
         "lidar_hit_fraction": round(hit_frac, 4),
-        "reference_cuda": ref,
         "clocks": clocks.summary(),
     }
 
@@ -819,14 +811,35 @@ def run_mesh_update(args, rank, world, local_rank, dist):
     }
 
 
+def reference_cuda_arm(run, what):
+    """run(torch) on cuda:0 when a GPU is present: the reference's own CUDA backend (built from its sources into
+    oracle/_ref) timed on the same workload, reported beside the reference arm's CPU figure."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+        torch.cuda.set_device(0)
+        out = run(torch)
+        return out if out is not None else {"unavailable": f"oracle/_ref was built without CUDA ({what})"}
+    except Exception as e:  # reported, not fatal: the CPU figure is the arm's value
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
 def run_reference(args, rank):
-    """The reference's own CPU implementation, rank 0 only, with every host core."""
+    """The reference's own CPU implementation, rank 0 only, with every host core; and, beside it, the reference's
+    CUDA backend on the GPU on the same workload (reference_cuda)."""
     from neraulgraphics_b200 import workloads
     import oracle as O
     if rank != 0:
         return None
     if not O.reference_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libngref.so is not built (make -C oracle ref)"}
+    if args.config == "large_world":
+        return run_reference_large(args)
+    if args.config != "body_worlds":
+        return {"impl": "reference", "unavailable": f"--config {args.config} has no reference arm: the reference "
+                "has no gradients, no uneven worlds and no device mesh build (its host build is this config's "
+                "cpu_baseline)"}
     from neraulgraphics_b200.scene import SceneDesc
     wl = workloads.body_worlds(worlds=args.worlds, seed=0)
     sample = 64
@@ -855,6 +868,76 @@ def run_reference(args, rank):
         "cpu_baseline": {"value": round(value, 2), "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{sample} worlds per step, {args.steps} steps, neraulgraphics 0.5.0 CPU backend"},
         "e2e": {"value": round(value, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": None if args.no_reference_cuda else reference_cuda_arm(
+            lambda torch: reference_cuda_body(args, torch), "body_worlds"),
+    }
+
+
+def reference_cuda_body(args, torch):
+    """The reference's CUDA backend on the whole body_worlds workload: the same seeded poses and cameras on the
+    device as the other arm's timed steps."""
+    from neraulgraphics_b200 import workloads
+    wl = workloads.body_worlds(worlds=args.worlds, seed=0)
+    K, W = min(args.steps, 10), min(args.warmup, 3)
+    poses = torch.from_numpy(workloads.random_walk(wl.poses, W + K, seed=1)).cuda()
+    cams = torch.from_numpy(wl.cameras).cuda()
+    return reference_cuda(wl, torch, poses, cams, K, W)
+
+
+def run_reference_large(args):
+    """The reference's CPU backend on the large world (one world of 100,000 instances: matrices in, its host
+    tree build, 1280x720 RGB+depth+ID, the 64x2048 LiDAR sweep), every host core, on a bounded sample of each
+    frame: a full frame takes it about ten minutes (0.7 ms per pixel, 0.8 ms per LiDAR ray on 8 cores), so it
+    renders the frame at 64x36 (the same camera and aspect, 1/400 of the pixels) and casts every 128th LiDAR
+    ray, and the frame's time is extrapolated from those per-pixel and per-ray costs. Its CUDA backend runs
+    the whole frames on the GPU."""
+    from neraulgraphics_b200 import workloads
+    from neraulgraphics_b200.scene import SceneDesc
+    import oracle as O
+    K, W = min(args.steps, 2), min(args.warmup, 1)
+    wl = workloads.large_world(seed=0, frames=W + K)
+    d = wl.desc
+    lidar = wl.info["lidar"]
+    cores = os.cpu_count() or 1
+    sw, sh, every = 64, 36, 128
+    small = SceneDesc(sw, sh, 1, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    ref = O.Reference(small, threads=cores)
+    lo_s = np.ascontiguousarray(lidar["origins"][:, ::every])
+    ld_s = np.ascontiguousarray(lidar["directions"][:, ::every])
+    pixel_scale = (d.width * d.height) / (sw * sh)
+    ray_scale = lidar["origins"].shape[1] / lo_s.shape[1]
+    frame_s = []
+    for s in range(W + K):
+        t0 = time.perf_counter()
+        ref.set_instance_transforms(wl.matrices[s])
+        t1 = time.perf_counter()
+        ref.render(wl.cameras, wl.fov, 1, rgb=True, depth=True, object_ids=True)
+        t2 = time.perf_counter()
+        ref.cast_rays(lo_s, ld_s, lidar["max_distance"])
+        t3 = time.perf_counter()
+        if s >= W:
+            frame_s.append((t1 - t0) + (t2 - t1) * pixel_scale + (t3 - t2) * ray_scale)
+    value = 1.0 / statistics.median(frame_s)
+
+    def cuda(torch):
+        mats = torch.from_numpy(wl.matrices).cuda()
+        cams = torch.from_numpy(wl.cameras).cuda()
+        lo, ld = torch.from_numpy(lidar["origins"]).cuda(), torch.from_numpy(lidar["directions"]).cuda()
+        return reference_cuda_large(wl, torch, mats, cams, lo, ld, K, W)
+
+    return {
+        "impl": "reference", "metric": "frames/s at 1 world x 100,000 instances, 1280x720 RGB+depth+ID + 64x2048 "
+        "LiDAR, matrices redrawn and tree rebuilt every frame", "value": round(value, 6), "unit": "frames/s",
+        "n_gpus": args.gpus, "steps": K, "warmup": W, "ms_per_step": round(1000 / value, 1),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded large_world scene)",
+        "config": {"workload": "large_world: 1 world x 100,000 instances, 1280x720, 64x2048 LiDAR, max range 150"},
+        "cpu_baseline": {"value": round(value, 6), "unit": "frames/s", "cores": cores, "kind": "reference",
+                         "sample": f"{K} frames after {W} warm-up, neraulgraphics 0.5.0 CPU backend: "
+                                   f"set_instance_transforms in full, render_host at {sw}x{sh} (x{pixel_scale:.0f}) "
+                                   f"and every {every}th LiDAR ray (x{ray_scale:.0f}), extrapolated to whole frames"},
+        "e2e": {"value": round(value, 6), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": None if args.no_reference_cuda else reference_cuda_arm(cuda, "large_world"),
     }
 
 
