@@ -1,9 +1,11 @@
-// The tile render kernel: the batched path's common case (one sample per pixel, at most one light, no mirror
-// bounces) for worlds of at most 32 instances, which is what a batch of small simulator worlds holds.
+// The tile render kernels: the batched path's common case (one sample per pixel, at most one light, no mirror
+// bounces), in three launches (camera rays, shading, shadow rays), for worlds of any size: candidate lists for
+// worlds of up to TILE_MAX_INSTANCES instances (what a batch of simulator worlds holds), a packet walk of the
+// world tree above that.
 //
 // One warp renders an 8 x 4 pixel tile of one view. All 32 rays of a tile start at the same eye and point into
-// the same narrow pyramid, and a small world has at most one instance per lane, so the warp replaces the world
-// tree's walk by one conservative test per instance:
+// the same narrow pyramid, so in a world of up to TILE_MAX_INSTANCES instances the warp replaces the world
+// tree's walk by one conservative test per instance, 32 instances at a time:
 //   - lane j tests instance j's world box against the tile's pyramid (four planes through the eye, widened by
 //     a margin far above rounding) and against the eye's distance; the ballot is the tile's candidate list,
 //     sorted by the distance below which no ray of the tile can enter the box;
