@@ -70,6 +70,11 @@ def test_band_arguments_are_checked(torch_cuda):
         with pytest.raises(ValueError, match="rows"):
             r.set_rows(first, count)
     assert r.rows == (0, 12)
+    d = wl.desc
+    u = ng.UnevenBatchRenderer([(16, 12, d.instances[:2]), (8, 8, d.instances[:1])], lights=d.lights, floor=d.floor,
+                               meshes=d.meshes, device="cuda:0")
+    with pytest.raises(ValueError, match="uneven sizes render whole images"):
+        u.set_rows(0, 4)
 
 
 def test_band_hit_records_and_adjoint_are_the_whole_images_restricted(torch_cuda):

@@ -215,6 +215,23 @@ def test_stream_entry_points_check_their_arguments_before_any_launch():
     assert b"grad_scales needs scales" in L.ngb_last_error(None)
 
 
+def test_row_band_and_memory_entry_points_without_a_renderer():
+    """ngb_set_rows on no renderer is a logic error, ngb_rows checks its pointers, and with no renderer made the
+    device-bytes count is 0, also after a construction that validation refused (its cleanup touches no GPU)."""
+    import ctypes
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200._lib import lib
+    L = lib()
+    assert L.ngb_set_rows(None, 0, 1) == 4
+    first, count = ctypes.c_int32(), ctypes.c_int32()
+    assert L.ngb_rows(None, ctypes.byref(first), ctypes.byref(count)) == 1
+    assert L.ngb_inject_allocation_failure(-1) == 0
+    assert ng.device_bytes() == 0
+    with pytest.raises(ValueError, match="world_count must be 1 or more"):
+        ng.BatchRenderer(8, 8, 0, 1)
+    assert ng.device_bytes() == 0
+
+
 def test_construction_rejects_bad_scenes_with_the_reference_messages():
     import neraulgraphics_b200 as ng
     with pytest.raises(ValueError, match="world_count must be 1 or more, got 0"):
