@@ -462,7 +462,15 @@ __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs 
             const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
             const float3 specular = zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), L.d)), mat.exponent);
             const float3 c_shadow = radiance_of(mat, s.ambient, zero, zero);
-            cold.put3(C_LIT, radiance_of(mat, s.ambient, diffuse, specular));
+            const float3 c_lit = radiance_of(mat, s.ambient, diffuse, specular);
+            // A shadow ray whose answer cannot change the pixel (lit and shadowed bytes equal, as where the
+            // surface faces away from the light and the highlight rounds away) is not traced.
+            if (rgb_packed(s.srgb_table, c_lit) == rgb_packed(s.srgb_table, c_shadow)) {
+                write_rgb(s.srgb_table, a.rgb, pix, c_shadow);
+                L.state = ST_IDLE;
+                return;
+            }
+            cold.put3(C_LIT, c_lit);
             cold.put3(C_SHADOW, c_shadow);
             // The shadow ray: spheres and the floor first, then any hit in the meshes (scene_occluded,
             // src/render_core.h:146-161).

@@ -327,11 +327,7 @@ __device__ __forceinline__ void resolve(const SceneParams &s, int world, float3 
 
 // sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283), packed r | g << 8 | b << 16.
 // Not inlined: one copy serves every colour the kernel writes.
-__device__ __noinline__ int rgb_bytes(const float *table, float3 radiance) {
-    float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
-    sum = sum * (1.0f / 1.0f);
-    return srgb_byte(table, sum.x) | (srgb_byte(table, sum.y) << 8) | (srgb_byte(table, sum.z) << 16);
-}
+__device__ __noinline__ int rgb_bytes(const float *table, float3 radiance) { return rgb_packed(table, radiance); }
 
 __device__ __forceinline__ void put_rgb(uint8_t *rgb, long long pix, int bytes) {
     uint8_t *o = rgb + 3 * static_cast<size_t>(pix);
@@ -695,6 +691,9 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
             }
         }
         const int bytes = rgb_bytes(s.srgb_table, radiance);
+        // A shadow ray whose answer cannot change the pixel (lit and shadowed bytes equal, as where the surface
+        // faces away from the light and the highlight rounds away) is not traced: the bytes are final here.
+        if (pending && bytes == shadow_bytes) pending = false;
         if (pending) {
             lit_bytes = bytes;
             // The shadow ray's own mesh: walked first when the ray starts on its body's side (the light is behind

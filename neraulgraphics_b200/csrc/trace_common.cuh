@@ -416,6 +416,13 @@ __device__ __forceinline__ float3 radiance_of(const DevMaterial &m, float ambien
     return mk3(0.0f, 0.0f, 0.0f) + (direct + m.diffuse_color * (ambient * m.kd)) * 1.0f;
 }
 
+// The bytes write_rgb stores for a radiance, packed r | g << 8 | b << 16.
+__device__ __forceinline__ int rgb_packed(const float *table, float3 radiance) {
+    float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
+    sum = sum * (1.0f / 1.0f);
+    return srgb_byte(table, sum.x) | (srgb_byte(table, sum.y) << 8) | (srgb_byte(table, sum.z) << 16);
+}
+
 // sample_pixel's average of one sample, sRGB, bytes (src/render_core.h:248-283).
 __device__ __forceinline__ void write_rgb(const float *table, uint8_t *rgb, long long pix, float3 radiance) {
     float3 sum = mk3(0.0f, 0.0f, 0.0f) + radiance;
