@@ -381,6 +381,28 @@ __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, i
     return t;
 }
 
+// The camera kernel's tiles when a render asks for the picture and the centre-ray outputs of views of one
+// size: 4 x 4 pixels, lanes 2k and 2k + 1 on pixel k (k = 0..15, row-major), the even lane tracing the centre
+// ray and the odd one the picture ray, so the two nearly equal walks of a pixel run side by side.
+__device__ __forceinline__ TileAt pair_tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view,
+    int lane) {
+    TileAt t;
+    t.view = static_cast<int>(tile / tiles_per_view);
+    t.width = a.width;
+    t.height = a.height;
+    t.aspect = a.aspect;
+    const int q = static_cast<int>(tile % tiles_per_view);
+    const int k = lane >> 1;
+    t.x0 = (q % tiles_x) * 4;
+    t.y0 = a.row_first + (q / tiles_x) * 4;
+    t.x = t.x0 + (k & 3);
+    t.y = t.y0 + (k >> 2);
+    t.pixel = t.x < t.width && t.y < a.row_first + a.rows;
+    t.world = t.view / a.cameras_per_world;
+    t.pix = static_cast<long long>(t.view) * a.rows * a.width + static_cast<long long>(t.y - a.row_first) * t.width + t.x;
+    return t;
+}
+
 // A warp's next run of tiles, TILES_PER_FETCH of them from one atomic; first >= tiles when none are left.
 __device__ __forceinline__ long long fetch_tiles(int *counter, int lane) {
     long long first = 0;
@@ -408,7 +430,7 @@ constexpr int CODE_NONE = -1, CODE_FLOOR = -2, CODE_SPHERE = -3;
 // Camera kernel. THREADS per CTA and MIN_BLOCKS resident CTAs per SM set the register budget. Per tile: the
 // candidates, then the centre rays (depth, normals, IDs written here) and the picture rays (their closest
 // hits written for the shade kernel).
-template <int THREADS, int MIN_BLOCKS, int CAP>
+template <int THREADS, int MIN_BLOCKS, int CAP, bool PAIRED>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const __grid_constant__ SceneParams s,
     const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
     __shared__ WarpSmem<CAP> warp_smem[THREADS / 32];
@@ -423,7 +445,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
         if (first >= tiles) break;
         const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
         for (long long tile = first; tile < last; ++tile) {
-            const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
+            const TileAt T = PAIRED ? pair_tile_at(a, tile, tiles_x, tiles_per_view, lane)
+                                    : tile_at(a, tile, tiles_x, tiles_per_view, lane);
+            constexpr int TW = PAIRED ? 4 : TILE_W, TH = PAIRED ? 4 : TILE_H;
             const int P = s.instance_count > 0 ? world_count_of(s, T.world) : 0;
             const float fw = static_cast<float>(T.width), fh = static_cast<float>(T.height), asp = T.aspect;
             // The view's camera (camera_from_matrix, src/render_core.h:264-273).
@@ -438,9 +462,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             // The tile's pyramid: the tangent-plane offsets of its pixel edges (every jittered and centre ray of
             // the tile lies inside), widened by 1e-3, and the four side planes through the eye, facing inwards.
             const float sxa = (2.0f * static_cast<float>(T.x0) / fw - 1.0f) * fs * asp;
-            const float sxb = (2.0f * static_cast<float>(T.x0 + TILE_W) / fw - 1.0f) * fs * asp;
+            const float sxb = (2.0f * static_cast<float>(T.x0 + TW) / fw - 1.0f) * fs * asp;
             const float sya = -(2.0f * static_cast<float>(T.y0) / fh - 1.0f) * fs;
-            const float syb = -(2.0f * static_cast<float>(T.y0 + TILE_H) / fh - 1.0f) * fs;
+            const float syb = -(2.0f * static_cast<float>(T.y0 + TH) / fh - 1.0f) * fs;
             const float sx_lo = fminf(sxa, sxb) - 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sx_hi = fmaxf(sxa, sxb) + 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
@@ -504,8 +528,10 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
 
             // The centre ray for depth, normals and IDs (aov_pixel, src/render_core.h:313-327), then the picture
             // ray (trace, src/render_core.h:202-245) up to its closest hit. Spheres and the floor first.
-            const int last_pass = a.rgb ? 1 : 0;
-            for (int pass = want_aov ? 0 : 1; pass <= last_pass; ++pass) {
+            // Paired tiles: one pass, each lane its own kind of ray (the trip count is the same on every lane).
+            const int first_pass = PAIRED ? (lane & 1) : (want_aov ? 0 : 1);
+            const int last_pass = PAIRED ? (lane & 1) : (a.rgb ? 1 : 0);
+            for (int pass = first_pass; pass <= last_pass; ++pass) {
                 float3 d;
                 if (pass == 0) {
                     d = camera_dir(right, up, fwd, static_cast<float>(T.x) + 0.5f, static_cast<float>(T.y) + 0.5f, fw, fh,
@@ -875,9 +901,16 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         return e;
     }
     e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
-    if (e == cudaSuccess)
-        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x, tiles_per_view,
-            stream);
+    // Both kinds of camera ray over views of one size: paired 4 x 4 tiles (pair_tile_at).
+    const bool paired = !a.view_info && a.rgb && aov;
+    if (e == cudaSuccess && paired) {
+        const int ptx = (a.width + 3) / 4, pty = (a.rows + 3) / 4;
+        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, true>, THREADS, s, a, counter,
+            static_cast<long long>(ptx) * pty * a.views, ptx, ptx * pty, stream);
+    } else if (e == cudaSuccess) {
+        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, false>, THREADS, s, a, counter, tiles, tiles_x,
+            tiles_per_view, stream);
+    }
     mark(after_camera);
     if (e != cudaSuccess || !a.rgb) {
         mark(after_shade);
