@@ -3,7 +3,9 @@
 // worlds of up to TILE_MAX_INSTANCES instances (what a batch of simulator worlds holds), a packet walk of the
 // world tree above that.
 //
-// One warp renders an 8 x 4 pixel tile of one view. All 32 rays of a tile start at the same eye and point into
+// One warp renders an 8 x 4 pixel tile of one view (the camera kernel, when a render asks for the picture and
+// the centre-ray outputs of views of one size: a 4 x 4 tile with a pixel's two rays on adjacent lanes, so its
+// two nearly equal walks run side by side). All 32 rays of a tile start at the same eye and point into
 // the same narrow pyramid, so in a world of up to TILE_MAX_INSTANCES instances the warp replaces the world
 // tree's walk by one conservative test per instance, 32 instances at a time:
 //   - lane j tests instance j's world box against the tile's pyramid (four planes through the eye, widened by
