@@ -98,6 +98,9 @@ struct RenderArgs {
     const int4 *view_info;
     long long total_pixels;
     long long total_tiles;
+    // Uneven views: per view its first tile of 4 x 4 pixels, and their total (the camera kernel's paired tiles).
+    const int *view_pair_tile;
+    long long total_pair_tiles;
 };
 
 // The per-view camera basis of camera_from_matrix (src/render_core.h:264-273): (position.xyz, right.x)

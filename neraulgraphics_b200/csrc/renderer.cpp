@@ -223,6 +223,8 @@ struct Renderer {
     std::vector<int> world_first_host;
     DevBuf<int> world_first;
     DevBuf<int4> view_info;
+    DevBuf<int> view_pair_tile;  // per view: its first 4 x 4 tile (the camera kernel's paired tiles)
+    long long total_pair_tiles = 0;
     long long total_pixels = 0, total_tiles = 0;
 
     explicit Renderer(const ngb_scene &s, const UnevenLayout *layout = nullptr);
@@ -393,16 +395,22 @@ void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
     if (uneven) {
         // Per view: (width, height, first pixel, first tile of 8 x 4 pixels).
         std::vector<int4> info(worlds);
-        long long pix = 0, tile = 0;
+        std::vector<int> pair_first(worlds);
+        long long pix = 0, tile = 0, pair_tile = 0;
         for (int w = 0; w < worlds; ++w) {
             const int vw = layout->width[w], vh = layout->height[w];
             info[w] = make_int4(vw, vh, static_cast<int>(pix), static_cast<int>(tile));
+            pair_first[w] = static_cast<int>(pair_tile);
             pix += static_cast<long long>(vw) * vh;
             tile += static_cast<long long>((vw + 7) / 8) * ((vh + 3) / 4);
+            pair_tile += static_cast<long long>((vw + 3) / 4) * ((vh + 3) / 4);
         }
         total_tiles = tile;
+        total_pair_tiles = pair_tile;
         view_info.ensure(worlds);
         CK(cudaMemcpy(view_info.p, info.data(), info.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        view_pair_tile.ensure(worlds);
+        CK(cudaMemcpy(view_pair_tile.p, pair_first.data(), pair_first.size() * sizeof(int), cudaMemcpyHostToDevice));
         world_first.ensure(worlds + 1);
         CK(cudaMemcpy(world_first.p, world_first_host.data(), (worlds + 1) * sizeof(int), cudaMemcpyHostToDevice));
         params.world_first = world_first.p;
@@ -572,7 +580,7 @@ void Renderer::teardown() {
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
     hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
-    world_first.release(), view_info.release();
+    world_first.release(), view_info.release(), view_pair_tile.release();
     if (previous >= 0 && previous != device) cudaSetDevice(previous);
 }
 
@@ -950,6 +958,8 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
             a.view_info = view_info.p;
             a.total_pixels = total_pixels;
             a.total_tiles = total_tiles;
+            a.view_pair_tile = view_pair_tile.p;
+            a.total_pair_tiles = total_pair_tiles;
         }
         if (a.rgb) {
             a.pic_hit = pic_hit.ensure(pixels());

@@ -4,7 +4,7 @@
 // world tree above that.
 //
 // One warp renders an 8 x 4 pixel tile of one view (the camera kernel, when a render asks for the picture and
-// the centre-ray outputs of views of one size: a 4 x 4 tile with a pixel's two rays on adjacent lanes, so its
+// the centre-ray outputs: a 4 x 4 tile with a pixel's two rays on adjacent lanes, so its
 // two nearly equal walks run side by side). All 32 rays of a tile start at the same eye and point into
 // the same narrow pyramid, so in a world of up to TILE_MAX_INSTANCES instances the warp replaces the world
 // tree's walk by one conservative test per instance, 32 instances at a time:
@@ -383,25 +383,49 @@ __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, i
     return t;
 }
 
-// The camera kernel's tiles when a render asks for the picture and the centre-ray outputs of views of one
-// size: 4 x 4 pixels, lanes 2k and 2k + 1 on pixel k (k = 0..15, row-major), the even lane tracing the centre
+// The camera kernel's tiles when a render asks for the picture and the centre-ray outputs: 4 x 4 pixels, lanes 2k and 2k + 1 on pixel k (k = 0..15, row-major), the even lane tracing the centre
 // ray and the odd one the picture ray, so the two nearly equal walks of a pixel run side by side.
 __device__ __forceinline__ TileAt pair_tile_at(const RenderArgs &a, long long tile, int tiles_x, int tiles_per_view,
     int lane) {
     TileAt t;
-    t.view = static_cast<int>(tile / tiles_per_view);
-    t.width = a.width;
-    t.height = a.height;
-    t.aspect = a.aspect;
-    const int q = static_cast<int>(tile % tiles_per_view);
+    int q, row0, row_end;  // the view's rendered rows [row0, row_end)
+    long long first_pixel;
+    if (a.view_info) {
+        // Uneven views: the last view whose first 4 x 4 tile is at most tile.
+        int lo = 0, hi = a.views - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(a.view_pair_tile + mid) <= tile) lo = mid;
+            else hi = mid - 1;
+        }
+        t.view = lo;
+        const int4 v = __ldg(a.view_info + lo);
+        t.width = v.x;
+        t.height = v.y;
+        t.aspect = static_cast<float>(v.x) / static_cast<float>(v.y);
+        tiles_x = (v.x + 3) / 4;
+        q = static_cast<int>(tile - __ldg(a.view_pair_tile + lo));
+        first_pixel = v.z;
+        row0 = 0;
+        row_end = v.y;
+    } else {
+        t.view = static_cast<int>(tile / tiles_per_view);
+        t.width = a.width;
+        t.height = a.height;
+        t.aspect = a.aspect;
+        q = static_cast<int>(tile % tiles_per_view);
+        first_pixel = static_cast<long long>(t.view) * a.rows * a.width;
+        row0 = a.row_first;
+        row_end = a.row_first + a.rows;
+    }
     const int k = lane >> 1;
     t.x0 = (q % tiles_x) * 4;
-    t.y0 = a.row_first + (q / tiles_x) * 4;
+    t.y0 = row0 + (q / tiles_x) * 4;
     t.x = t.x0 + (k & 3);
     t.y = t.y0 + (k >> 2);
-    t.pixel = t.x < t.width && t.y < a.row_first + a.rows;
+    t.pixel = t.x < t.width && t.y < row_end;
     t.world = t.view / a.cameras_per_world;
-    t.pix = static_cast<long long>(t.view) * a.rows * a.width + static_cast<long long>(t.y - a.row_first) * t.width + t.x;
+    t.pix = first_pixel + static_cast<long long>(t.y - row0) * t.width + t.x;
     return t;
 }
 
@@ -903,12 +927,13 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         return e;
     }
     e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
-    // Both kinds of camera ray over views of one size: paired 4 x 4 tiles (pair_tile_at).
-    const bool paired = !a.view_info && a.rgb && aov;
+    // Both kinds of camera ray: paired 4 x 4 tiles (pair_tile_at).
+    const bool paired = a.rgb && aov && (!a.view_info || a.view_pair_tile);
     if (e == cudaSuccess && paired) {
         const int ptx = (a.width + 3) / 4, pty = (a.rows + 3) / 4;
-        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, true>, THREADS, s, a, counter,
-            static_cast<long long>(ptx) * pty * a.views, ptx, ptx * pty, stream);
+        const long long pair_tiles = a.view_info ? a.total_pair_tiles : static_cast<long long>(ptx) * pty * a.views;
+        e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, true>, THREADS, s, a, counter, pair_tiles, ptx,
+            ptx * pty, stream);
     } else if (e == cudaSuccess) {
         e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, false>, THREADS, s, a, counter, tiles, tiles_x,
             tiles_per_view, stream);
