@@ -594,3 +594,40 @@ def test_packet_tiles_with_partial_tiles_two_cameras_spheres_and_floor(torch_cud
     got = r.render(cams, 1.0, 1, **ALL, frame=2)
     assert (got["object_ids"] >= 34).mean() > 0.1 and (got["object_ids"] == 33).mean() > 0.01
     assert_same_images(got, want, ties=want["ties"])
+
+
+@pytest.mark.parametrize("per_world", [8, 40, 300])
+def test_paired_camera_rays_equal_one_kind_at_a_time(torch_cuda, per_world):
+    """A render asking for the picture and the centre-ray outputs traces a pixel's two rays on adjacent lanes of a
+    4x4 tile; asking for one kind only traces it over 8x4 tiles. Every output is the same bit for bit either
+    way (candidate lists of 32 and 256, the packet walk; 37x29 images, partial tiles, two cameras per world)."""
+    wl = workloads.icosphere_worlds(worlds=3, per_world=per_world, width=37, height=29, seed=31)
+    d = wl.desc
+    desc = ng.SceneDesc(d.width, d.height, 3, 2, d.spheres, d.lights, d.floor, d.meshes, d.instances)
+    cams = np.repeat(wl.cameras, 2, axis=0)
+    cams[1::2, :, 3] += np.float32([0.3, 0.2, 0.1])
+    r = product(desc)
+    r.set_instance_transforms(wl.matrices)
+    both = r.render(cams, 1.0, 1, **ALL, frame=5)
+    rgb = r.render(cams, 1.0, 1, rgb=True, frame=5)
+    aov = r.render(cams, 1.0, 1, rgb=False, depth=True, normals=True, object_ids=True, frame=5)
+    assert (both["object_ids"] >= 34).mean() > 0.1
+    assert np.array_equal(both["rgb"], rgb["rgb"])
+    for k in ("depth", "normals", "object_ids"):
+        assert np.array_equal(both[k].view(np.uint32), aov[k].view(np.uint32)), k
+
+
+def test_paired_camera_rays_on_uneven_worlds_equal_one_kind_at_a_time(torch_cuda):
+    wl = workloads.icosphere_worlds(worlds=3, per_world=12, width=37, height=29, seed=37)
+    d = wl.desc
+    worlds = [(37, 29, d.instances[:12]), (16, 16, d.instances[:5]), (21, 9, d.instances[:9])]
+    u = ng.UnevenBatchRenderer(worlds, lights=d.lights, floor=d.floor, meshes=d.meshes, device="cuda:0")
+    m = np.concatenate([wl.matrices[0, :12], wl.matrices[1, :5], wl.matrices[2, :9]]).astype(np.float32)
+    u.set_instance_transforms(m)
+    both = u.render(wl.cameras, 1.0, **ALL)
+    rgb = u.render(wl.cameras, 1.0, rgb=True)
+    aov = u.render(wl.cameras, 1.0, rgb=False, depth=True, normals=True, object_ids=True)
+    assert (both["object_ids"] >= 34).mean() > 0.05
+    assert np.array_equal(both["rgb"], rgb["rgb"])
+    for k in ("depth", "normals", "object_ids"):
+        assert np.array_equal(both[k].view(np.uint32), aov[k].view(np.uint32)), k
