@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--worlds", type=int, default=4096)
-    p.add_argument("--e2e-steps", type=int, default=10)
+    p.add_argument("--e2e-steps", type=int, default=20)
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-reference-cuda", action="store_true",
                    help="--impl reference: skip timing the reference's CUDA backend on the GPU")
