@@ -593,8 +593,16 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                 float3 normal = mk3(0.0f, 0.0f, 0.0f);
                 DevMaterial mat{};
                 int object = OBJECT_NONE;
-                if (found) resolve(s, T.world, eye + d * tmax, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal,
-                    mat, object);
+                // The object ID needs only which object was hit; the surface (normal, material) only when normals
+                // are asked for.
+                if (found && a.normal) {
+                    resolve(s, T.world, eye + d * tmax, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal,
+                        mat, object);
+                } else if (found) {
+                    object = mesh ? OBJECT_INSTANCE + (hit_inst - world_first_of(s, T.world))
+                        : hit_floor ? OBJECT_FLOOR
+                                    : OBJECT_SPHERE + best_sphere;
+                }
                 if (a.depth) a.depth[p] = found ? tmax * dot(d, fwd) : __int_as_float(0x7f800000);
                 if (a.normal) {
                     a.normal[3 * p] = normal.x;
