@@ -373,12 +373,12 @@ def run_ours(args, rank, world, local_rank, dist):
                       "render": round(rmed, 4),
                       **({"camera_rays": round(stage_ms[0], 4), "shading": round(stage_ms[1], 4),
                           "shadow_rays": round(stage_ms[2], 4)} if len(stage_ms) == 3 else {})},
-        "rays_per_s": None if rpi is None else round(value * rpi, 1),
-        "rays_per_image": None if rpi is None else round(rpi, 1),
         # Reference-equivalent work: the rays the reference's path traces per image and the bytes its walks fetch
         # (nodes, child-box pairs, instance inverses, triangles; almost all from L1/L2), as the oracle counts them
         # (it traces every shadow ray; this build leaves out those whose answer cannot change the pixel), at this
         # build's images/s, and that byte rate over the measured HBM peak (above 1 shows cache reuse).
+        "reference_rays_per_s": None if rpi is None else round(value * rpi, 1),
+        "reference_rays_per_image": None if rpi is None else round(rpi, 1),
         "traversal": None if not counts else {
             "bytes_per_image": round(counts["traversal_bytes_per_image"], 1),
             "achieved_gbs": round(counts["traversal_bytes_per_image"] * value / 1e9, 1),
