@@ -169,9 +169,19 @@ void check_environment(const ngb_environment &e) {
 
 // ----------------------------------------------------------------------------- bottom-level trees --
 //
-// The binned surface-area-heuristic build of src/bvh.cpp:46-174 (16 bins, leaf at most 4 triangles, depth
-// at most 60), with the same tie rules, partition and node order, so every mesh gets the reference's tree
-// node for node and its triangles in the reference's leaf order.
+// Each mesh's tree is the binned surface-area-heuristic tree of src/bvh.cpp:46-174 (16 bins, leaves of at
+// most 4 triangles, depth at most 60), node for node, with its triangles in the same leaf order. It is built
+// the way the device rebuild in blas_build.cu builds it, so the two builders are one algorithm:
+//   - level by level: every node of a depth is split before any node of the next depth; a node's children are
+//     appended to the next depth's list (a split's outcome depends only on its own triangle range, so the
+//     order in which nodes are split does not change the tree);
+//   - a split moves its range's triangles with the swaps std::partition (libstdc++'s bidirectional form)
+//     makes: the k-th triangle from the left that fails the test trades places with the k-th from the right
+//     that passes it, for every k before the two runs meet;
+//   - the numbering comes last, in closed form: the reference numbers a node's children 2k + 1 and 2k + 2 when
+//     it splits the k-th internal node in depth-first, left-first order, and an internal node's k is the count
+//     of internal nodes starting (in leaf order) before it plus its depth below the topmost internal node that
+//     starts where it starts.
 
 namespace {
 
@@ -179,22 +189,134 @@ struct Box {
     float lo[3], hi[3];
 };
 
-Box empty_box() {
-    const float inf = std::numeric_limits<float>::infinity();
-    return Box{{inf, inf, inf}, {-inf, -inf, -inf}};
-}
+constexpr float INF = std::numeric_limits<float>::infinity();
+constexpr int BINS = 16;
+constexpr uint32_t MAX_LEAF = 4;
+constexpr int MAX_DEPTH = 60;
 
-void grow(Box &b, const Box &o) {
+// Box arithmetic with the reference's tie rule: of two equal values (only -0 and +0 differ) the earlier in
+// range order is kept, as std::min / std::max keep their first argument.
+void take(Box &b, const float *lo, const float *hi) {
     for (int k = 0; k < 3; ++k) {
-        b.lo[k] = std::min(b.lo[k], o.lo[k]);
-        b.hi[k] = std::max(b.hi[k], o.hi[k]);
+        if (lo[k] < b.lo[k]) b.lo[k] = lo[k];
+        if (b.hi[k] < hi[k]) b.hi[k] = hi[k];
     }
 }
 
-float area(const Box &b) {
+float surface(const Box &b) {
     const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
     if (dx < 0.0f || dy < 0.0f || dz < 0.0f) return 0.0f;
     return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+int bin_index(float c, float lo, float scale) {
+    const int b = static_cast<int>((c - lo) * scale);
+    return b < BINS - 1 ? b : BINS - 1;
+}
+
+// A node while the tree is built: its triangle range in `order`, its depth, its box and its first child in
+// level order (-1 for a leaf).
+struct Draft {
+    uint32_t begin, end;
+    int depth;
+    int first_child;
+    Box box;
+};
+
+// The triangles of one mesh: their boxes (6 floats) and centroids (3 floats), and their order.
+struct Items {
+    std::vector<float> box, centre;
+    std::vector<uint32_t> order;
+};
+
+// The cheapest split plane of a range, over the axes in order (src/bvh.cpp:94-125): axis -1 when no axis
+// has spread centroids or no plane leaves triangles on both sides.
+struct Plane {
+    int axis = -1, bin = 0;
+    float cost = INF;
+};
+
+Plane cheapest_plane(const Items &it, uint32_t begin, uint32_t end, const Box &cbox) {
+    Plane best;
+    for (int axis = 0; axis < 3; ++axis) {
+        const float extent = cbox.hi[axis] - cbox.lo[axis];
+        if (!(extent > 0.0f)) continue;
+        const float scale = static_cast<float>(BINS) / extent;
+        Box bins[BINS];
+        int count[BINS] = {};
+        for (Box &b : bins) b = Box{{INF, INF, INF}, {-INF, -INF, -INF}};
+        for (uint32_t i = begin; i < end; ++i) {
+            const float *tb = &it.box[6 * static_cast<size_t>(it.order[i])];
+            const int b = bin_index(it.centre[3 * static_cast<size_t>(it.order[i]) + axis], cbox.lo[axis], scale);
+            ++count[b];
+            take(bins[b], tb, tb + 3);
+        }
+        // Suffix areas and counts: plane p separates bins [0, p] from [p + 1, BINS).
+        float suffix_area[BINS];
+        int suffix_count[BINS];
+        Box acc{{INF, INF, INF}, {-INF, -INF, -INF}};
+        int n = 0;
+        for (int b = BINS - 1; b >= 1; --b) {
+            take(acc, bins[b].lo, bins[b].hi);
+            n += count[b];
+            suffix_area[b] = surface(acc);
+            suffix_count[b] = n;
+        }
+        acc = Box{{INF, INF, INF}, {-INF, -INF, -INF}};
+        n = 0;
+        for (int p = 0; p + 1 < BINS; ++p) {
+            take(acc, bins[p].lo, bins[p].hi);
+            n += count[p];
+            if (n == 0 || suffix_count[p + 1] == 0) continue;
+            const float cost = static_cast<float>(n) * surface(acc) +
+                static_cast<float>(suffix_count[p + 1]) * suffix_area[p + 1];
+            if (cost < best.cost) best = Plane{axis, p, cost};
+        }
+    }
+    return best;
+}
+
+// Splits drafts[x]: fills its box and, unless it stays a leaf, partitions its range and appends its two
+// children to `drafts` (src/bvh.cpp:62-170).
+void split(Items &it, std::vector<Draft> &drafts, size_t x) {
+    const uint32_t begin = drafts[x].begin, end = drafts[x].end, count = end - begin;
+    const int depth = drafts[x].depth;
+    Box box{{INF, INF, INF}, {-INF, -INF, -INF}}, cbox = box;
+    for (uint32_t i = begin; i < end; ++i) {
+        const uint32_t p = it.order[i];
+        take(box, &it.box[6 * static_cast<size_t>(p)], &it.box[6 * static_cast<size_t>(p) + 3]);
+        const float *c = &it.centre[3 * static_cast<size_t>(p)];
+        take(cbox, c, c);
+    }
+    drafts[x].box = box;
+    drafts[x].first_child = -1;
+    const Plane plane = count > 1 ? cheapest_plane(it, begin, end, cbox) : Plane{};
+    const float here = surface(box);
+    const bool leaf = count == 1 || depth >= MAX_DEPTH ||
+        (count <= MAX_LEAF && (plane.axis < 0 || static_cast<float>(count) * here <= 1.0f * here + plane.cost));
+    if (leaf) return;
+    uint32_t mid = begin + count / 2;
+    if (plane.axis >= 0) {
+        const float lo = cbox.lo[plane.axis];
+        const float scale = static_cast<float>(BINS) / (cbox.hi[plane.axis] - lo);
+        auto passes = [&](uint32_t i) {
+            return bin_index(it.centre[3 * static_cast<size_t>(it.order[i]) + plane.axis], lo, scale) <= plane.bin;
+        };
+        uint32_t meet = begin;
+        for (uint32_t i = begin; i < end; ++i) meet += passes(i) ? 1u : 0u;
+        // The k-th failing position left of meet and the k-th passing position right of it, from the right.
+        std::vector<uint32_t> fail_left, pass_right;
+        for (uint32_t i = begin; i < meet; ++i)
+            if (!passes(i)) fail_left.push_back(i);
+        for (uint32_t j = end; j-- > meet;)
+            if (passes(j)) pass_right.push_back(j);
+        for (size_t k = 0; k < fail_left.size(); ++k) std::swap(it.order[fail_left[k]], it.order[pass_right[k]]);
+        mid = meet;
+        if (mid == begin || mid == end) mid = begin + count / 2;
+    }
+    drafts[x].first_child = static_cast<int>(drafts.size());
+    drafts.push_back(Draft{begin, mid, depth + 1, -1, {}});
+    drafts.push_back(Draft{mid, end, depth + 1, -1, {}});
 }
 
 struct Node {
@@ -204,115 +326,55 @@ struct Node {
     int32_t count;
 };
 
-constexpr int BINS = 16;
-constexpr int MAX_DEPTH = 60;
-
-// Returns the nodes (root first) and fills order with the primitives in leaf order.
-std::vector<Node> sah_build(const std::vector<Box> &bounds, std::vector<uint32_t> &order) {
-    const uint32_t n = static_cast<uint32_t>(bounds.size());
+// The tree over the triangle boxes `tri_box` (6 floats each): nodes in the reference's numbering (root first)
+// with mesh-local references, and `order` the triangles in leaf order.
+std::vector<Node> build_tree(std::vector<float> tri_box, std::vector<uint32_t> &order) {
+    Items it;
+    const uint32_t n = static_cast<uint32_t>(tri_box.size() / 6);
+    it.box = std::move(tri_box);
+    it.centre.resize(3 * static_cast<size_t>(n));
+    for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) it.centre[3 * i + k] = 0.5f * (it.box[6 * i + k] + it.box[6 * i + 3 + k]);
+    it.order.resize(n);
+    std::iota(it.order.begin(), it.order.end(), 0u);
     std::vector<Node> nodes;
-    order.resize(n);
-    if (n == 0) return nodes;
-    std::iota(order.begin(), order.end(), 0u);
-    std::vector<std::array<float, 3>> centre(n);
-    for (uint32_t i = 0; i < n; ++i)
-        for (int k = 0; k < 3; ++k) centre[i][k] = 0.5f * (bounds[i].lo[k] + bounds[i].hi[k]);
-    nodes.reserve(2 * static_cast<size_t>(n));
-    nodes.emplace_back();
-    struct Work {
-        int node;
-        uint32_t begin, end;
-        int depth;
-    };
-    std::vector<Work> stack{{0, 0, n, 0}};
-    auto bin_of = [](float c, float lo, float scale) { return std::min(BINS - 1, static_cast<int>((c - lo) * scale)); };
-    while (!stack.empty()) {
-        const Work wk = stack.back();
-        stack.pop_back();
-        const uint32_t count = wk.end - wk.begin;
-        uint32_t *prims = order.data() + wk.begin;
-        Box box = empty_box(), cbox = empty_box();
-        for (uint32_t i = 0; i < count; ++i) {
-            grow(box, bounds[prims[i]]);
-            for (int k = 0; k < 3; ++k) {
-                cbox.lo[k] = std::min(cbox.lo[k], centre[prims[i]][k]);
-                cbox.hi[k] = std::max(cbox.hi[k], centre[prims[i]][k]);
-            }
-        }
-        Node node{};
-        for (int k = 0; k < 3; ++k) {
-            node.lo[k] = box.lo[k];
-            node.hi[k] = box.hi[k];
-        }
-        int best_axis = -1, best_bin = 0;
-        float best_cost = std::numeric_limits<float>::infinity();
-        if (count > 1) {
-            for (int axis = 0; axis < 3; ++axis) {
-                const float extent = cbox.hi[axis] - cbox.lo[axis];
-                if (!(extent > 0.0f)) continue;
-                const float scale = static_cast<float>(BINS) / extent;
-                int bin_count[BINS] = {};
-                Box bin_box[BINS];
-                for (Box &b : bin_box) b = empty_box();
-                for (uint32_t i = 0; i < count; ++i) {
-                    const int b = bin_of(centre[prims[i]][axis], cbox.lo[axis], scale);
-                    ++bin_count[b];
-                    grow(bin_box[b], bounds[prims[i]]);
-                }
-                float right_area[BINS - 1];
-                int right_count[BINS - 1];
-                Box acc = empty_box();
-                int running = 0;
-                for (int i = BINS - 1; i >= 1; --i) {
-                    grow(acc, bin_box[i]);
-                    running += bin_count[i];
-                    right_area[i - 1] = area(acc);
-                    right_count[i - 1] = running;
-                }
-                acc = empty_box();
-                running = 0;
-                for (int i = 0; i < BINS - 1; ++i) {
-                    grow(acc, bin_box[i]);
-                    running += bin_count[i];
-                    if (running == 0 || right_count[i] == 0) continue;
-                    const float cost = static_cast<float>(running) * area(acc) +
-                        static_cast<float>(right_count[i]) * right_area[i];
-                    if (cost < best_cost) {
-                        best_cost = cost;
-                        best_axis = axis;
-                        best_bin = i;
-                    }
-                }
-            }
-        }
-        const float leaf_cost = static_cast<float>(count) * area(box);
-        const float split_cost = 1.0f * area(box) + best_cost;
-        const bool small = count <= 4u;
-        if (count == 1 || wk.depth >= MAX_DEPTH || (small && (best_axis < 0 || leaf_cost <= split_cost))) {
-            node.a = static_cast<int32_t>(wk.begin);
-            node.count = static_cast<int32_t>(count);
-            nodes[wk.node] = node;
-            continue;
-        }
-        uint32_t mid;
-        if (best_axis >= 0) {
-            const float lo = cbox.lo[best_axis];
-            const float scale = static_cast<float>(BINS) / (cbox.hi[best_axis] - lo);
-            const uint32_t *p = std::partition(prims, prims + count,
-                [&](uint32_t prim) { return bin_of(centre[prim][best_axis], lo, scale) <= best_bin; });
-            mid = wk.begin + static_cast<uint32_t>(p - prims);
-            if (mid == wk.begin || mid == wk.end) mid = wk.begin + count / 2;
-        } else {
-            mid = wk.begin + count / 2;
-        }
-        const int left = static_cast<int>(nodes.size());
-        nodes.resize(nodes.size() + 2);
-        node.a = left;
-        node.count = 0;
-        nodes[wk.node] = node;
-        stack.push_back({left + 1, mid, wk.end, wk.depth + 1});
-        stack.push_back({left, wk.begin, mid, wk.depth + 1});
+    if (n == 0) {
+        order.clear();
+        return nodes;
     }
+    std::vector<Draft> drafts{Draft{0, n, 0, -1, {}}};
+    drafts.reserve(2 * static_cast<size_t>(n));
+    for (size_t first = 0, last = 1; first < last; first = last, last = drafts.size())
+        for (size_t x = first; x < last; ++x) split(it, drafts, x);
+
+    // Closed-form numbering of the depth-first order.
+    std::vector<int> starts(n + 1, 0), top(n, INT_MAX);
+    for (const Draft &d : drafts)
+        if (d.first_child >= 0) {
+            ++starts[d.begin + 1];
+            top[d.begin] = std::min(top[d.begin], d.depth);
+        }
+    for (uint32_t i = 0; i < n; ++i) starts[i + 1] += starts[i];  // internal nodes starting before i
+    std::vector<int> index(drafts.size(), 0);
+    for (const Draft &d : drafts) {
+        if (d.first_child < 0) continue;
+        const int k = starts[d.begin] + d.depth - top[d.begin];
+        index[d.first_child] = 2 * k + 1;
+        index[d.first_child + 1] = 2 * k + 2;
+    }
+    nodes.resize(drafts.size());
+    for (size_t x = 0; x < drafts.size(); ++x) {
+        const Draft &d = drafts[x];
+        Node &nd = nodes[index[x]];
+        for (int k = 0; k < 3; ++k) {
+            nd.lo[k] = d.box.lo[k];
+            nd.hi[k] = d.box.hi[k];
+        }
+        const bool leaf = d.first_child < 0;
+        nd.a = leaf ? static_cast<int32_t>(d.begin) : index[d.first_child];
+        nd.count = leaf ? static_cast<int32_t>(d.end - d.begin) : 0;
+    }
+    order = std::move(it.order);
     return nodes;
 }
 
@@ -325,20 +387,25 @@ BuiltMeshes build_meshes(const ngb_scene &s, bool node_capacity) {
     for (int m = 0; m < s.mesh_count; ++m) {
         const ngb_mesh &mesh = s.meshes[m];
         const size_t tri_count = static_cast<size_t>(mesh.index_count) / 3;
-        std::vector<Box> tri_bounds(tri_count);
+        // Triangle boxes over the vertices in order; of two equal values (-0 and +0) the later is kept, as the
+        // reference's std::fmin / std::fmax give them (src/mesh_build.cpp:98-110).
+        std::vector<float> tri_box(6 * tri_count);
         for (size_t t = 0; t < tri_count; ++t) {
-            Box b = empty_box();
+            float *b = &tri_box[6 * t];
+            for (int a = 0; a < 3; ++a) {
+                b[a] = INF;
+                b[3 + a] = -INF;
+            }
             for (int k = 0; k < 3; ++k) {
                 const float *v = mesh.vertices + 3 * static_cast<size_t>(mesh.indices[3 * t + k]);
                 for (int a = 0; a < 3; ++a) {
-                    b.lo[a] = std::fmin(b.lo[a], v[a]);
-                    b.hi[a] = std::fmax(b.hi[a], v[a]);
+                    b[a] = b[a] < v[a] ? b[a] : v[a];
+                    b[3 + a] = b[3 + a] > v[a] ? b[3 + a] : v[a];
                 }
             }
-            tri_bounds[t] = b;
         }
         std::vector<uint32_t> order;
-        const std::vector<Node> tree = sah_build(tri_bounds, order);
+        const std::vector<Node> tree = build_tree(std::move(tri_box), order);
         const int node_base = static_cast<int>(out.nodes.size() / 8);
         const int tri_base = static_cast<int>(out.triangles.size() / 12);
         out.roots.push_back(node_base);

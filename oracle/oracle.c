@@ -358,9 +358,11 @@ static void build_meshes(orc_scene *s, const ngb_mesh *meshes, int mesh_count) {
             aabb_t b = empty_aabb();
             for (int k = 0; k < 3; ++k) {
                 const float *v = mesh->vertices + 3 * (size_t)mesh->indices[3 * t + k];
+                /* std::fmin / std::fmax as the reference's build compiles them: of two equal values (-0 and
+                 * +0) the second, the vertex; glibc's fminf keeps the first (mesh_build.cpp:98-110). */
                 for (int a = 0; a < 3; ++a) {
-                    b.lo[a] = fminf(b.lo[a], v[a]);
-                    b.hi[a] = fmaxf(b.hi[a], v[a]);
+                    b.lo[a] = b.lo[a] < v[a] ? b.lo[a] : v[a];
+                    b.hi[a] = b.hi[a] > v[a] ? b.hi[a] : v[a];
                 }
             }
             tb[t] = b;

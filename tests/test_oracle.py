@@ -144,8 +144,18 @@ def test_blas_builders_are_the_references():
     """The product's host builder (libngb.so) and the oracle's both give the reference's trees bit for bit."""
     import neraulgraphics_b200 as ng
     smooth = S.make_icosphere(1.0, 2)
+    rng = np.random.default_rng(5)
+    soup = S.Mesh(rng.normal(size=(600, 3)).astype(np.float32), np.arange(600, dtype=np.uint32).reshape(200, 3))
+    same = S.Mesh(np.tile(np.float32([[0, 0, 0], [1, 0, 0], [0, 1, 0]]), (10, 1)),
+                  np.arange(30, dtype=np.uint32).reshape(10, 3))
+    one = S.Mesh(np.float32([[0, 0, 0], [1, 0, 0], [0, 1, 0]]), np.uint32([[0, 1, 2]]))
+    zeros = S.Mesh(np.float32([[0, 0, 0], [-0.0, 1, 0], [0, -0.0, 1], [1, 1, -0.0], [-0.0, -0.0, -0.0]]),
+                   np.uint32([[0, 1, 2], [1, 3, 4], [4, 2, 0], [3, 2, 1]]))
+    line = S.Mesh(np.float32([[i, 0, 0] for i in range(40)] + [[i, 1e-3, 0] for i in range(40)]),
+                  np.uint32([[i, i + 1, 40 + i] for i in range(39)]))
     meshes = [S.make_icosphere(0.5, 3), S.make_box((0.4, 0.4, 0.4)), S.cylinder(1.0, 1.0, 128),
-              S.Mesh(smooth.vertices, smooth.triangles, normals=smooth.vertices), S.make_icosphere(1.0, 5)]
+              S.Mesh(smooth.vertices, smooth.triangles, normals=smooth.vertices), S.make_icosphere(1.0, 5),
+              soup, same, one, zeros, line]
     want = O.ref_build_meshes(meshes)
     got = ng.build_meshes(meshes)
     inst = [S.Instance(i) for i in range(len(meshes))]
