@@ -457,11 +457,15 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
  * Queued on `stream` (a cudaStream_t; NULL is the default stream), not waited for.
  * The build's scratch lives in a static device array of the library: at most 65536 instances over all
  * worlds (and 1024 per world); larger calls return NGB_INVALID_ARGUMENT. Every GPU that loads the library
- * keeps that array (about 0.8 MB) until exit. The first call on a device looks up the array's address, so
- * make it before any stream capture. All calls share the array: calls that overlap on the GPU race. */
+ * keeps that array (about 0.8 MB) until exit. The first call in a CUDA context (and the first after the
+ * calling thread's current context changed, as after cudaDeviceReset) looks up the array's address, so make
+ * it before any stream capture. All calls share the array: calls that overlap on the GPU race.
+ * error_word (device memory, 4-byte aligned, or NULL): set to 0 by the call's work on the stream, then to a
+ * nonzero code if the build's bottom-up box climb ran past the step limit a valid tree allows (3: within a
+ * world, 4: between worlds), which leaves the tree malformed. Read it once the stream has passed the call. */
 int ngb_build_tlas_noalloc(int32_t world_count, int32_t instances_per_world, const float *matrices,
     const float *slot_bounds, const int32_t *slot_blas_root, float *instance_records, uint64_t *keys,
-    int32_t *sorted_ids, float *tlas_nodes, int32_t *roots, void *stream);
+    int32_t *sorted_ids, float *tlas_nodes, int32_t *roots, int32_t *error_word, void *stream);
 
 #ifdef __cplusplus
 }

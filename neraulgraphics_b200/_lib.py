@@ -74,7 +74,7 @@ def lib():
     L.ngb_last_kernel_ms.restype = C.c_float
     L.ngb_last_kernel_ms.argtypes = [_vp]
     L.ngb_build_meshes.argtypes = [C.POINTER(_abi.MeshC), C.c_int32, _i32p, _i32p, _vp, _vp, _vp, _vp, _vp]
-    L.ngb_build_tlas_noalloc.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.ngb_build_tlas_noalloc.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
     L.ngb_set_rows.argtypes = [_vp, C.c_int32, C.c_int32]

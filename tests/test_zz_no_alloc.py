@@ -3,7 +3,8 @@
 This entry point serves callers that cannot call cudaMalloc -- a step captured into a CUDA graph, or a
 framework that owns the GPU's memory through its own pool -- so its scratch lives in a static device array
 instead. Here the test allocates the inputs and outputs (with PyTorch) and checks that two calls in a row
-give exactly the trees ngb_set_instance_transforms builds for the same matrices. It sorts last, so a run that
+give exactly the trees ngb_set_instance_transforms builds for the same matrices, and that the caller's error
+word reads 0 after each (a build whose box climb overran would set it). It sorts last, so a run that
 stops at its first failure has run every other test first, and it passes alone in a fresh process as well.
 """
 
@@ -37,6 +38,7 @@ def test_static_scratch_build_matches_the_renderers_build_twice(torch_cuda):
     ids = torch.empty(n, dtype=torch.int32, device="cuda:0")
     nodes = torch.empty((2 * n - 1, 8), dtype=torch.int32, device="cuda:0")
     roots = torch.empty(W, dtype=torch.int32, device="cuda:0")
+    error = torch.full((1,), -7, dtype=torch.int32, device="cuda:0")
     L = lib()
     stream = torch.cuda.current_stream().cuda_stream
     for step in workloads.random_walk(wl.poses, 2, seed=9):
@@ -47,8 +49,9 @@ def test_static_scratch_build_matches_the_renderers_build_twice(torch_cuda):
             t.fill_(-7)  # anything the call leaves unwritten shows up
         ptr = lambda t: C.c_void_p(t.data_ptr())
         check(L.ngb_build_tlas_noalloc(W, P, ptr(mats), ptr(bounds), ptr(blas_root), ptr(records), ptr(keys),
-                                       ptr(ids), ptr(nodes), ptr(roots), C.c_void_p(stream)))
+                                       ptr(ids), ptr(nodes), ptr(roots), ptr(error), C.c_void_p(stream)))
         torch.cuda.synchronize()
+        assert int(error.item()) == 0
         got_nodes = nodes.cpu().numpy()
         assert np.array_equal(keys.cpu().numpy().view(np.uint64), want["keys"])
         assert np.array_equal(ids.cpu().numpy(), want["sorted_ids"])
@@ -64,6 +67,6 @@ def test_static_scratch_build_matches_the_renderers_build_twice(torch_cuda):
 def test_static_scratch_build_rejects_sizes_beyond_its_limit(torch_cuda):
     L = lib()
     nul = C.c_void_p(16)
-    status = L.ngb_build_tlas_noalloc(70, 1000, nul, nul, nul, nul, nul, nul, nul, nul, None)
+    status = L.ngb_build_tlas_noalloc(70, 1000, nul, nul, nul, nul, nul, nul, nul, nul, None, None)
     assert status == 1
     assert "at most 65536" in L.ngb_last_error(None).decode()
