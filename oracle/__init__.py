@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libngref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libngref_cuda.so")
+REF_TLAS_SO = os.path.join(HERE, "_ref", "libngref_tlas.so")
 
 TIE_AOV_INSTANCE = 1
 TIE_AOV_TRIANGLE = 2
@@ -352,6 +353,36 @@ class Reference:
     @property
     def last_kernel_ms(self) -> float:
         return float(self.lib.ngref_last_kernel_ms(self.h))
+
+
+def ref_tlas_available() -> bool:
+    return os.path.exists(REF_TLAS_SO)
+
+
+def ref_tlas_cuda(worlds, per_world, local_bounds, matrices):
+    """The reference's own GPU instance-tree build (src/cuda_tlas.cuh, compiled with its -use_fast_math flags into
+    oracle/_ref/libngref_tlas.so by ref_tlas_cuda.cu) over these matrices: keys in instance order, sorted ids,
+    nodes (2n - 1, 8 words) and roots, as ngb_inspect_tlas gives them. Needs a GPU."""
+    if "tlas" not in _ref_libs:
+        if not os.path.exists(REF_TLAS_SO):
+            raise RuntimeError(f"{REF_TLAS_SO} is not built: run `make -C oracle ref-cuda` where the reference's sources are")
+        lib = C.CDLL(REF_TLAS_SO)
+        lib.ngref_tlas_last_error.restype = C.c_char_p
+        lib.ngref_tlas_build.argtypes = [C.c_int, C.c_int, _f32p, _f32p, C.POINTER(C.c_uint64), C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        _ref_libs["tlas"] = lib
+    lib = _ref_libs["tlas"]
+    n = worlds * per_world
+    lb = np.ascontiguousarray(local_bounds, np.float32).reshape(per_world, 6)
+    m = np.ascontiguousarray(matrices, np.float32).reshape(n, 12)
+    keys = np.zeros(n, np.uint64)
+    ids = np.zeros(n, np.int32)
+    nodes = np.zeros((2 * n - 1, 8), np.int32)
+    roots = np.zeros(worlds, np.int32)
+    if lib.ngref_tlas_build(int(worlds), int(per_world), _p(lb), _p(m), _p(keys, C.c_uint64), _p(ids, C.c_int32),
+                            _p(nodes, C.c_int32), _p(roots, C.c_int32)) != 0:
+        raise RuntimeError(lib.ngref_tlas_last_error().decode())
+    return {"keys": keys, "sorted_ids": ids, "nodes": nodes, "roots": roots}
 
 
 def ref_build_meshes(meshes):
