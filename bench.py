@@ -57,6 +57,8 @@ def parse():
                         "differentiable: 1024 worlds x 128x128 depth+normals, forward+backward against forward; "
                         "uneven: 2048 worlds of 1..200 instances at 32/64/128 px, one CUDA graph per step, against "
                         "bucketed plain renderers")
+    p.add_argument("--no-forms", action="store_true",
+                   help="body_worlds: leave out the differentiable and uneven sub-objects of the line")
     p.add_argument("--profile", action="store_true",
                    help="device-resident steps only (no autotune, e2e, CPU or reference arms): for ncu captures")
     return p.parse_args()
@@ -148,16 +150,56 @@ def traffic_per_image():
     return None
 
 
-def camera_kernel_algorithmic_bytes(wl, per_world, blas_bytes):
-    """Compulsory bytes of one camera-kernel launch: its outputs (depth 4 and ID 4 per pixel, and the picture
-    ray's hit handed to the shade kernel, 16 + 4), the cameras (48 per view), each world's leaf boxes (32 per
-    instance) and instance records (64), and the shared meshes once."""
+def issue_figures():
+    """The camera kernel's issue-side counters from the committed ncu summary's full capture: issue active (% of
+    peak) and threads per warp instruction (of 32), or None."""
+    want = {"issue active (% of peak)": "issue_active_pct", "threads per warp instruction": "threads_per_warp_instruction",
+            "warps active (% of peak)": "warps_active_pct"}
+    out = {}
+    try:
+        for line in open(PROFILE):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if len(cells) >= 2 and cells[0] in want:
+                out[want[cells[0]]] = float(cells[1])
+    except (OSError, ValueError):
+        return None
+    if not out:
+        return None
+    out["source"] = "profiles/camera_tiles_kernel_body_worlds.md (ncu --set full, 1024 worlds)"
+    return out
+
+
+def algorithmic_bytes_per_image(wl, blas_bytes):
+    """Compulsory bytes of one image of the body-worlds step, each counted once: the outputs (RGB 3, depth 4 and
+    object ID 4 bytes per pixel); the inputs (the camera's 48 bytes and the world's body poses, 28 per body); and
+    the tree build: per instance its matrix written and read (48 + 48), its inverse written (48), its box written
+    and read (24 + 24) and its key and id through a two-pass sort (16 bytes, 2 reads and 2 writes); per world its
+    2P - 1 nodes written (32 each); and the shared meshes' nodes and triangles read once per step, spread over the
+    step's images."""
     d = wl.desc
-    views = d.view_count
-    out = views * d.height * d.width * (4 + 4 + 16 + 4)
-    cams = views * 48
-    trees = d.world_count * per_world * (32 + 64)
-    return out + cams + trees + blas_bytes
+    P = d.per_world
+    out = d.height * d.width * (3 + 4 + 4)
+    inputs = 48 + wl.binding["bodies_per_world"] * 28
+    build = P * (48 + 48 + 48 + 24 * 2 + 16 * 4) + (2 * P - 1) * 32 + blas_bytes / d.view_count
+    return out + inputs + build
+
+
+def l2_copy_gbs(torch, dev, mib=16, repeats=200):
+    """Copy bandwidth between two buffers that stay in L2 (2 x 16 MiB), read + write bytes over CUDA-event time:
+    this GPU's on-chip figure for byte rates served from cache."""
+    a = torch.empty(mib << 18, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    a.fill_(1.0)
+    for _ in range(10):
+        b.copy_(a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(repeats):
+        b.copy_(a)
+    e1.record()
+    e1.synchronize()
+    return 2 * a.numel() * 4 * repeats / (e0.elapsed_time(e1) / 1000.0) / 1e9
 
 
 def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64, count_worlds=16):
@@ -346,6 +388,16 @@ def run_ours(args, rank, world, local_rank, dist):
     h2d = pinned_poses[0].numel() * 4 + wl.cameras.nbytes
     d2h = sum(a.numel() * a.element_size() for a in out.values())
 
+    # The other two forms of the metric, on the same GPU in the same run (one GPU only: they are single-GPU
+    # figures): forward + backward against forward at 1024 worlds x 128x128, and the uneven batch.
+    differentiable = uneven = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        with ClockSampler(local_rank) as form_clocks:
+            differentiable = differentiable_figures(dev, K, W)
+            uneven = uneven_figures(dev, K, W)
+        differentiable["clocks"] = uneven["clocks"] = form_clocks.summary()
+    l2_gbs = l2_copy_gbs(torch, dev) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_baseline(wl, steps_np, args.cpu_seconds)
@@ -355,7 +407,8 @@ def run_ours(args, rank, world, local_rank, dist):
     peak, peak_kind = peaks()
     built = ng.build_meshes(d.meshes)
     blas_bytes = built["nodes"].nbytes + built["triangles"].nbytes
-    alg = camera_kernel_algorithmic_bytes(wl, d.per_world, blas_bytes)
+    b_img = algorithmic_bytes_per_image(wl, blas_bytes)
+    alg = b_img * views
     rmed = statistics.median(render_ms)
     cam_ms = stage_ms[0]
     achieved = alg / (cam_ms / 1000.0) / 1e9
@@ -382,15 +435,24 @@ def run_ours(args, rank, world, local_rank, dist):
         "traversal": None if not counts else {
             "bytes_per_image": round(counts["traversal_bytes_per_image"], 1),
             "achieved_gbs": round(counts["traversal_bytes_per_image"] * value / 1e9, 1),
-            "frac_of_hbm_peak": round(counts["traversal_bytes_per_image"] * value / 1e9 / peak, 3)},
+            "l2_copy_gbs": round(l2_gbs, 1),
+            "frac_of_l2_copy": round(counts["traversal_bytes_per_image"] * value / 1e9 / l2_gbs, 3),
+            "what": "bytes the reference's walks fetch per image (32 per node, 64 per child-box pair, 48 per "
+                    "instance inverse, 48 per triangle; the oracle's count) at this build's images/s, against "
+                    "this GPU's copy bandwidth between two buffers resident in L2, measured in this run"},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": KE, "path": "pinned host poses and cameras -> device (copy) -> BatchRenderer.set_body_poses + render(into= one of "
                         "two device image sets) -> pinned host images on a copy stream, overlapping the next step"},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+        # The dominant kernel's launch carries the step's compulsory bytes (B_img per image, algorithmic_bytes_per
+        # _image's terms) over its own CUDA-event duration; whole_step spreads them over the whole step instead.
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
                      "traffic": None if tr is None else int(tr * views),
                      "kernel": "camera_tiles_kernel", "kernel_ms": round(cam_ms, 4),
-                     "algorithmic_bytes_per_launch": int(alg)},
+                     "algorithmic_bytes_per_image": round(b_img, 1), "algorithmic_bytes_per_launch": int(alg),
+                     "whole_step": {"achieved": round(b_img * value / 1e9, 2),
+                                    "frac": round(b_img * value / 1e9 / peak, 5)},
+                     "issue": issue_figures()},
         "cpu_baseline": cpu,
         # Per step: the tree build (compose + per-world build, inter-world links) and the render: the camera-basis
         # kernel and the camera, shade and shadow kernels (tile path), or the camera-basis and one render kernel.
@@ -399,6 +461,8 @@ def run_ours(args, rank, world, local_rank, dist):
                                                                             "leaf_batch", "ms")},
         # The renderers' own device arrays (scene, trees, per-pixel scratch; ngb_device_bytes), not the images.
         "device_mb": round(ng.device_bytes() / 1e6, 1),
+        "differentiable": differentiable,
+        "uneven": uneven,
         "clocks": clk,
     }
 
@@ -490,21 +554,21 @@ def run_large(args, rank, world, local_rank, dist):
     }
 
 
-def run_differentiable(args, rank, world, local_rank, dist):
+def differentiable_figures(dev, K, W, seed=0, fd_world=3):
     """1024 worlds x 128x128, 12 instances: an L2 depth loss against a target rendered from perturbed poses.
     Forward only = poses -> matrices -> render depth + normals -> loss; forward + backward adds the hit
     records, the adjoint kernel and autograd back to positions, quaternions and cameras. Both timed per step
-    with CUDA events; the ratio is the metric."""
+    with CUDA events (L2 flushed before each). The gradient is checked in the same run against central
+    differences (h = 1e-3) of world fd_world's loss in float64, on its 12 instance positions and its camera
+    position, with the target 0.5 nearer on pixels at least 2 px from a silhouette (every pixel's weight about
+    1, so the float32 rounding of the rendered depths stays far below the differences)."""
     import torch
 
     import neraulgraphics_b200 as ng
     from neraulgraphics_b200 import workloads
     from neraulgraphics_b200.autodiff import pose_matrices, render_depth_normals
 
-    torch.cuda.set_device(local_rank)
-    dev = f"cuda:{local_rank}"
-    K, W = args.steps, args.warmup
-    wl = workloads.differentiable_worlds(worlds=1024, seed=rank)
+    wl = workloads.differentiable_worlds(worlds=1024, seed=seed)
     d, info = wl.desc, wl.info
     r = ng.BatchRenderer(d.width, d.height, d.world_count, 1, d.spheres, d.lights, d.floor, d.meshes, d.instances,
                          device=dev)
@@ -547,69 +611,108 @@ def run_differentiable(args, rank, world, local_rank, dist):
             ms.append(e0.elapsed_time(e1))
         return statistics.median(ms)
 
-    with ClockSampler(local_rank) as clocks:
-        fwd_ms = timed(forward)
-        fb_ms = timed(forward_backward)
+    fwd_ms = timed(forward)
+    fb_ms = timed(forward_backward)
     r.set_instance_transforms(pose_matrices(pos, quat, scale).detach().contiguous())
     forward_backward()
     adj_ms = r.last_kernel_ms
-    if rank != 0:
-        return None
+
+    # Central differences of world fd_world's conditioned loss.
+    w = fd_world
+    with torch.no_grad():
+        base = render_depth_normals(r, pose_matrices(pos, quat, scale), cams, wl.fov)[0][w].clone()
+    ids = r.render(cams, wl.fov, 1, rgb=False, object_ids=True, zero_copy=True)["object_ids"][w]
+    edge = torch.zeros_like(ids, dtype=torch.bool)
+    edge[1:, :] |= ids[1:, :] != ids[:-1, :]
+    edge[:-1, :] |= ids[1:, :] != ids[:-1, :]
+    edge[:, 1:] |= ids[:, 1:] != ids[:, :-1]
+    edge[:, :-1] |= ids[:, 1:] != ids[:, :-1]
+    near_edge = torch.nn.functional.max_pool2d(edge[None, None].float(), 5, 1, 2)[0, 0] > 0
+    mask = ~near_edge & torch.isfinite(base)
+    nearer = torch.where(mask, base - 0.5, 0.0)
+
+    def world_loss(pp, qq, cc, grad=False):
+        dep = render_depth_normals(r, pose_matrices(pp, qq, scale), cc, wl.fov)[0][w]
+        value = (torch.where(mask, dep - nearer, 0.0).double() ** 2).sum()
+        return value if grad else float(value)
+
+    p.grad = q.grad = c.grad = None
+    world_loss(p, q, c, grad=True).backward()
+    h = 1e-3
+    got, fd = [], []
+    with torch.no_grad():
+        for i in range(d.per_world):
+            for k in range(3):
+                plus, minus = pos.clone(), pos.clone()
+                plus[w, i, k] += h
+                minus[w, i, k] -= h
+                fd.append((world_loss(plus, quat, cams) - world_loss(minus, quat, cams)) / (2 * h))
+                got.append(float(p.grad[w, i, k]))
+        for k in range(3):
+            plus, minus = cams.clone(), cams.clone()
+            plus[w, k, 3] += h
+            minus[w, k, 3] -= h
+            fd.append((world_loss(pos, quat, plus) - world_loss(pos, quat, minus)) / (2 * h))
+            got.append(float(c.grad[w, k, 3]))
+    got, fd = np.array(got), np.array(fd)
+    err = float(np.linalg.norm(got - fd) / max(np.linalg.norm(fd), 1e-30))
     views = d.view_count
-    return {
-        "metric": "forward+backward time / forward-only time at 1024 worlds x 128x128 depth+normals (L2 depth loss)",
-        "value": round(fb_ms / fwd_ms, 4), "unit": "ratio", "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": round(fb_ms, 4), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded differentiable_worlds scene and perturbed target poses)",
-        "config": {"workload": "differentiable_worlds: 1024 worlds x 12 instances (icosphere 1280 / box 12 tris), "
-                               "128x128, depth+normals, target poses N(0, 0.01) position and 0.02 rad rotation",
-                   "l2": "flushed before every timed step (256 MiB write)"},
-        "forward_ms": round(fwd_ms, 4), "forward_backward_ms": round(fb_ms, 4), "adjoint_kernel_ms": round(adj_ms, 4),
-        "forward_images_per_s": round(views / (fwd_ms / 1000.0), 1),
-        "forward_backward_images_per_s": round(views / (fb_ms / 1000.0), 1),
-        "gradient_check": "float64 reference and central differences within 1e-3 (tests/test_gpu_adjoint.py)",
-        "clocks": clocks.summary(),
-    }
+    return {"forward_ms": round(fwd_ms, 4), "forward_backward_ms": round(fb_ms, 4),
+            "ratio": round(fb_ms / fwd_ms, 4), "adjoint_kernel_ms": round(adj_ms, 4),
+            "forward_images_per_s": round(views / (fwd_ms / 1000.0), 1),
+            "forward_backward_images_per_s": round(views / (fb_ms / 1000.0), 1),
+            "gradient_rel_err": round(err, 6),
+            "gradient_check": f"central differences (h = 1e-3) of world {w}'s float64 loss on its {d.per_world} "
+                              f"instance positions and its camera position ({len(got)} parameters); the tests add "
+                              "a float64 CPU restatement of the gradient on sampled worlds",
+            "workload": "differentiable_worlds: 1024 worlds x 12 instances (icosphere 1280 / box 12 tris), 128x128, "
+                        "depth+normals, L2 depth loss against a target rendered from poses perturbed by N(0, 0.01) "
+                        "position and 0.02 rad rotation"}
 
 
-def run_uneven(args, rank, world, local_rank, dist):
-    """2048 worlds of 1..200 instances at 32x32, 64x64 or 128x128, RGB + depth + ID. Per step the instance
-    matrices of the random walk go to the device (one copy into the graph's input), then one CUDA graph
-    replays the whole step: the tree build of every world and the render of every view (camera, shade and
-    shadow kernels). Against the same steps through plain renderers, one per (resolution, instance count)
-    bucket, launched one after another."""
+def run_differentiable(args, rank, world, local_rank, dist):
+    """The differentiable form alone (differentiable_figures): forward + backward over forward-only time."""
     import torch
-
-    import neraulgraphics_b200 as ng
-    from neraulgraphics_b200 import workloads
 
     torch.cuda.set_device(local_rank)
     dev = f"cuda:{local_rank}"
     K, W = args.steps, args.warmup
-    wl = workloads.uneven_worlds(seed=rank)
-    mats = torch.from_numpy(workloads.walk_uneven(wl, W + K, seed=1 + rank)).to(dev)
+    with ClockSampler(local_rank) as clocks:
+        f = differentiable_figures(dev, K, W, seed=rank)
+    if rank != 0:
+        return None
+    return {
+        "metric": "forward+backward time / forward-only time at 1024 worlds x 128x128 depth+normals (L2 depth loss)",
+        "value": f["ratio"], "unit": "ratio", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": f["forward_backward_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded differentiable_worlds scene and perturbed target poses)",
+        "config": {"workload": f["workload"], "l2": "flushed before every timed step (256 MiB write)"},
+        **{k: v for k, v in f.items() if k not in ("ratio", "workload")},
+        "clocks": clocks.summary(),
+    }
+
+
+def uneven_figures(dev, K, W, seed=0, buckets=False):
+    """2048 worlds of 1..200 instances at 32x32, 64x64 or 128x128, RGB + depth + ID. Per step the instance
+    matrices of the random walk go to the device (one copy into the graph's input), then one CUDA graph
+    replays the whole step: the tree build of every world and the render of every view (camera, shade and
+    shadow kernels). With buckets, also the same steps through plain renderers, one per (resolution, instance
+    count) bucket, launched one after another."""
+    import torch
+
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+    from neraulgraphics_b200.autotune import tune
+
+    wl = workloads.uneven_worlds(seed=seed)
+    mats = torch.from_numpy(workloads.walk_uneven(wl, W + K, seed=1 + seed)).to(dev)
     cams = torch.from_numpy(wl["cameras"]).to(dev)
     r = ng.UnevenBatchRenderer(wl["worlds"], lights=wl["lights"], floor=wl["floor"], meshes=wl["meshes"], device=dev)
     kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True)
     static = mats[0].clone()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    # The tile kernel's shape, timed on this batch.
     r.set_instance_transforms(static)
-    shapes = []
-    from neraulgraphics_b200.autotune import TILE_CANDIDATES
-    for threads, regs, _, _ in TILE_CANDIDATES:
-        r.set_tuning(kernel=3, threads_per_block=threads, registers=regs)
-        r.render(cams, wl["fov"], 1, **kw)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(3):
-            r.render(cams, wl["fov"], 1, **kw)
-        e1.record()
-        e1.synchronize()
-        shapes.append((e0.elapsed_time(e1) / 3, threads, regs))
-    best = min(shapes)
-    r.set_tuning(kernel=3, threads_per_block=best[1], registers=best[2])
+    tuned = tune(r, cams, wl["fov"], rgb=True, depth=True, object_ids=True, use_cache=False)
     # One graph for the whole step, captured after warm-up renders on the capture stream.
     side = torch.cuda.Stream()
     side.wait_stream(torch.cuda.current_stream())
@@ -623,13 +726,14 @@ def run_uneven(args, rank, world, local_rank, dist):
     with torch.cuda.graph(graph):
         r.set_instance_transforms(static)
         out = r.render(cams, wl["fov"], 1, **kw)
-    # The graph's images equal an eager render's.
+    # The graph's images equal an eager render's, after a pose change.
     static.copy_(mats[1])
     graph.replay()
     torch.cuda.synchronize()
-    graph_ids = out["object_ids"].clone()
+    from_graph = {k: v.clone() for k, v in out.items()}
     r.set_instance_transforms(mats[1].clone())
-    same = bool(torch.equal(graph_ids, r.render(cams, wl["fov"], 1, **kw)["object_ids"]))
+    eager = r.render(cams, wl["fov"], 1, **kw)
+    same = all(bool(torch.equal(from_graph[k], eager[k])) for k in from_graph)
 
     def timed(step):
         for s in range(W):
@@ -650,15 +754,23 @@ def run_uneven(args, rank, world, local_rank, dist):
         static.copy_(mats[s])
         graph.replay()
 
-    with ClockSampler(local_rank) as clocks:
-        graph_ms = timed(graph_step)
-    # Plain renderers, one per (resolution, instance count) bucket, launched one after another.
+    graph_ms = timed(graph_step)
+    views = len(wl["worlds"])
     first = r.instance_first
-    buckets = {}
+    res = {"images_per_s": round(views / (graph_ms / 1000.0), 1), "ms_per_step": round(graph_ms, 4),
+           "kernel_shape": {k: tuned[k] for k in tuned if k != "timings"},
+           "shape_timings_ms": {f"{t['threads']}/{t['registers']}" + (f" {t['tile']}" if "tile" in t else ""):
+                                round(t["ms"], 4) for t in tuned["timings"]},
+           "graph_matches_eager": same, "gpu_launches_per_step": 6,
+           "workload": f"uneven_worlds: {views} worlds, {int(first[-1])} instances, {r.pixel_count} pixels; six "
+                       "meshes of 12 to 20480 triangles; one light, spp 1, RGB+depth+ID"}
+    if not buckets:
+        return res
+    groups = {}
     for w, (size, _, insts) in enumerate(wl["worlds"]):
-        buckets.setdefault((size, len(insts)), []).append(w)
+        groups.setdefault((size, len(insts)), []).append(w)
     plain = []
-    for (size, count), ws in sorted(buckets.items()):
+    for (size, count), ws in sorted(groups.items()):
         insts = wl["worlds"][ws[0]][2]
         rb = ng.BatchRenderer(size, size, len(ws), 1, [], wl["lights"], wl["floor"], wl["meshes"], insts, device=dev)
         idx = torch.from_numpy(np.concatenate([np.arange(first[w], first[w + 1]) for w in ws])).to(dev)
@@ -670,25 +782,32 @@ def run_uneven(args, rank, world, local_rank, dist):
             rb.render(cb, wl["fov"], 1, **kw)
 
     plain_ms = timed(plain_step)
+    res["bucketed_plain"] = {"value": round(views / (plain_ms / 1000.0), 1), "unit": "images/s",
+                             "ms_per_step": round(plain_ms, 4), "buckets": len(plain),
+                             "what": "one plain BatchRenderer per (resolution, instance count) bucket, set_instance_"
+                                     "transforms + render each, launched one after another"}
+    return res
+
+
+def run_uneven(args, rank, world, local_rank, dist):
+    """The uneven form alone (uneven_figures), against bucketed plain renderers."""
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    K, W = args.steps, args.warmup
+    with ClockSampler(local_rank) as clocks:
+        f = uneven_figures(dev, K, W, seed=rank, buckets=True)
     if rank != 0:
         return None
-    views = len(wl["worlds"])
     return {
         "metric": "images/s at 2048 uneven worlds (1..200 instances, 32/64/128 px) RGB+depth+ID, one CUDA graph per "
                   "step (tree build + render)",
-        "value": round(world * views / (graph_ms / 1000.0), 1), "unit": "images/s", "n_gpus": world, "steps": K,
-        "warmup": W, "ms_per_step": round(graph_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "value": round(world * f["images_per_s"], 1), "unit": "images/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": f["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uneven_worlds scene and random-walk poses)",
-        "config": {"workload": f"uneven_worlds: {views} worlds, {int(first[-1])} instances, {r.pixel_count} pixels; "
-                               "six meshes of 12 to 20480 triangles; one light, spp 1",
-                   "l2": "flushed before every timed step (256 MiB write)"},
-        "kernel_shape": {"threads": best[1], "registers": best[2], "timings_ms": [round(x[0], 4) for x in shapes]},
-        "graph_matches_eager": same,
-        "bucketed_plain": {"value": round(views / (plain_ms / 1000.0), 1), "unit": "images/s",
-                           "ms_per_step": round(plain_ms, 4), "buckets": len(plain),
-                           "what": "one plain BatchRenderer per (resolution, instance count) bucket, set_instance_"
-                                   "transforms + render each, launched one after another"},
-        "gpu_launches_per_step": 6,
+        "config": {"workload": f["workload"], "l2": "flushed before every timed step (256 MiB write)"},
+        **{k: v for k, v in f.items() if k not in ("images_per_s", "ms_per_step", "workload")},
         "clocks": clocks.summary(),
     }
 

@@ -469,6 +469,50 @@ def test_uneven_worlds_are_each_worlds_own_render(torch_cuda):
         assert_same_images(mine, want, ties=want["ties"])
 
 
+def test_uneven_step_captured_in_a_cuda_graph_is_the_eager_step(torch_cuda):
+    """One uneven step (every world's tree build and the render's kernels) captured into a CUDA graph, replayed
+    after the matrices changed in place: RGB, depth and IDs bit for bit those of the same step run eagerly, and
+    those of the oracle (apart from near ties)."""
+    torch = torch_cuda
+    worlds, meshes, floor, lights, mats, cams = uneven_scene(seed=8)
+    u = ng.UnevenBatchRenderer(worlds, lights=lights, floor=floor, meshes=meshes, device="cuda:0")
+    moved = mats.copy()
+    rng = np.random.default_rng(2)
+    moved[:, :, 3] += rng.normal(0.0, 0.05, size=moved[:, :, 3].shape).astype(np.float32)
+    static = torch.from_numpy(mats).cuda()
+    cams_dev = torch.from_numpy(cams).cuda()
+    kw = dict(rgb=True, depth=True, object_ids=True, zero_copy=True, frame=4)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            u.set_instance_transforms(static)
+            u.render(cams_dev, 1.0, 1, **kw)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        u.set_instance_transforms(static)
+        out = u.render(cams_dev, 1.0, 1, **kw)
+    static.copy_(torch.from_numpy(moved))
+    graph.replay()
+    torch.cuda.synchronize()
+    replayed = {k: v.cpu().numpy() for k, v in out.items()}
+    u.set_instance_transforms(moved)
+    eager = u.render(cams, 1.0, 1, rgb=True, depth=True, object_ids=True, frame=4)
+    for k in ("rgb", "depth", "object_ids"):
+        a, b = np.ascontiguousarray(replayed[k]), np.ascontiguousarray(eager[k])
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), k
+    first = u.instance_first
+    for w, (width, height, insts) in enumerate(worlds):
+        desc = ng.SceneDesc(width, height, 1, 1, [], lights, floor, meshes, insts)
+        o = O.Oracle(desc)
+        if insts:
+            o.set_instance_transforms(moved[first[w]:first[w + 1]].reshape(1, len(insts), 3, 4))
+        want = o.render(cams[w:w + 1], 1.0, 1, rgb=True, depth=True, object_ids=True, frame=4, ties=True)
+        assert_same_images({k: u.image(v, w)[None] for k, v in replayed.items()}, want, ties=want["ties"])
+
+
 def test_ray_queries_on_both_kernels(torch_cuda):
     """Ray queries through the persistent kernel's walk (the default) and the per-thread kernel: the same
     distances, normals and IDs, with rays of zero length, rays stopped by max_distance and rays in worlds
