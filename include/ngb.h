@@ -189,6 +189,17 @@ typedef struct {
     const int32_t *object_id;
 } ngb_ray_hits;
 
+/* neraulgraphics::Camera (include/neraulgraphics/scene.h:125-132): the single-view renderer's camera, used as
+ * given: an eye, a right / up / forward basis, tan(fov / 2) and width / height. */
+typedef struct {
+    ngb_vec3 position;
+    ngb_vec3 right;
+    ngb_vec3 up;
+    ngb_vec3 forward;
+    float fov_scale;
+    float aspect;
+} ngb_camera;
+
 typedef struct ngb_renderer ngb_renderer;
 
 /* ---- lifetime -------------------------------------------------------------------------------------- */
@@ -357,6 +368,35 @@ float ngb_last_kernel_ms(const ngb_renderer *r);
  * kernels (camera rays, shading, shadow rays), 1 for the others (the whole launch). Up to capacity entries are
  * written. No counterpart in the reference, which times the render as one launch. */
 int ngb_last_stage_ms(ngb_renderer *r, float *ms, int32_t capacity, int32_t *count);
+
+/* ---- one view: the single-view Renderer ------------------------------------------------------------- */
+
+/* A renderer made by ngb_create with world_count 1 and cameras_per_world 1 serves as the reference's single-view
+ * Renderer (include/neraulgraphics/renderer.h:135-277): its instances move with ngb_set_instance_transforms, its
+ * ray queries are ngb_cast_rays with rays_per_world the ray count, and these calls render its view. */
+
+/* A camera at position looking at target, fov the vertical field of view in radians (make_camera,
+ * src/renderer.cpp:39-59: the basis in double, then rounded). */
+int ngb_make_camera(ngb_vec3 position, ngb_vec3 target, ngb_vec3 world_up, float fov, int32_t width, int32_t height,
+    ngb_camera *out);
+
+/* Renderer::render (src/renderer.cpp:104-108; src/cuda_backend.cu:365-374, 642-655): the picture of
+ * samples_per_frame jittered rays per pixel, averaged with the frames before it (frame 0 starts the average
+ * afresh; frame k > 0 adds its samples to it), as 0xAARRGGBB pixels (alpha 0xFF, gamma-encoded), rows top to
+ * bottom, copied into the caller's host buffer argb (width x height; the rows drawn, ngb_set_rows). Waits for the
+ * work. Checks as the reference (src/validate.cpp:82-89). */
+int ngb_render_view(ngb_renderer *r, const ngb_camera *camera, int32_t frame, int32_t samples_per_frame,
+    uint32_t *argb);
+
+/* Renderer::render_frame (src/renderer.cpp:174-182; src/cuda_backend.cu:376-407): the images asked for in the
+ * renderer's own device buffers, described in *out (views 1): RGB the running average's bytes (the picture of
+ * ngb_render_view, which it also advances), depth, normals and IDs from one ray through each pixel's middle. */
+int ngb_render_view_frame(ngb_renderer *r, const ngb_camera *camera, int32_t frame, int32_t samples_per_frame,
+    uint32_t outputs, ngb_batch_frame *out);
+
+/* The last view render's 0xAARRGGBB pixels in the renderer's device memory (valid until the next view render):
+ * for a caller that shows the picture from the GPU. No counterpart in the reference, whose render copies them. */
+int ngb_view_pixels(ngb_renderer *r, const uint32_t **argb);
 
 /* ---- worlds of uneven sizes ------------------------------------------------------------------------- */
 

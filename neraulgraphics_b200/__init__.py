@@ -15,7 +15,7 @@ from . import _abi
 from ._abi import (MAX_LIGHTS, MAX_SPHERES, OBJECT_FLOOR, OBJECT_INSTANCE, OBJECT_NONE, OBJECT_SPHERE,
                    OUTPUT_DEPTH, OUTPUT_NORMAL, OUTPUT_OBJECT_ID, OUTPUT_RGB)
 from ._lib import CudaError, DeviceTimeout
-from .renderer import BatchRenderer, UnevenBatchRenderer
+from .renderer import BatchRenderer, Renderer, UnevenBatchRenderer
 from .scene import (Camera, Environment, Instance, Light, Material, Mesh, Plane, SceneDesc, Sphere, Transform, cylinder,
                     identity_transform, look_at, make_box, make_camera, make_icosphere, make_material, make_transform)
 

@@ -75,6 +75,12 @@ class SceneC(C.Structure):
                 ("instance_count", C.c_int32), ("device", C.c_int32)]
 
 
+class CameraC(C.Structure):
+    """ngb_camera: neraulgraphics::Camera (include/neraulgraphics/scene.h:125-132)."""
+    _fields_ = [("position", Vec3), ("right", Vec3), ("up", Vec3), ("forward", Vec3), ("fov_scale", C.c_float),
+                ("aspect", C.c_float)]
+
+
 class BatchFrameC(C.Structure):
     _fields_ = [("memory", C.c_int32), ("device_id", C.c_int32), ("views", C.c_int32), ("width", C.c_int32),
                 ("height", C.c_int32), ("rgb", C.c_void_p), ("depth", C.c_void_p), ("normal", C.c_void_p),

@@ -77,6 +77,12 @@ def lib():
     L.ngb_build_tlas_noalloc.argtypes = [C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
+    L.ngb_make_camera.argtypes = [_abi.Vec3, _abi.Vec3, _abi.Vec3, C.c_float, C.c_int32, C.c_int32,
+                                  C.POINTER(_abi.CameraC)]
+    L.ngb_render_view.argtypes = [_vp, C.POINTER(_abi.CameraC), C.c_int32, C.c_int32, _vp]
+    L.ngb_render_view_frame.argtypes = [_vp, C.POINTER(_abi.CameraC), C.c_int32, C.c_int32, C.c_uint32,
+                                        C.POINTER(_abi.BatchFrameC)]
+    L.ngb_view_pixels.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.ngb_set_rows.argtypes = [_vp, C.c_int32, C.c_int32]
     L.ngb_device_bytes.argtypes = []
     L.ngb_device_bytes.restype = C.c_int64

@@ -101,7 +101,18 @@ struct RenderArgs {
     // Uneven views: per view its first tile of 4 x 4 pixels, and their total (the camera kernel's paired tiles).
     const int *view_pair_tile;
     long long total_pair_tiles;
+    // Single-view renders (Renderer::render / render_frame): camera_basis already holds each view's camera as the
+    // caller gave it (no matrix, no renormalising), and the picture's linear radiance per pixel (the average of
+    // its samples this frame) goes to radiance instead of bytes to rgb, for launch_accumulate.
+    int basis_given;
+    float4 *radiance;
 };
+
+// The running average of a single-view renderer's pictures (render_pixel, src/render_core.h:288-301): per pixel
+// acc = this frame's radiance with count 1 at frame 0, else the previous acc plus it; the average's sRGB bytes
+// as 0xAARRGGBB into argb and, when rgb is not null, as red, green, blue bytes.
+cudaError_t launch_accumulate(const float4 *radiance, float4 *accum, int frame, long long pixels, const float *srgb_table,
+    uint32_t *argb, uint8_t *rgb, cudaStream_t stream);
 
 // The per-view camera basis of camera_from_matrix (src/render_core.h:264-273): (position.xyz, right.x)
 // (right.yz, up.xy) (up.z, forward.xyz) for each view.

@@ -365,6 +365,11 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
 __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, const RayArgs &ra, Lane &L,
     const ColdRef &cold) {
     const long long pix = cold.pix();
+    if (L.job == JOB_SHADOW_PIXEL && a.radiance) {  // a single-view render: the shadowed radiance, over pic_hit
+        if (L.blocked) a.radiance[pix] = a.pic_hit[pix];
+        L.state = ST_IDLE;
+        return;
+    }
     if (L.job == JOB_SHADOW_PIXEL) {  // the shade kernel's bytes: shadowed over pic_code, lit in shadow_d.w
         const int bytes = L.blocked ? a.pic_code[pix] : __float_as_int(a.shadow_d[pix].w);
         uint8_t *o = a.rgb + 3 * static_cast<size_t>(pix);
@@ -593,7 +598,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayA
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
     if (!rays && !shadows) {
-        e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+        if (!a.basis_given) e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
         if (e != cudaSuccess) return e;
     }
     kernel<<<static_cast<unsigned>(blocks), THREADS, smem, stream>>>(s, a, ra, counter, total, kinds, tiles_x,

@@ -157,6 +157,10 @@ struct Renderer {
     DevBuf<float4> pic_hit, shadow_o, shadow_d;  // the tile render's per-pixel hand-over between its kernels
     DevBuf<int> pic_code, shadow_self;
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
+    // Single-view renders (ngb_render_view): the running sums of the picture (zeroed when made, so a first render
+    // with frame > 0 adds to zero), this frame's radiance, and the average's 0xAARRGGBB pixels.
+    DevBuf<float4> view_accum, view_radiance;
+    DevBuf<uint32_t> view_argb;
     bool reflective = false;                  // some material bounces light (reflectivity >= 1e-3)
     int kernel_choice = 0;                    // 0: automatic, 1: per pixel, 2: persistent, 3: tiles
     PersistentTuning tuning{128, 28, 72, 16};
@@ -251,7 +255,8 @@ struct Renderer {
     void set_geom_poses(const float *xpos, const float *xmat, int memory);
     void check_render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory);
     void render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
-        float *depth, float *normal, int32_t *ids);
+        float *depth, float *normal, int32_t *ids, const ngb_camera *view = nullptr);
+    void check_view(const ngb_camera *camera, int frame, int spp);
     void cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory, ngb_ray_hits *out,
         float *distance, float *normal, int32_t *ids);
     int rows() const { return band_rows > 0 ? band_rows : height; }
@@ -581,6 +586,7 @@ void Renderer::teardown() {
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
     hit_instance.release(), hit_triangle.release(), hit_u.release(), hit_v.release(), error_flag.release();
     world_first.release(), view_info.release(), view_pair_tile.release();
+    view_accum.release(), view_radiance.release(), view_argb.release();
     if (previous >= 0 && previous != device) cudaSetDevice(previous);
 }
 
@@ -900,12 +906,26 @@ void Renderer::check_render(const float *cams, float fov, int spp, unsigned outp
         require(all_finite(cams, 12 * static_cast<size_t>(worlds) * cpw), "a camera has a NaN or infinite value");
 }
 
+// src/renderer.cpp:104-108, 174-182 and src/validate.cpp:82-89: a single-view render's checks.
+void Renderer::check_view(const ngb_camera *c, int frame, int spp) {
+    require(worlds == 1 && cpw == 1 && !uneven,
+        "a view render needs a renderer of one world seen by one camera (world_count 1, cameras_per_world 1)");
+    require(c != nullptr, "camera must not be null");
+    require(frame >= 0, "frame must be 0 or more, got " + std::to_string(frame));
+    require(spp >= 1, "samples_per_frame must be 1 or more, got " + std::to_string(spp));
+    const float v[14] = {c->position.x, c->position.y, c->position.z, c->right.x, c->right.y, c->right.z, c->up.x,
+        c->up.y, c->up.z, c->forward.x, c->forward.y, c->forward.z, c->fov_scale, c->aspect};
+    require(all_finite(v, 14), "camera has a NaN or infinite value (is its target on the view axis, or up parallel to it?)");
+}
+
 void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
-    float *depth, float *normal, int32_t *ids) {
-    Range range("ngb render");
+    float *depth, float *normal, int32_t *ids, const ngb_camera *view) {
+    Range range(view ? "ngb render_view" : "ngb render");
     const int views = worlds * cpw;
     const float *cam = cams;
-    if (memory == NGB_MEMORY_HOST) {
+    if (view) {
+        cam = nullptr;
+    } else if (memory == NGB_MEMORY_HOST) {
         cameras.ensure(12 * static_cast<size_t>(views));
         CK(cudaMemcpyAsync(cameras.p, cams, 12 * static_cast<size_t>(views) * sizeof(float), cudaMemcpyHostToDevice, stream));
         cam = cameras.p;
@@ -914,6 +934,17 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     a.cameras = cam;
     a.fov_scale = std::tan(fov * 0.5f);  // tanf on the host, as the reference's CPU backend computes it
     a.aspect = uneven ? 1.0f : static_cast<float>(width) / static_cast<float>(height);
+    if (view) {
+        // The camera as the caller gave it (src/cuda_backend.cu:651-652 passes it to the kernel unchanged).
+        a.fov_scale = view->fov_scale;
+        a.aspect = view->aspect;
+        const float4 basis[3] = {make_float4(view->position.x, view->position.y, view->position.z, view->right.x),
+            make_float4(view->right.y, view->right.z, view->up.x, view->up.y),
+            make_float4(view->up.z, view->forward.x, view->forward.y, view->forward.z)};
+        a.camera_basis = camera_basis.ensure(3);
+        CK(cudaMemcpyAsync(a.camera_basis, basis, sizeof(basis), cudaMemcpyHostToDevice, stream));
+        a.basis_given = 1;
+    }
     a.width = width;
     a.height = height;
     a.row_first = band_first;
@@ -944,8 +975,17 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     // else takes the per-pixel kernel, which runs trace in full. Automatic: the tile kernels (candidate lists
     // for worlds of at most TILE_MAX_INSTANCES instances, a packet walk of the world tree above).
     const bool persistent_ok = spp == 1 && params.light_count <= 1 && !reflective;
-    const bool tiles = persistent_ok && (uneven || kernel_choice == 3 || kernel_choice == 0);
-    const bool persistent = !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
+    // A view render's picture is a running average of radiance, which the tile and per-pixel kernels hand over.
+    const bool tiles = persistent_ok && (uneven || kernel_choice == 3 || kernel_choice == 0 || (view && kernel_choice == 2));
+    const bool persistent = !view && !tiles && persistent_ok && (kernel_choice == 0 || kernel_choice == 2);
+    if (view && a.rgb) {
+        a.radiance = view_radiance.ensure(pixels());
+        if (view_accum.n < pixels()) {
+            view_accum.ensure(pixels());
+            CK(cudaMemsetAsync(view_accum.p, 0, pixels() * sizeof(float4), stream));
+        }
+        view_argb.ensure(pixels());
+    }
     require(!uneven || tiles, "worlds of uneven sizes render with one sample per pixel, at most one light and no "
         "reflective material");
     // Inside a CUDA graph capture the timing events would be graph nodes whose times cannot be read: the
@@ -979,6 +1019,9 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
         CK(launch_render(params, a, stream));
         stages = 1;
     }
+    if (a.radiance)
+        CK(launch_accumulate(a.radiance, view_accum.p, frame, static_cast<long long>(pixels()), srgb_table.p,
+            view_argb.p, a.rgb, stream));
     if (timed) {
         CK(cudaEventRecord(ev_stop, stream));
         timing_pending = true;
@@ -1239,6 +1282,72 @@ int ngb_render_host(ngb_renderer *h, const float *cams, float fov, int32_t spp, 
         CK(cudaEventRecord(r.ev_done, r.stream));
         r.wait(r.ev_done, r.timeout);
         if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
+    });
+}
+
+int ngb_make_camera(ngb_vec3 position, ngb_vec3 target, ngb_vec3 world_up, float fov, int32_t width, int32_t height,
+    ngb_camera *out) {
+    if (!out || width <= 0 || height <= 0) {
+        ngb::set_global_error("out must not be null and width and height must be positive");
+        return NGB_INVALID_ARGUMENT;
+    }
+    // In double, then rounded (src/renderer.cpp:39-59).
+    struct V {
+        double x, y, z;
+    };
+    auto sub = [](V a, V b) { return V{a.x - b.x, a.y - b.y, a.z - b.z}; };
+    auto cross = [](V a, V b) { return V{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; };
+    auto unit = [](V a) {
+        const double n = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+        return V{a.x / n, a.y / n, a.z / n};
+    };
+    auto f32 = [](V a) { return ngb_vec3{static_cast<float>(a.x), static_cast<float>(a.y), static_cast<float>(a.z)}; };
+    const V fwd = unit(sub(V{target.x, target.y, target.z}, V{position.x, position.y, position.z}));
+    const V right = unit(cross(fwd, V{world_up.x, world_up.y, world_up.z}));
+    const V up = cross(right, fwd);
+    *out = ngb_camera{position, f32(right), f32(up), f32(fwd), std::tan(fov * 0.5f),
+        static_cast<float>(width) / static_cast<float>(height)};
+    ngb::set_global_error("");
+    return NGB_OK;
+}
+
+int ngb_render_view(ngb_renderer *h, const ngb_camera *camera, int32_t frame, int32_t spp, uint32_t *argb) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        r.check_view(camera, frame, spp);
+        ngb::require(argb != nullptr, "argb must not be null");
+        const size_t px = r.pixels();
+        r.render(nullptr, 0.0f, spp, NGB_OUTPUT_RGB, frame, NGB_MEMORY_DEVICE, r.out_rgb.ensure(3 * px), nullptr,
+            nullptr, nullptr, camera);
+        CK(cudaMemcpyAsync(argb, r.view_argb.p, px * sizeof(uint32_t), cudaMemcpyDeviceToHost, r.stream));
+        r.queue_error_read();
+        CK(cudaEventRecord(r.ev_done, r.stream));
+        r.wait(r.ev_done, r.timeout);
+        if (*r.host_error) throw ngb::CudaFailure(-1, ngb::device_error_message(*r.host_error));
+    });
+}
+
+int ngb_render_view_frame(ngb_renderer *h, const ngb_camera *camera, int32_t frame, int32_t spp, uint32_t outputs,
+    ngb_batch_frame *out) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        constexpr unsigned ALL = NGB_OUTPUT_RGB | NGB_OUTPUT_DEPTH | NGB_OUTPUT_NORMAL | NGB_OUTPUT_OBJECT_ID;
+        r.check_view(camera, frame, spp);
+        ngb::require(outputs != 0, "render_frame needs at least one output");
+        ngb::require((outputs & ~ALL) == 0, "unknown output bits in " + std::to_string(outputs));
+        ngb::require(out != nullptr, "out must not be null");
+        const size_t px = r.pixels();
+        uint8_t *rgb = (outputs & NGB_OUTPUT_RGB) ? r.out_rgb.ensure(3 * px) : nullptr;
+        float *depth = (outputs & NGB_OUTPUT_DEPTH) ? r.out_depth.ensure(px) : nullptr;
+        float *normal = (outputs & NGB_OUTPUT_NORMAL) ? r.out_normal.ensure(3 * px) : nullptr;
+        int32_t *ids = (outputs & NGB_OUTPUT_OBJECT_ID) ? r.out_id.ensure(px) : nullptr;
+        r.render(nullptr, 0.0f, spp, outputs, frame, NGB_MEMORY_DEVICE, rgb, depth, normal, ids, camera);
+        *out = ngb_batch_frame{NGB_MEMORY_DEVICE, r.device, 1, r.width, r.rows(), rgb, depth, normal, ids};
+    });
+}
+
+int ngb_view_pixels(ngb_renderer *h, const uint32_t **argb) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(argb != nullptr, "argb must not be null");
+        *argb = r.view_argb.p;
     });
 }
 

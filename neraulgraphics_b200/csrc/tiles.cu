@@ -659,6 +659,9 @@ __device__ __forceinline__ bool shadow_misses_own_mesh(const SceneParams &s, int
 // first bounce, src/render_core.h:202-245): a pixel with nothing left to trace gets its bytes here; a lit
 // surface leaves its shadow ray (origin, light distance) (direction, lit bytes) and its shadowed bytes (over
 // the hit's code) for the shadow kernel. shadow_o.w = 0 marks a pixel without a shadow ray.
+// RADIANCE: a single-view render's kernel (a.radiance set), keeping each pixel's radiance for its running average;
+// otherwise the batch's, writing bytes.
+template <bool RADIANCE>
 __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ SceneParams s, const RenderArgs a,
     long long pixels) {
     const long long per_view = static_cast<long long>(a.width) * a.rows;
@@ -689,7 +692,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
         const float3 d = picture_ray(a, x, y, width, height, aspect, right, up, fwd, rng);
         const int code = a.pic_code[p];
         const float4 h = a.pic_hit[p];
-        float3 radiance;
+        float3 radiance, shadowed = zero;
         float3 self_normal = zero, self_point = zero;  // the picture hit's shading normal and point
         bool pending = false;
         float3 so = zero, sd = zero;
@@ -743,17 +746,26 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
                         const float3 diffuse = zero + lit * fmaxf(0.0f, dot(light_dir, normal));
                         const float3 specular =
                             zero + lit * powf(fmaxf(0.0f, dot(reflect(light_dir, normal), d)), mat.exponent);
-                        shadow_bytes = rgb_bytes(s.srgb_table, radiance);
+                        if (RADIANCE) shadowed = radiance;
+                        else shadow_bytes = rgb_bytes(s.srgb_table, radiance);
                         radiance = radiance_of(mat, s.ambient, diffuse, specular);
                         pending = true;
                     }
                 }
             }
         }
-        const int bytes = rgb_bytes(s.srgb_table, radiance);
-        // A shadow ray whose answer cannot change the pixel (lit and shadowed bytes equal, as where the surface
-        // faces away from the light and the highlight rounds away) is not traced: the bytes are final here.
-        if (pending && bytes == shadow_bytes) pending = false;
+        int bytes = 0;
+        if (RADIANCE) {
+            // A single-view render keeps the sample's radiance (sample_pixel's sum over one sample) for its running
+            // average: the lit one, which a blocking shadow ray replaces with the shadowed one (kept in pic_hit).
+            const float3 lit = (zero + radiance) * (1.0f / 1.0f);
+            a.radiance[p] = make_float4(lit.x, lit.y, lit.z, 0.0f);
+        } else {
+            bytes = rgb_bytes(s.srgb_table, radiance);
+            // A shadow ray whose answer cannot change the pixel (lit and shadowed bytes equal, as where the surface
+            // faces away from the light and the highlight rounds away) is not traced: the bytes are final here.
+            if (pending && bytes == shadow_bytes) pending = false;
+        }
         if (pending) {
             lit_bytes = bytes;
             // The shadow ray's own mesh: walked first when the ray starts on its body's side (the light is behind
@@ -768,9 +780,14 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
             a.shadow_self[p] = self;
             a.shadow_o[p] = make_float4(so.x, so.y, so.z, sdist);
             a.shadow_d[p] = make_float4(sd.x, sd.y, sd.z, __int_as_float(lit_bytes));
-            a.pic_code[p] = shadow_bytes;
+            if (RADIANCE) {
+                const float3 dark = (zero + shadowed) * (1.0f / 1.0f);
+                a.pic_hit[p] = make_float4(dark.x, dark.y, dark.z, 0.0f);
+            } else {
+                a.pic_code[p] = shadow_bytes;
+            }
         } else {
-            put_rgb(a.rgb, p, bytes);
+            if (!RADIANCE) put_rgb(a.rgb, p, bytes);
             a.shadow_o[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
     }
@@ -894,7 +911,11 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                         ht, hu, hv, max_steps, a.error_flag);
                 }
             }
-            if (pending) put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));
+            if (pending && a.radiance) {
+                if (blocked) a.radiance[T.pix] = a.pic_hit[T.pix];
+            } else if (pending) {
+                put_rgb(a.rgb, T.pix, blocked ? a.pic_code[T.pix] : __float_as_int(d4.w));
+            }
         }
     }
 }
@@ -934,7 +955,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         mark(after_shade);
         return e;
     }
-    e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+    if (!a.basis_given) e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
     // Both kinds of camera ray: paired 4 x 4 tiles (pair_tile_at).
     const bool paired = a.rgb && aov && (!a.view_info || a.view_pair_tile);
     if (e == cudaSuccess && paired) {
@@ -958,7 +979,8 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     if (e != cudaSuccess) return e;
     long long blocks = (pixels + 255) / 256;
     if (blocks > 32LL * sms) blocks = 32LL * sms;
-    shade_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(s, a, pixels);
+    if (a.radiance) shade_kernel<true><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(s, a, pixels);
+    else shade_kernel<false><<<static_cast<unsigned>(blocks), 256, 0, stream>>>(s, a, pixels);
     e = cudaGetLastError();
     mark(after_shade);
     if (e != cudaSuccess || s.light_count != 1) return e;

@@ -28,14 +28,25 @@ __global__ void __launch_bounds__(128) render_kernel(const __grid_constant__ Sce
     const int x = (tile % tiles_x) * TILE_W + (warp & 1) * 8 + (lane & 7);
     const int y = a.row_first + (tile / tiles_x) * TILE_H + (warp >> 1) * 4 + (lane >> 3);
     if (view >= a.views || x >= a.width || y >= a.row_first + a.rows) return;
-    // camera_from_matrix (src/render_core.h:264-273); tan(fov / 2) and the aspect come from the host.
-    const float *m = a.cameras + 12 * static_cast<size_t>(view);
-    float cm[12];
-    for (int k = 0; k < 12; ++k) cm[k] = __ldg(m + k);
-    const float3 position = mk3(cm[3], cm[7], cm[11]);
-    const float3 right = normalize(mk3(cm[0], cm[4], cm[8]));
-    const float3 up = normalize(mk3(cm[1], cm[5], cm[9]));
-    const float3 forward = normalize(mk3(-cm[2], -cm[6], -cm[10]));
+    // camera_from_matrix (src/render_core.h:264-273); tan(fov / 2) and the aspect come from the host. A
+    // single-view render's camera is used as given.
+    float3 position, right, up, forward;
+    if (a.basis_given) {
+        const float4 b0 = __ldg(a.camera_basis + 3 * view), b1 = __ldg(a.camera_basis + 3 * view + 1);
+        const float4 b2 = __ldg(a.camera_basis + 3 * view + 2);
+        position = mk3(b0.x, b0.y, b0.z);
+        right = mk3(b0.w, b1.x, b1.y);
+        up = mk3(b1.z, b1.w, b2.x);
+        forward = mk3(b2.y, b2.z, b2.w);
+    } else {
+        const float *m = a.cameras + 12 * static_cast<size_t>(view);
+        float cm[12];
+        for (int k = 0; k < 12; ++k) cm[k] = __ldg(m + k);
+        position = mk3(cm[3], cm[7], cm[11]);
+        right = normalize(mk3(cm[0], cm[4], cm[8]));
+        up = normalize(mk3(cm[1], cm[5], cm[9]));
+        forward = normalize(mk3(-cm[2], -cm[6], -cm[10]));
+    }
     const int world = view / a.cameras_per_world;
     const size_t pix = (static_cast<size_t>(view) * a.rows + (y - a.row_first)) * a.width + x;
     const float fw = static_cast<float>(a.width), fh = static_cast<float>(a.height);
@@ -55,10 +66,14 @@ __global__ void __launch_bounds__(128) render_kernel(const __grid_constant__ Sce
                               rng, a.error_flag);
         }
         sum = sum * (1.0f / static_cast<float>(a.spp));
-        uint8_t *o = a.rgb + 3 * pix;
-        o[0] = srgb_byte(s.srgb_table, sum.x);
-        o[1] = srgb_byte(s.srgb_table, sum.y);
-        o[2] = srgb_byte(s.srgb_table, sum.z);
+        if (a.radiance) {
+            a.radiance[pix] = make_float4(sum.x, sum.y, sum.z, 0.0f);
+        } else {
+            uint8_t *o = a.rgb + 3 * pix;
+            o[0] = srgb_byte(s.srgb_table, sum.x);
+            o[1] = srgb_byte(s.srgb_table, sum.y);
+            o[2] = srgb_byte(s.srgb_table, sum.z);
+        }
     }
     if (a.depth || a.normal || a.object_id || a.hit_instance) {  // aov_pixel (src/render_core.h:313-327)
         const float3 dir = camera_ray(static_cast<float>(x) + 0.5f, static_cast<float>(y) + 0.5f);
@@ -117,7 +132,42 @@ __global__ void __launch_bounds__(128) prepare_cameras_kernel(const float *camer
     basis[3 * v + 2] = make_float4(up.z, fwd.x, fwd.y, fwd.z);
 }
 
+// One thread per pixel: the running average and its bytes (render_pixel, src/render_core.h:288-301, and
+// pack_argb8888, src/geom_dev.h:179-184).
+__global__ void __launch_bounds__(256) accumulate_kernel(const float4 *radiance, float4 *accum, int frame,
+    long long pixels, const float *srgb_table, uint32_t *argb, uint8_t *rgb) {
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < pixels;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float4 r = radiance[p];
+        float4 acc = make_float4(r.x, r.y, r.z, 1.0f);
+        if (frame != 0) {
+            const float4 prev = accum[p];
+            acc = make_float4(prev.x + r.x, prev.y + r.y, prev.z + r.z, prev.w + 1.0f);
+        }
+        accum[p] = acc;
+        const float inv = recip(acc.w);
+        const uint32_t red = srgb_byte(srgb_table, acc.x * inv), green = srgb_byte(srgb_table, acc.y * inv);
+        const uint32_t blue = srgb_byte(srgb_table, acc.z * inv);
+        argb[p] = 0xFF000000u | (red << 16) | (green << 8) | blue;
+        if (rgb) {
+            rgb[3 * p] = static_cast<uint8_t>(red);
+            rgb[3 * p + 1] = static_cast<uint8_t>(green);
+            rgb[3 * p + 2] = static_cast<uint8_t>(blue);
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_accumulate(const float4 *radiance, float4 *accum, int frame, long long pixels, const float *srgb_table,
+    uint32_t *argb, uint8_t *rgb, cudaStream_t stream) {
+    if (pixels <= 0) return cudaSuccess;
+    long long blocks = (pixels + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    accumulate_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(radiance, accum, frame, pixels, srgb_table,
+        argb, rgb);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_render(const SceneParams &s, const RenderArgs &a, cudaStream_t stream) {
     const long long tiles = static_cast<long long>((a.width + TILE_W - 1) / TILE_W) * ((a.rows + TILE_H - 1) / TILE_H);

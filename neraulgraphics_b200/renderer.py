@@ -571,3 +571,138 @@ class UnevenBatchRenderer(BatchRenderer):
         width, height = self._sizes[w]
         x = packed[a:b]
         return x.reshape((height, width) + tuple(x.shape[1:]))
+
+
+class _DeviceArray:
+    """A device array the renderer owns, as __cuda_array_interface__ describes it, for a zero-copy torch view."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def _device_view(ptr, shape, dtype, device):
+    torch = _torch()
+    typestr = {torch.uint8: "|u1", torch.float32: "<f4", torch.int32: "<i4"}[dtype]
+    return torch.as_tensor(_DeviceArray(ptr, shape, typestr), device=f"cuda:{device}")
+
+
+def _camera_c(camera) -> _abi.CameraC:
+    """An ngb_camera from a scene.Camera (or anything with its six fields)."""
+    v = lambda t: _abi.Vec3(float(t[0]), float(t[1]), float(t[2]))
+    return _abi.CameraC(v(camera.position), v(camera.right), v(camera.up), v(camera.forward), float(camera.fov_scale),
+                        float(camera.aspect))
+
+
+class Renderer:
+    """The reference's single-view Renderer (include/neraulgraphics/renderer.h:135-277, python/bindings.cpp:801-943):
+    one scene seen by one camera, over a one-world BatchRenderer and the C ABI's view calls.
+
+    render() traces one frame and averages it with the frames before it (frame 0 starts afresh); render_frame()
+    returns the images asked for; cast_rays() answers ray queries; set_instance_transforms() moves the instances.
+    Cameras are scene.Camera objects (make_camera), used as given."""
+
+    def __init__(self, width, height, spheres=(), lights=(), floor=None, meshes=(), instances=(), device="auto"):
+        self._batch = BatchRenderer(width, height, 1, 1, spheres, lights, floor, meshes, instances, device=device)
+        self._lib = self._batch._lib
+        self._h = self._batch._h
+
+    def __repr__(self):
+        return f"Renderer({self.width}x{self.height}, {self.instance_count} instances, {self.device})"
+
+    def set_instance_transforms(self, transforms):
+        """Move the instances: (N, 3, 4) matrices (host arrays, checked; CUDA tensors, used where they are), or a
+        list of Transform objects."""
+        if isinstance(transforms, (list, tuple)) and transforms and hasattr(transforms[0], "matrix"):
+            transforms = np.stack([np.asarray(t.matrix, np.float32) for t in transforms])
+        self._batch.set_instance_transforms(transforms)
+
+    def render(self, camera, frame=0, samples_per_frame=1):
+        """One frame, averaged with the frames before it: a (height, width, 3) uint8 RGB array (the 0xAARRGGBB
+        pixels of Renderer::render, unpacked)."""
+        argb = self.render_argb(camera, frame, samples_per_frame)
+        out = np.empty(argb.shape + (3,), np.uint8)
+        out[..., 0] = (argb >> 16) & 0xFF
+        out[..., 1] = (argb >> 8) & 0xFF
+        out[..., 2] = argb & 0xFF
+        return out
+
+    def render_argb(self, camera, frame=0, samples_per_frame=1):
+        """The same picture as (height, width) uint32 0xAARRGGBB pixels, as Renderer::render returns them."""
+        h, w = self._batch.rows[1], self.width
+        argb = np.empty((h, w), np.uint32)
+        cam = _camera_c(camera)
+        self._batch._stream()
+        check(self._lib.ngb_render_view(self._h, C.byref(cam), int(frame), int(samples_per_frame),
+                                        argb.ctypes.data_as(C.c_void_p)), self._h)
+        return argb
+
+    def render_frame(self, camera, frame=0, samples_per_frame=1, *, rgb=True, depth=False, normals=False,
+                     object_ids=False, zero_copy=False):
+        """The images asked for: 'rgb' (H, W, 3) uint8 (the running average's bytes; it advances the average as
+        render() does), 'depth' (H, W) float32, 'normals' (H, W, 3) float32, 'object_ids' (H, W) int32. Copies by
+        default; with zero_copy=True, CUDA tensors aliasing the renderer's own buffers, queued on PyTorch's current
+        stream and overwritten by the next render."""
+        torch = _torch()
+        outputs = ((_abi.OUTPUT_RGB if rgb else 0) | (_abi.OUTPUT_DEPTH if depth else 0) |
+                   (_abi.OUTPUT_NORMAL if normals else 0) | (_abi.OUTPUT_OBJECT_ID if object_ids else 0))
+        cam = _camera_c(camera)
+        f = _abi.BatchFrameC()
+        self._batch._stream()
+        check(self._lib.ngb_render_view_frame(self._h, C.byref(cam), int(frame), int(samples_per_frame), outputs,
+                                              C.byref(f)), self._h)
+        h, w = f.height, f.width
+        images = {"rgb": (f.rgb, (h, w, 3), torch.uint8), "depth": (f.depth, (h, w), torch.float32),
+                  "normals": (f.normal, (h, w, 3), torch.float32), "object_ids": (f.object_id, (h, w), torch.int32)}
+        views = {k: _device_view(ptr, shape, dtype, self._batch._device) for k, (ptr, shape, dtype) in images.items()
+                 if ptr}
+        if zero_copy:
+            return views
+        host = {k: v.cpu().numpy() for k, v in views.items()}
+        self._batch.synchronize()
+        return host
+
+    def cast_rays(self, origins, directions, max_distance=math.inf):
+        """Rays into the scene: (N, 3) origins and directions (directions need not be unit length). Returns
+        'distance' (N,), 'normal' (N, 3) and 'object_id' (N,); CUDA tensors in give CUDA tensors out."""
+        if _count(origins) != _count(directions):
+            raise ValueError("origins and directions must have the same number of rays")
+        hits = self._batch.cast_rays(origins, directions, max_distance)
+        return {k: v[0] for k, v in hits.items()}
+
+    def set_environment(self, environment: Environment):
+        self._batch.set_environment(environment)
+
+    @property
+    def ambient(self) -> float:
+        return self._batch.ambient
+
+    @ambient.setter
+    def ambient(self, value):
+        self._batch.ambient = value
+
+    @property
+    def instance_count(self) -> int:
+        return self._batch.instances_per_world
+
+    @property
+    def width(self) -> int:
+        return self._batch.width
+
+    @property
+    def height(self) -> int:
+        return self._batch.height
+
+    @property
+    def device(self) -> str:
+        return self._batch.device
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return self._batch.last_kernel_ms
+
+    def set_tuning(self, *args, **kwargs):
+        self._batch.set_tuning(*args, **kwargs)
+
+    def synchronize(self, timeout=_TIMEOUT_S):
+        self._batch.synchronize(timeout)

@@ -229,6 +229,21 @@ class Camera:
                         np.float32)
 
 
+_libm = None
+
+
+def _tanf(x: float) -> float:
+    """The C library's single-precision tangent, which std::tan(float) calls (numpy's float32 tan is its own)."""
+    global _libm
+    if _libm is None:
+        import ctypes
+        import ctypes.util
+        _libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+        _libm.tanf.restype = ctypes.c_float
+        _libm.tanf.argtypes = [ctypes.c_float]
+    return float(_libm.tanf(x))
+
+
 def make_camera(position, target, *, width: int, height: int, world_up=(0.0, 1.0, 0.0), fov=1.5707964) -> Camera:
     """A camera at position looking at target: the basis in double, then rounded (src/renderer.cpp:39-59)."""
     pos = [float(np.float32(v)) for v in position]
@@ -246,7 +261,7 @@ def make_camera(position, target, *, width: int, height: int, world_up=(0.0, 1.0
     right = norm(cross(fwd, wup))
     up = cross(right, fwd)
     f32 = lambda a: tuple(float(np.float32(x)) for x in a)
-    fov_scale = float(np.float32(math.tan(float(np.float32(np.float32(fov) * np.float32(0.5))))))
+    fov_scale = _tanf(float(np.float32(np.float32(fov) * np.float32(0.5))))
     return Camera(f32(pos), f32(right), f32(up), f32(fwd), fov_scale, float(np.float32(width) / np.float32(height)))
 
 

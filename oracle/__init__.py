@@ -63,6 +63,9 @@ def oracle_lib():
                                  C.POINTER(C.c_int32), _f32p, C.POINTER(C.c_int32)]
         lib.orc_traversal_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.orc_compose.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int32), _f32p, _f32p, _f32p, _f32p]
+        lib.orc_render_view.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_uint, C.c_int, _f32p, C.POINTER(C.c_uint32),
+                                        C.POINTER(C.c_uint8), _f32p, _f32p, C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_uint8), C.c_int]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -142,6 +145,30 @@ class Oracle:
                             _p(hv), _p(tf, C.c_uint8), int(threads))
         if hits:
             out.update(hit_instance=hi, hit_triangle=ht, hit_u=hu, hit_v=hv)
+        if ties:
+            out["ties"] = tf
+        return out
+
+    def render_view(self, camera, frame=0, samples_per_frame=1, *, rgb=True, depth=False, normals=False,
+                    object_ids=False, ties=False, threads=0):
+        """The single-view Renderer's render / render_frame on a scene of one world and one camera (a
+        scene.Camera, used as given): the running average's 'argb' (H, W) uint32 and 'rgb' bytes, and the other
+        images asked for. The average carries over between calls on this oracle; frame 0 starts it."""
+        d = self.desc
+        cam = np.float32(list(camera.position) + list(camera.right) + list(camera.up) + list(camera.forward) +
+                         [camera.fov_scale, camera.aspect])
+        if getattr(self, "_accum", None) is None:
+            self._accum = np.zeros((d.height, d.width, 4), np.float32)
+        outputs = outputs_mask(rgb, depth, normals, object_ids)
+        out = {k: v[0] for k, v in _images(1, d.height, d.width, outputs).items()}
+        argb = np.zeros((d.height, d.width), np.uint32) if rgb else None
+        tf = np.zeros((d.height, d.width), np.uint8) if ties else None
+        self.lib.orc_render_view(self.h, _p(cam), int(samples_per_frame), outputs, int(frame),
+                                 _p(self._accum) if rgb else None, _p(argb, C.c_uint32), _p(out.get("rgb"), C.c_uint8),
+                                 _p(out.get("depth")), _p(out.get("normals")), _p(out.get("object_ids"), C.c_int32),
+                                 _p(tf, C.c_uint8), int(threads))
+        if rgb:
+            out["argb"] = argb
         if ties:
             out["ties"] = tf
         return out
@@ -355,6 +382,66 @@ class Reference:
         return float(self.lib.ngref_last_kernel_ms(self.h))
 
 
+class ReferenceView:
+    """neraulgraphics 0.5.0's own single-view Renderer (Device::Cpu, or Device::Cuda with cuda=True) on a scene
+    of one world (desc.width x desc.height)."""
+
+    def __init__(self, desc: SceneDesc, cuda=False, threads=None):
+        self.lib = ref_lib(cuda)
+        for name, args in (("ngref_view_create", [C.POINTER(_abi.SceneC), C.c_int, C.POINTER(C.c_void_p)]),
+                           ("ngref_view_destroy", [C.c_void_p]), ("ngref_view_set_matrices", [C.c_void_p, _f32p]),
+                           ("ngref_view_set_ambient", [C.c_void_p, C.c_float]),
+                           ("ngref_view_render", [C.c_void_p, C.POINTER(_abi.CameraC), C.c_int, C.c_int,
+                                                  C.POINTER(C.c_uint32)]),
+                           ("ngref_view_render_frame", [C.c_void_p, C.POINTER(_abi.CameraC), C.c_int, C.c_int, C.c_uint,
+                                                        C.POINTER(C.c_uint8), _f32p, _f32p, C.POINTER(C.c_int32)])):
+            getattr(self.lib, name).argtypes = args
+        self.desc = desc
+        if threads is not None:
+            self.lib.ngref_set_threads(int(threads))
+        h = C.c_void_p()
+        _ref_check(self.lib, self.lib.ngref_view_create(C.byref(desc.c), 1 if cuda else 0, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ngref_view_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def _camera(camera):
+        v = lambda t: _abi.Vec3(float(t[0]), float(t[1]), float(t[2]))
+        return _abi.CameraC(v(camera.position), v(camera.right), v(camera.up), v(camera.forward),
+                            float(camera.fov_scale), float(camera.aspect))
+
+    def set_instance_transforms(self, matrices):
+        m = np.ascontiguousarray(matrices, np.float32)
+        _ref_check(self.lib, self.lib.ngref_view_set_matrices(self.h, _p(m)))
+
+    def set_ambient(self, a):
+        _ref_check(self.lib, self.lib.ngref_view_set_ambient(self.h, float(a)))
+
+    def render(self, camera, frame=0, samples_per_frame=1):
+        """Renderer::render: (H, W) uint32 0xAARRGGBB."""
+        out = np.zeros((self.desc.height, self.desc.width), np.uint32)
+        cam = self._camera(camera)
+        _ref_check(self.lib, self.lib.ngref_view_render(self.h, C.byref(cam), int(frame), int(samples_per_frame),
+                                                        _p(out, C.c_uint32)))
+        return out
+
+    def render_frame(self, camera, frame=0, samples_per_frame=1, *, rgb=True, depth=False, normals=False,
+                     object_ids=False):
+        d = self.desc
+        outputs = outputs_mask(rgb, depth, normals, object_ids)
+        out = {k: v[0] for k, v in _images(1, d.height, d.width, outputs).items()}
+        cam = self._camera(camera)
+        _ref_check(self.lib, self.lib.ngref_view_render_frame(self.h, C.byref(cam), int(frame), int(samples_per_frame),
+                                                              outputs, _p(out.get("rgb"), C.c_uint8),
+                                                              _p(out.get("depth")), _p(out.get("normals")),
+                                                              _p(out.get("object_ids"), C.c_int32)))
+        return out
+
+
 def ref_tlas_available() -> bool:
     return os.path.exists(REF_TLAS_SO)
 
@@ -446,6 +533,16 @@ def ref_camera_matrix(position, target, world_up=(0, 1, 0), fov=1.0, width=64, h
     lib.ngref_camera_matrix(_p(np.asarray(position, np.float32)), _p(np.asarray(target, np.float32)),
                             _p(np.asarray(world_up, np.float32)), float(fov), int(width), int(height), _p(out))
     return out.reshape(3, 4)
+
+
+def ref_make_camera(position, target, world_up=(0, 1, 0), fov=1.0, width=64, height=64):
+    """The reference's make_camera: 14 floats (position, right, up, forward, fov_scale, aspect)."""
+    lib = ref_lib()
+    lib.ngref_make_camera.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int, C.c_int, _f32p]
+    out = np.zeros(14, np.float32)
+    lib.ngref_make_camera(_p(np.asarray(position, np.float32)), _p(np.asarray(target, np.float32)),
+                          _p(np.asarray(world_up, np.float32)), float(fov), int(width), int(height), _p(out))
+    return out
 
 
 def ref_invert_affine(m):

@@ -1261,6 +1261,9 @@ typedef struct {
     int32_t *ids, *hit_instance, *hit_triangle;
     float *hit_u, *hit_v;
     uint8_t *ties;
+    const float *view;   /* a single-view render's camera as given (14 floats), or NULL: the matrices */
+    float *accum;        /* the single-view running sums (4 floats per pixel), or NULL */
+    uint32_t *argb;      /* the single-view average's 0xAARRGGBB pixels */
     long total;
     atomic_long next;
     double bytes, rays;
@@ -1273,7 +1276,18 @@ static void render_pixel(render_job_t *j, long pix, double *bytes, double *rays)
     const int view = (int)(pix / ((long)W * H));
     const int idx = (int)(pix % ((long)W * H));
     const int y = idx / W, x = idx % W, world = view / s->cpw;
-    const camera_t cam = camera_from_matrix(j->cameras + 12 * (size_t)view, j->fov, W, H);
+    camera_t cam;
+    if (j->view) { /* the Camera as given (cuda_backend.cu:651-652 passes it unchanged) */
+        const float *c = j->view;
+        cam.position = mk(c[0], c[1], c[2]);
+        cam.right = mk(c[3], c[4], c[5]);
+        cam.up = mk(c[6], c[7], c[8]);
+        cam.forward = mk(c[9], c[10], c[11]);
+        cam.fov_scale = c[12];
+        cam.aspect = c[13];
+    } else {
+        cam = camera_from_matrix(j->cameras + 12 * (size_t)view, j->fov, W, H);
+    }
     uint8_t tie = 0;
     if (j->outputs & NGB_OUTPUT_RGB) { /* render_pixel_rgb8 (:276-283) via sample_pixel (:248-259) */
         uint32_t r = make_rng((uint32_t)(y * W + x), (uint32_t)j->frame);
@@ -1286,7 +1300,21 @@ static void render_pixel(render_job_t *j, long pix, double *bytes, double *rays)
                                  j->ties ? &t : NULL, bytes, rays));
         }
         sum = muls(sum, 1.0f / (float)j->spp);
+        if (j->accum) { /* render_pixel's running average (render_core.h:288-301) */
+            float *a = j->accum + 4 * (size_t)pix;
+            if (j->frame == 0) {
+                a[0] = sum.x, a[1] = sum.y, a[2] = sum.z, a[3] = 1.0f;
+            } else {
+                a[0] = a[0] + sum.x, a[1] = a[1] + sum.y, a[2] = a[2] + sum.z, a[3] = a[3] + 1.0f;
+            }
+            sum = muls(mk(a[0], a[1], a[2]), 1.0f / a[3]);
+        }
         const f3 c = mk(srgb_channel(sum.x), srgb_channel(sum.y), srgb_channel(sum.z));
+        if (j->argb) { /* pack_argb8888 (geom_dev.h:179-184) */
+            const uint32_t r8 = (uint32_t)(saturate(c.x) * 255.0f + 0.5f), g8 = (uint32_t)(saturate(c.y) * 255.0f + 0.5f);
+            const uint32_t b8 = (uint32_t)(saturate(c.z) * 255.0f + 0.5f);
+            j->argb[pix] = 0xFF000000u | (r8 << 16) | (g8 << 8) | b8;
+        }
         if (j->rgb) {
             uint8_t *o = j->rgb + 3 * (size_t)pix;
             o[0] = (uint8_t)(saturate(c.x) * 255.0f + 0.5f);
@@ -1337,6 +1365,8 @@ static void *render_worker(void *arg) {
     return NULL;
 }
 
+static int run_render(render_job_t *jp, int threads);
+
 int orc_render(orc_scene *s, const float *cameras, float fov, int spp, unsigned outputs, int frame, uint8_t *rgb,
     float *depth, float *normal, int32_t *ids, int32_t *hit_instance, int32_t *hit_triangle, float *hit_u,
     float *hit_v, uint8_t *ties, int threads) {
@@ -1357,6 +1387,34 @@ int orc_render(orc_scene *s, const float *cameras, float fov, int spp, unsigned 
     j.hit_u = hit_u;
     j.hit_v = hit_v;
     j.ties = ties;
+    return run_render(&j, threads);
+}
+
+/* The single-view Renderer's render / render_frame (renderer.cpp:104-108, 174-182) for a scene of one world
+ * and one camera: camera = position, right, up, forward (3 floats each), fov_scale, aspect, used as given;
+ * accum (4 floats per pixel) carries the running average between calls, argb receives its pixels. */
+int orc_render_view(orc_scene *s, const float *camera, int spp, unsigned outputs, int frame, float *accum,
+    uint32_t *argb, uint8_t *rgb, float *depth, float *normal, int32_t *ids, uint8_t *ties, int threads) {
+    render_job_t j;
+    memset(&j, 0, sizeof(j));
+    j.s = s;
+    j.view = camera;
+    j.spp = spp;
+    j.frame = frame;
+    j.outputs = outputs;
+    j.rgb = rgb;
+    j.depth = depth;
+    j.normal = normal;
+    j.ids = ids;
+    j.ties = ties;
+    j.accum = accum;
+    j.argb = argb;
+    return run_render(&j, threads);
+}
+
+static int run_render(render_job_t *jp, int threads) {
+    render_job_t j = *jp;
+    orc_scene *s = j.s;
     j.total = (long)s->worlds * s->cpw * s->H * s->W;
     atomic_init(&j.next, 0);
     pthread_mutex_init(&j.lock, NULL);

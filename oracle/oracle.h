@@ -57,6 +57,13 @@ int orc_cast_rays(orc_scene *s, const float *origins, const float *directions, i
 
 /* The last LBVH build: keys in instance order, sorted ids, nodes (8 words each), roots, matrices. */
 int orc_tlas(const orc_scene *s, uint64_t *keys, int32_t *sorted_ids, int32_t *nodes, int32_t *roots, float *matrices);
+/* The single-view Renderer's render / render_frame for a scene of one world and one camera: camera = position,
+ * right, up, forward (3 floats each), fov_scale, aspect, used as given; accum (4 floats per pixel) carries the
+ * running average between calls (frame 0 starts it); argb receives the average's 0xAARRGGBB pixels and rgb its
+ * bytes; depth, normals, IDs and near-tie flags as orc_render. */
+int orc_render_view(orc_scene *s, const float *camera, int spp, unsigned outputs, int frame, float *accum,
+    uint32_t *argb, uint8_t *rgb, float *depth, float *normal, int32_t *ids, uint8_t *ties, int threads);
+
 /* The meshes' built trees: counts, then nodes (8 words each), packed triangles (12 floats), per-mesh roots and
  * bounds (6 floats), and each packed triangle's index in its own mesh. */
 void orc_blas(const orc_scene *s, int *node_count, int *triangle_count, int32_t *nodes, float *triangles,

@@ -5,6 +5,7 @@
 // It exposes:
 //   - BatchRenderer on Device::Cpu (or Device::Cuda when the library was built with the reference's CUDA
 //     backend) with the scene passed as the same plain structs the product's ABI takes (include/ngb.h);
+//   - its single-view Renderer (render's running average, render_frame) on the same structs;
 //   - the reference's host helpers the product restates, for bit-exact pinning: detail::build_meshes
 //     (src/mesh_build.cpp:91-157), detail::body_poses_to_matrices (src/instances.cpp:137-164),
 //     make_icosphere / make_box / make_transform (src/mesh.cpp), make_camera (src/renderer.cpp:39-59),
@@ -101,6 +102,14 @@ Scene convert(const ngb_scene &s) {
 struct Handle {
     std::unique_ptr<BatchRenderer> batch;
 };
+
+struct ViewHandle {
+    std::unique_ptr<Renderer> view;
+};
+
+Camera camera_of(const ngb_camera &c) {
+    return Camera{v3(c.position), v3(c.right), v3(c.up), v3(c.forward), c.fov_scale, c.aspect};
+}
 
 }  // namespace
 
@@ -346,6 +355,80 @@ void ngref_transform_aabb(const float *m, const float *box, float *out) {
     const bvh::Aabb r = detail::transform_aabb(t, b);
     std::memcpy(out, r.lo, 3 * sizeof(float));
     std::memcpy(out + 3, r.hi, 3 * sizeof(float));
+}
+
+// The reference's single-view Renderer (include/neraulgraphics/renderer.h:135-277) over the same plain scene
+// structs: scene->width and height are its frame; world_count and cameras_per_world are not read.
+int ngref_view_create(const ngb_scene *scene, int device, void **out) {
+    *out = nullptr;
+    try {
+        const Scene s = convert(*scene);
+        auto h = std::make_unique<ViewHandle>();
+        h->view = std::make_unique<Renderer>(scene->width, scene->height, s.spheres, s.lights, s.floor, s.meshes,
+            s.instances, std::vector<Texture>{}, device == 1 ? Device::Cuda : Device::Cpu);
+        *out = h.release();
+        g_error.clear();
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+void ngref_view_destroy(void *h) { delete static_cast<ViewHandle *>(h); }
+
+int ngref_view_set_matrices(void *h, const float *matrices) {
+    try {
+        static_cast<ViewHandle *>(h)->view->set_instance_matrices(matrices, Memory::Host);
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+int ngref_view_set_ambient(void *h, float ambient) {
+    try {
+        static_cast<ViewHandle *>(h)->view->set_ambient(ambient);
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Renderer::render: width x height 0xAARRGGBB pixels into argb.
+int ngref_view_render(void *h, const ngb_camera *camera, int frame, int spp, uint32_t *argb) {
+    try {
+        Renderer &r = *static_cast<ViewHandle *>(h)->view;
+        const uint32_t *p = r.render(camera_of(*camera), frame, spp);
+        std::memcpy(argb, p, static_cast<size_t>(r.width()) * r.height() * sizeof(uint32_t));
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// Renderer::render_frame_host into the caller's buffers (any may be NULL).
+int ngref_view_render_frame(void *h, const ngb_camera *camera, int frame, int spp, unsigned outputs, uint8_t *rgb,
+    float *depth, float *normal, int32_t *ids) {
+    try {
+        const HostFrame f = static_cast<ViewHandle *>(h)->view->render_frame_host(camera_of(*camera), frame, spp, outputs);
+        if (rgb && !f.rgb.empty()) std::memcpy(rgb, f.rgb.data(), f.rgb.size());
+        if (depth && !f.depth.empty()) std::memcpy(depth, f.depth.data(), f.depth.size() * sizeof(float));
+        if (normal && !f.normal.empty()) std::memcpy(normal, f.normal.data(), f.normal.size() * sizeof(float));
+        if (ids && !f.object_id.empty()) std::memcpy(ids, f.object_id.data(), f.object_id.size() * sizeof(int32_t));
+        return NGB_OK;
+    } catch (const std::exception &e) {
+        return fail(e);
+    }
+}
+
+// make_camera (src/renderer.cpp:39-59), the whole Camera: position, right, up, forward, fov_scale, aspect.
+void ngref_make_camera(const float *position, const float *target, const float *world_up, float fov, int width,
+    int height, float *out) {
+    const Camera c = make_camera(Vec3{position[0], position[1], position[2]}, Vec3{target[0], target[1], target[2]},
+        Vec3{world_up[0], world_up[1], world_up[2]}, fov, width, height);
+    const float v[14] = {c.position.x, c.position.y, c.position.z, c.right.x, c.right.y, c.right.z, c.up.x, c.up.y,
+        c.up.z, c.forward.x, c.forward.y, c.forward.z, c.fov_scale, c.aspect};
+    std::memcpy(out, v, sizeof(v));
 }
 
 }  // extern "C"

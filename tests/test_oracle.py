@@ -195,6 +195,65 @@ def test_oracle_matches_reference_on_scattered_worlds_except_near_ties():
     assert (np.abs(a["rgb"].astype(int) - b["rgb"].astype(int)).max(-1)[~rgb_tie] == 0).all()
 
 
+def view_scenes():
+    """Single-view scenes: the template (mirror sphere, two hard-shadow lights, checker floor, smooth normals) and
+    eight icospheres under one soft-shadow light, each with its camera (make_camera)."""
+    t = scenes.template(worlds=1)
+    wl = workloads.icosphere_worlds(worlds=1, width=80, height=60, seed=5)
+    return [(t, scenes.template_matrices(1), S.make_camera((0.3, 0.6, 0.2), (0, 0, -8), width=t.width,
+                                                            height=t.height, fov=scenes.FOV)),
+            (wl.desc, wl.matrices, S.make_camera((0.1, 1.1, 0.1), (0, 0, -6), width=80, height=60, fov=1.0))]
+
+
+@needs_ref
+def test_oracle_view_renders_are_the_references_renderer():
+    """The oracle's single-view render (the running average over frames, and render_frame's images) against the
+    reference's own Renderer on its CPU backend, frame after frame: ARGB, RGB, depth, normals and IDs bit for bit
+    but on near ties (the reference's CPU backend builds its instance tree by SAH, the oracle by LBVH)."""
+    for desc, mats, cam in view_scenes():
+        o, r = O.Oracle(desc), O.ReferenceView(desc)
+        o.set_instance_transforms(mats)
+        r.set_instance_transforms(mats)
+        tie = np.zeros((desc.height, desc.width), bool)
+        for frame, spp in ((0, 1), (1, 2), (2, 1), (0, 2), (1, 1)):
+            got = o.render_view(cam, frame, spp, rgb=True, depth=True, normals=True, object_ids=True, ties=True)
+            want_argb = r.render(cam, frame, spp)
+            tie = (tie | (got["ties"] != 0)) if frame else (got["ties"] != 0)
+            assert np.array_equal(got["argb"][~tie], want_argb[~tie]), (frame, spp)
+            assert (got["argb"] >> 24 == 0xFF).all()
+            rgb = np.stack([(got["argb"] >> 16) & 0xFF, (got["argb"] >> 8) & 0xFF, got["argb"] & 0xFF], -1)
+            assert np.array_equal(rgb.astype(np.uint8), got["rgb"])
+            want = r.render_frame(cam, frame + 1, spp, rgb=False, depth=True, normals=True, object_ids=True)
+            ok = ~tie
+            assert np.array_equal(got["object_ids"][ok], want["object_ids"][ok])
+            assert np.array_equal(bits(got["depth"][ok]), bits(want["depth"][ok]))
+            assert np.array_equal(bits(got["normals"][ok]), bits(want["normals"][ok]))
+
+
+@needs_ref
+def test_make_camera_is_the_references():
+    """ngb_make_camera (the C ABI) and the Python make_camera against the reference's make_camera, every field."""
+    import ctypes as C
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import _abi
+    from neraulgraphics_b200._lib import lib
+    L = lib()
+    rng = np.random.default_rng(4)
+    for _ in range(300):
+        p, t = rng.uniform(-5, 5, 3).astype(np.float32), rng.uniform(-5, 5, 3).astype(np.float32)
+        fov, w, h = float(np.float32(rng.uniform(0.3, 2.0))), int(rng.integers(8, 300)), int(rng.integers(8, 300))
+        want = O.ref_make_camera(p, t, (0, 1, 0), fov, w, h)
+        c = _abi.CameraC()
+        v = lambda a: _abi.Vec3(*[float(x) for x in a])
+        assert L.ngb_make_camera(v(p), v(t), v((0, 1, 0)), fov, w, h, C.byref(c)) == 0
+        got = np.float32([c.position.x, c.position.y, c.position.z, c.right.x, c.right.y, c.right.z, c.up.x, c.up.y,
+                          c.up.z, c.forward.x, c.forward.y, c.forward.z, c.fov_scale, c.aspect])
+        py = ng.make_camera(p, t, width=w, height=h, fov=fov)
+        mine = np.float32(list(py.position) + list(py.right) + list(py.up) + list(py.forward) + [py.fov_scale,
+                                                                                                py.aspect])
+        assert np.array_equal(bits(got), bits(want)) and np.array_equal(bits(mine), bits(want))
+
+
 # ----------------------------------------------------------------------------------------- the ABI --
 
 def test_library_exports_every_declared_entry_point():
