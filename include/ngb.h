@@ -300,6 +300,9 @@ int ngb_copy_to_host(ngb_renderer *r, const void *src, void *dst, size_t bytes);
 int ngb_set_ambient(ngb_renderer *r, float ambient);      /* src/batch.cpp:230-233 */
 float ngb_ambient(const ngb_renderer *r);
 int ngb_set_environment(ngb_renderer *r, const ngb_environment *environment); /* src/batch.cpp:224-227 */
+/* Replaces the lights, at most NGB_MAX_LIGHTS, checked as ngb_create checks them; takes effect on the next render
+ * (Renderer::set_lights, src/renderer.cpp:139-143). */
+int ngb_set_lights(ngb_renderer *r, const ngb_light *lights, int32_t count);
 
 /* The stream every later call queues its work on: a cudaStream_t, or NULL for the renderer's own stream
  * (created non-blocking at ngb_create). CUDA's legacy default stream is named by its handle,

@@ -83,6 +83,7 @@ def lib():
     L.ngb_render_view_frame.argtypes = [_vp, C.POINTER(_abi.CameraC), C.c_int32, C.c_int32, C.c_uint32,
                                         C.POINTER(_abi.BatchFrameC)]
     L.ngb_view_pixels.argtypes = [_vp, C.POINTER(C.c_void_p)]
+    L.ngb_set_lights.argtypes = [_vp, C.POINTER(_abi.LightC), C.c_int32]
     L.ngb_set_rows.argtypes = [_vp, C.c_int32, C.c_int32]
     L.ngb_device_bytes.argtypes = []
     L.ngb_device_bytes.restype = C.c_int64

@@ -47,7 +47,7 @@ void check_frame_size(int width, int height) {
         "frame of " + std::to_string(width) + "x" + std::to_string(height) + " pixels is too large");
 }
 
-static void check_lights(const ngb_light *lights, int count) {
+void check_lights(const ngb_light *lights, int count) {
     require(count <= NGB_MAX_LIGHTS, "scene has " + std::to_string(count) + " lights, at most " +
         std::to_string(NGB_MAX_LIGHTS) + " fit");
     for (int i = 0; i < count; ++i) {

@@ -33,6 +33,7 @@ std::string fstr(float v);  // std::to_string(float): "%f"
 
 void check_frame_size(int width, int height);                          // src/validate.cpp:34-40
 void check_scene(const ngb_scene &s);                                   // src/validate.cpp:61-78, 42-59
+void check_lights(const ngb_light *lights, int count);                  // src/validate.cpp:41-59
 void check_meshes(const ngb_scene &s);                                  // src/mesh_build.cpp:31-89
 void check_material(const ngb_material &m, const std::string &name);   // src/validate.cpp:22-31
 bool invert_affine(const float *m, float *out);                         // src/mesh_build.cpp:159-183

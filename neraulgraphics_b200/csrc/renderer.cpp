@@ -257,6 +257,7 @@ struct Renderer {
     void render(const float *cams, float fov, int spp, unsigned outputs, int frame, int memory, uint8_t *rgb,
         float *depth, float *normal, int32_t *ids, const ngb_camera *view = nullptr);
     void check_view(const ngb_camera *camera, int frame, int spp);
+    void put_lights(const ngb_light *lights, int count);
     void cast_rays(const float *o, const float *d, int rays_per_world, float max_distance, int memory, ngb_ray_hits *out,
         float *distance, float *normal, int32_t *ids);
     int rows() const { return band_rows > 0 ? band_rows : height; }
@@ -355,26 +356,8 @@ void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
         const ngb_sphere &sp = s.spheres[i];
         params.spheres[i] = DevSphere{make_float3(sp.center.x, sp.center.y, sp.center.z), sp.radius, dev_material(sp.material)};
     }
-    for (int i = 0; i < s.light_count; ++i) {
-        const ngb_light &l = s.lights[i];
-        float dx = l.direction.x, dy = l.direction.y, dz = l.direction.z;
-        const float nn = std::sqrt(dx * dx + dy * dy + dz * dz);
-        if (nn > 0.0f) {
-            dx = dx / nn;
-            dy = dy / nn;
-            dz = dz / nn;
-        } else {
-            dx = 0.0f;
-            dy = 0.0f;
-            dz = -1.0f;
-        }
-        const bool spot = l.spot_angle > 0.0f;
-        params.lights[i] = DevLight{make_float3(l.position.x, l.position.y, l.position.z), l.intensity, l.radius, l.falloff,
-            make_float3(dx, dy, dz), spot ? std::cos(l.spot_angle) : -2.0f,
-            spot ? std::cos(l.spot_angle * (1.0f - l.spot_softness)) : -2.0f, make_float3(l.color.x, l.color.y, l.color.z)};
-    }
+    put_lights(s.lights, s.light_count);
     params.sphere_count = s.sphere_count;
-    params.light_count = s.light_count;
     // A path bounces when throughput * reflectivity >= 1e-3 (src/render_core.h:238-239); with throughput 1
     // at the first hit, that is any material hit with reflectivity >= 1e-3.
     for (int i = 0; i < s.sphere_count; ++i) reflective = reflective || s.spheres[i].material.reflectivity >= 1e-3f;
@@ -906,6 +889,29 @@ void Renderer::check_render(const float *cams, float fov, int spp, unsigned outp
         require(all_finite(cams, 12 * static_cast<size_t>(worlds) * cpw), "a camera has a NaN or infinite value");
 }
 
+// The lights as the kernels read them (the reference's to_device: src/device_scene.h:265-272).
+void Renderer::put_lights(const ngb_light *lights, int count) {
+    for (int i = 0; i < count; ++i) {
+        const ngb_light &l = lights[i];
+        float dx = l.direction.x, dy = l.direction.y, dz = l.direction.z;
+        const float nn = std::sqrt(dx * dx + dy * dy + dz * dz);
+        if (nn > 0.0f) {
+            dx = dx / nn;
+            dy = dy / nn;
+            dz = dz / nn;
+        } else {
+            dx = 0.0f;
+            dy = 0.0f;
+            dz = -1.0f;
+        }
+        const bool spot = l.spot_angle > 0.0f;
+        params.lights[i] = DevLight{make_float3(l.position.x, l.position.y, l.position.z), l.intensity, l.radius, l.falloff,
+            make_float3(dx, dy, dz), spot ? std::cos(l.spot_angle) : -2.0f,
+            spot ? std::cos(l.spot_angle * (1.0f - l.spot_softness)) : -2.0f, make_float3(l.color.x, l.color.y, l.color.z)};
+    }
+    params.light_count = count;
+}
+
 // src/renderer.cpp:104-108, 174-182 and src/validate.cpp:82-89: a single-view render's checks.
 void Renderer::check_view(const ngb_camera *c, int frame, int spp) {
     require(worlds == 1 && cpw == 1 && !uneven,
@@ -1387,6 +1393,15 @@ int ngb_set_ambient(ngb_renderer *h, float ambient) {
 }
 
 float ngb_ambient(const ngb_renderer *h) { return h ? h->r.params.ambient : 0.0f; }
+
+int ngb_set_lights(ngb_renderer *h, const ngb_light *lights, int32_t count) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(count >= 0, "counts must not be negative");
+        ngb::require(count == 0 || lights != nullptr, "lights must not be null");
+        ngb::check_lights(lights, count);
+        r.put_lights(lights, count);
+    });
+}
 
 int ngb_set_environment(ngb_renderer *h, const ngb_environment *e) {
     return guarded(h, [&](ngb::Renderer &r) {

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _abi
 from ._lib import CudaError, check, lib
-from .scene import Environment, Plane, SceneDesc
+from .scene import Environment, Plane, SceneDesc, lights_abi
 
 _TIMEOUT_S = 120.0
 
@@ -337,6 +337,11 @@ class BatchRenderer:
     def set_environment(self, environment: Environment):
         e = environment.to_abi()
         check(self._lib.ngb_set_environment(self._h, C.byref(e)), self._h)
+
+    def set_lights(self, lights):
+        """Replaces the lights (at most MAX_LIGHTS), checked as the constructor checks them."""
+        lig = lights_abi(list(lights))
+        check(self._lib.ngb_set_lights(self._h, lig, len(lights)), self._h)
 
     @property
     def ambient(self) -> float:
@@ -672,6 +677,10 @@ class Renderer:
 
     def set_environment(self, environment: Environment):
         self._batch.set_environment(environment)
+
+    def set_lights(self, lights):
+        """Replaces the lights: a flashlight that follows a camera, a lamp that flickers."""
+        self._batch.set_lights(lights)
 
     @property
     def ambient(self) -> float:

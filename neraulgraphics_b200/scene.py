@@ -229,6 +229,15 @@ class Camera:
                         np.float32)
 
 
+def lights_abi(lights):
+    """The lights as an ngb_light array (at least one entry long)."""
+    lig = (_abi.LightC * max(1, len(lights)))()
+    for i, l in enumerate(lights):
+        lig[i] = _abi.LightC(_abi.Vec3(*_v3(l.position)), l.intensity, l.radius, l.falloff,
+                             _abi.Vec3(*_v3(l.direction)), l.spot_angle, l.spot_softness, _abi.Vec3(*_v3(l.color)))
+    return lig
+
+
 _libm = None
 
 
@@ -332,10 +341,7 @@ class SceneDesc:
         sph = (_abi.SphereC * max(1, len(spheres)))()
         for i, s in enumerate(spheres):
             sph[i] = _abi.SphereC(_abi.Vec3(*_v3(s.center)), s.radius, s.material.to_abi())
-        lig = (_abi.LightC * max(1, len(lights)))()
-        for i, l in enumerate(lights):
-            lig[i] = _abi.LightC(_abi.Vec3(*_v3(l.position)), l.intensity, l.radius, l.falloff,
-                                 _abi.Vec3(*_v3(l.direction)), l.spot_angle, l.spot_softness, _abi.Vec3(*_v3(l.color)))
+        lig = lights_abi(lights)
         msh = (_abi.MeshC * max(1, len(self.meshes)))()
         for i, m in enumerate(self.meshes):
             v = np.ascontiguousarray(m.vertices, np.float32)

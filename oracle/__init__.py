@@ -24,6 +24,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libngref.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libngref_cuda.so")
 REF_TLAS_SO = os.path.join(HERE, "_ref", "libngref_tlas.so")
+REF_NGB_SO = os.path.join(HERE, "_ref", "libngref_ngb.so")
 
 TIE_AOV_INSTANCE = 1
 TIE_AOV_TRIANGLE = 2
@@ -245,12 +246,14 @@ def geom_matrices(geom_xpos, geom_xmat, geom_of_instance, scale):
 _ref_libs: dict = {}
 
 
-def reference_available(cuda=False) -> bool:
-    return os.path.exists(REF_CUDA_SO if cuda else REF_SO)
+def reference_available(cuda=False, ngb=False) -> bool:
+    return os.path.exists(REF_NGB_SO if ngb else REF_CUDA_SO if cuda else REF_SO)
 
 
-def ref_lib(cuda=False):
-    path = REF_CUDA_SO if cuda else REF_SO
+def ref_lib(cuda=False, ngb=False):
+    """The reference's library: its CPU backend, its CUDA backend (cuda), or its Device::Cuda drawing through this
+    library by oracle/ngb_backend.cpp (ngb)."""
+    path = REF_NGB_SO if ngb else REF_CUDA_SO if cuda else REF_SO
     if path not in _ref_libs:
         if not os.path.exists(path):
             raise RuntimeError(f"{path} is not built: run `make -C oracle ref` where the reference's sources are")
@@ -289,6 +292,12 @@ def ref_lib(cuda=False):
     return _ref_libs[path]
 
 
+def _use_meshes(lib, desc):
+    """The meshes ngb_backend.cpp hands the library (the reference's backend seam carries only their trees)."""
+    lib.ngref_use_meshes.argtypes = [C.POINTER(_abi.MeshC), C.c_int]
+    lib.ngref_use_meshes(desc.c.meshes, desc.c.mesh_count)
+
+
 class ReferenceError_(ValueError):
     pass
 
@@ -304,13 +313,15 @@ def _ref_check(lib, status):
 class Reference:
     """neraulgraphics 0.5.0's own BatchRenderer (Device::Cpu, or Device::Cuda with cuda=True)."""
 
-    def __init__(self, desc: SceneDesc, cuda=False, threads=None):
-        self.lib = ref_lib(cuda)
+    def __init__(self, desc: SceneDesc, cuda=False, threads=None, ngb=False):
+        self.lib = ref_lib(cuda, ngb)
         self.desc = desc
         if threads is not None:
             self.lib.ngref_set_threads(int(threads))
+        if ngb:
+            _use_meshes(self.lib, desc)
         h = C.c_void_p()
-        _ref_check(self.lib, self.lib.ngref_create(C.byref(desc.c), 1 if cuda else 0, C.byref(h)))
+        _ref_check(self.lib, self.lib.ngref_create(C.byref(desc.c), 1 if (cuda or ngb) else 0, C.byref(h)))
         self.h = h
 
     def __del__(self):
@@ -386,8 +397,8 @@ class ReferenceView:
     """neraulgraphics 0.5.0's own single-view Renderer (Device::Cpu, or Device::Cuda with cuda=True) on a scene
     of one world (desc.width x desc.height)."""
 
-    def __init__(self, desc: SceneDesc, cuda=False, threads=None):
-        self.lib = ref_lib(cuda)
+    def __init__(self, desc: SceneDesc, cuda=False, threads=None, ngb=False):
+        self.lib = ref_lib(cuda, ngb)
         for name, args in (("ngref_view_create", [C.POINTER(_abi.SceneC), C.c_int, C.POINTER(C.c_void_p)]),
                            ("ngref_view_destroy", [C.c_void_p]), ("ngref_view_set_matrices", [C.c_void_p, _f32p]),
                            ("ngref_view_set_ambient", [C.c_void_p, C.c_float]),
@@ -399,8 +410,10 @@ class ReferenceView:
         self.desc = desc
         if threads is not None:
             self.lib.ngref_set_threads(int(threads))
+        if ngb:
+            _use_meshes(self.lib, desc)
         h = C.c_void_p()
-        _ref_check(self.lib, self.lib.ngref_view_create(C.byref(desc.c), 1 if cuda else 0, C.byref(h)))
+        _ref_check(self.lib, self.lib.ngref_view_create(C.byref(desc.c), 1 if (cuda or ngb) else 0, C.byref(h)))
         self.h = h
 
     def __del__(self):
