@@ -458,7 +458,7 @@ def run_ours(args, rank, world, local_rank, dist):
         # kernel and the camera, shade and shadow kernels (tile path), or the camera-basis and one render kernel.
         "gpu_launches": (2 + (4 if len(stage_ms) == 3 else 2)) * K,
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
-                                                                            "leaf_batch", "ms")},
+                                                                            "leaf_batch", "fetch", "paired", "ms")},
         # The renderers' own device arrays (scene, trees, per-pixel scratch; ngb_device_bytes), not the images.
         "device_mb": round(ng.device_bytes() / 1e6, 1),
         "differentiable": differentiable,
@@ -548,7 +548,7 @@ def run_large(args, rank, world, local_rank, dist):
         "step_ms": [round(stage[0][k] + stage[1][k] + stage[2][k], 3) for k in range(K)],
         "lidar_rays_per_s": round(rays / (statistics.median(stage[2]) / 1000.0), 1),
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
-                                                                            "leaf_batch", "ms")},
+                                                                            "leaf_batch", "fetch", "paired", "ms")},
         "lidar_hit_fraction": round(hit_frac, 4),
         "clocks": clocks.summary(),
     }
@@ -759,8 +759,9 @@ def uneven_figures(dev, K, W, seed=0, buckets=False):
     first = r.instance_first
     res = {"images_per_s": round(views / (graph_ms / 1000.0), 1), "ms_per_step": round(graph_ms, 4),
            "kernel_shape": {k: tuned[k] for k in tuned if k != "timings"},
-           "shape_timings_ms": {f"{t['threads']}/{t['registers']}" + (f" {t['tile']}" if "tile" in t else ""):
-                                round(t["ms"], 4) for t in tuned["timings"]},
+           "shape_timings_ms": {f"{t['threads']}/{t['registers']} fetch {t['fetch']} "
+                                f"{'paired' if t['paired'] else 'one kind'}": round(t["ms"], 4)
+                                for t in tuned["timings"]},
            "graph_matches_eager": same, "gpu_launches_per_step": 6,
            "workload": f"uneven_worlds: {views} worlds, {int(first[-1])} instances, {r.pixel_count} pixels; six "
                        "meshes of 12 to 20480 triangles; one light, spp 1, RGB+depth+ID"}

@@ -326,6 +326,13 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
 int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, int32_t refill_lanes, int32_t registers,
     int32_t leaf_batch);
 
+/* The tile kernels' work shape (kernel 0 or 3 of ngb_set_tuning): tiles_per_fetch (1 to 8) tiles of 32 rays a warp
+ * takes with one atomic, 32 to 256 rays per fetch (default 1: the finest balance at the end of a launch); paired 1
+ * (default): when a render asks for the picture and the centre-ray images, the camera kernel puts each pixel's two
+ * rays on adjacent lanes of a 4 x 4 tile, one pass; 0: 8 x 4 tiles of one kind of ray, two passes. The images
+ * are the same bit for bit either way. No counterpart in the reference. */
+int ngb_set_tile_shape(ngb_renderer *r, int32_t tiles_per_fetch, int32_t paired);
+
 /* How the instance trees are built. mode 0 (default): one fused launch of per-world groups when a world
  * holds at most 1024 instances, else the global build; 1: always the per-world build (at most 1024 instances
  * per world); 2: always the global build (global radix sort, Karras nodes, bottom-up refit over global

@@ -139,6 +139,11 @@ struct PersistentTuning {
     int refill;       // a warp fetches new pixels once this many of its lanes are idle
     int registers;    // register budget per thread: 48, 64 or 72 (not every pair with threads is built)
     int leaf_batch;   // a warp takes a leaf step once this many lanes wait at leaves (or none is at an inner node)
+    // The tile kernels' shape: tiles (of 32 rays) a warp takes per fetch, and whether the camera kernel puts a
+    // pixel's two rays on adjacent lanes of a 4 x 4 tile (when a render asks for both kinds) or traces 8 x 4 tiles
+    // of one kind at a time.
+    int tile_fetch = 1;
+    int tile_pairs = 1;
 };
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
     const PersistentTuning &t, cudaStream_t stream);

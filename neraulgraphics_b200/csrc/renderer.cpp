@@ -1509,7 +1509,8 @@ int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, i
             ngb::require(built, "for the tile kernel, threads_per_block and registers must be one of 128/48, 128/56, "
                 "128/64, 128/80, 256/64");
             r.kernel_choice = kernel;
-            r.tile_tuning = ngb::PersistentTuning{threads_per_block, 0, registers, 0};
+            r.tile_tuning.threads = threads_per_block;
+            r.tile_tuning.registers = registers;
             return;
         }
         const bool built = (threads_per_block == 128 && (registers == 48 || registers == 64 || registers == 72)) ||
@@ -1519,6 +1520,16 @@ int ngb_set_tuning(ngb_renderer *h, int32_t kernel, int32_t threads_per_block, i
         ngb::require(leaf_batch >= 1 && leaf_batch <= 32, "leaf_batch must be 1 to 32");
         r.kernel_choice = kernel;
         r.tuning = ngb::PersistentTuning{threads_per_block, refill_lanes, registers, leaf_batch};
+    });
+}
+
+int ngb_set_tile_shape(ngb_renderer *h, int32_t tiles_per_fetch, int32_t paired) {
+    return guarded(h, [&](ngb::Renderer &r) {
+        ngb::require(tiles_per_fetch >= 1 && tiles_per_fetch <= 8, "tiles_per_fetch must be 1 to 8, got " +
+            std::to_string(tiles_per_fetch));
+        ngb::require(paired == 0 || paired == 1, "paired must be 0 or 1");
+        r.tile_tuning.tile_fetch = tiles_per_fetch;
+        r.tile_tuning.tile_pairs = paired;
     });
 }
 

@@ -37,7 +37,6 @@ using namespace tr;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int TILE_W = 8, TILE_H = 4;
 constexpr int WALK_STACK = 64;      // a mesh's tree is at most 60 deep
-constexpr int TILES_PER_FETCH = 1;  // tiles a warp takes with one atomic (1: the finest balance, measured fastest)
 
 // A tile's candidate instances as its warp holds them: each one's position in its world's run of sorted
 // leaves and the distance below which no camera ray of the tile can enter its box, collected in leaf order,
@@ -429,12 +428,13 @@ __device__ __forceinline__ TileAt pair_tile_at(const RenderArgs &a, long long ti
     return t;
 }
 
-// A warp's next run of tiles, TILES_PER_FETCH of them from one atomic; first >= tiles when none are left.
-__device__ __forceinline__ long long fetch_tiles(int *counter, int lane) {
+// A warp's next run of tiles, fetch of them from one atomic (32 rays each; a tuning choice: 1 gives the finest
+// balance at the end of a launch, more fewer atomics); first >= tiles when none are left.
+__device__ __forceinline__ long long fetch_tiles(int *counter, int lane, int fetch) {
     long long first = 0;
     if (lane == 0)
         first = static_cast<long long>(atomicAdd(reinterpret_cast<unsigned long long *>(counter),
-            static_cast<unsigned long long>(TILES_PER_FETCH)));
+            static_cast<unsigned long long>(fetch)));
     return __shfl_sync(FULL, first, 0);
 }
 
@@ -458,7 +458,7 @@ constexpr int CODE_NONE = -1, CODE_FLOOR = -2, CODE_SPHERE = -3;
 // hits written for the shade kernel).
 template <int THREADS, int MIN_BLOCKS, int CAP, bool PAIRED>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const __grid_constant__ SceneParams s,
-    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
+    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view, int fetch) {
     __shared__ WarpSmem<CAP> warp_smem[THREADS / 32];
     WarpSmem<CAP> &sm = warp_smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -467,9 +467,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
     const bool want_aov = a.depth || a.normal || a.object_id || a.hit_instance;
     const float fs = a.fov_scale;
     for (;;) {
-        const long long first = fetch_tiles(counter, lane);
+        const long long first = fetch_tiles(counter, lane, fetch);
         if (first >= tiles) break;
-        const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
+        const long long last = first + fetch < tiles ? first + fetch : tiles;
         for (long long tile = first; tile < last; ++tile) {
             const TileAt T = PAIRED ? pair_tile_at(a, tile, tiles_x, tiles_per_view, lane)
                                     : tile_at(a, tile, tiles_x, tiles_per_view, lane);
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ Scen
 // is taken over the segments' own end points, so any axis is a valid test; these make it a tight one.
 template <int THREADS, int MIN_BLOCKS, int CAP>
 __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const __grid_constant__ SceneParams s,
-    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view) {
+    const RenderArgs a, int *counter, long long tiles, int tiles_x, int tiles_per_view, int fetch) {
     __shared__ int warp_cand[THREADS / 32][CAP];
     int *cand_leaf = warp_cand[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -809,9 +809,9 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
     const DevLight &lt = s.lights[0];
     const float INF = __int_as_float(0x7f800000);
     for (;;) {
-        const long long first = fetch_tiles(counter, lane);
+        const long long first = fetch_tiles(counter, lane, fetch);
         if (first >= tiles) break;
-        const long long last = first + TILES_PER_FETCH < tiles ? first + TILES_PER_FETCH : tiles;
+        const long long last = first + fetch < tiles ? first + fetch : tiles;
         for (long long tile = first; tile < last; ++tile) {
             const TileAt T = tile_at(a, tile, tiles_x, tiles_per_view, lane);
             const int P = s.instance_count > 0 ? world_count_of(s, T.world) : 0;
@@ -922,7 +922,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
 
 template <class Kernel>
 cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const RenderArgs &a, int *counter,
-    long long tiles, int tiles_x, int tiles_per_view, cudaStream_t stream) {
+    long long tiles, int tiles_x, int tiles_per_view, int fetch, cudaStream_t stream) {
     int device = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -931,17 +931,18 @@ cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const
     if (per_sm < 1) per_sm = 1;
     // Every SM full of resident warps, and no more warps than there are fetches of tiles.
     long long blocks = static_cast<long long>(sms) * per_sm;
-    const long long needed = (tiles + TILES_PER_FETCH * (threads / 32) - 1) / (TILES_PER_FETCH * (threads / 32));
+    const long long needed = (tiles + fetch * (threads / 32) - 1) / (fetch * (threads / 32));
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    kernel<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(s, a, counter, tiles, tiles_x, tiles_per_view);
+    kernel<<<static_cast<unsigned>(blocks), threads, 0, stream>>>(s, a, counter, tiles, tiles_x, tiles_per_view, fetch);
     return cudaGetLastError();
 }
 
 template <int THREADS, int MIN_BLOCKS, int CAP>
-cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream,
-    cudaEvent_t after_camera, cudaEvent_t after_shade) {
+cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
+    cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade) {
+    const int fetch = t.tile_fetch;
     const int tiles_x = (a.width + TILE_W - 1) / TILE_W, tiles_y = (a.rows + TILE_H - 1) / TILE_H;
     const int tiles_per_view = tiles_x * tiles_y;
     const long long tiles = a.view_info ? a.total_tiles : static_cast<long long>(tiles_per_view) * a.views;
@@ -957,15 +958,15 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
     }
     if (!a.basis_given) e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
     // Both kinds of camera ray: paired 4 x 4 tiles (pair_tile_at).
-    const bool paired = a.rgb && aov && (!a.view_info || a.view_pair_tile);
+    const bool paired = t.tile_pairs && a.rgb && aov && (!a.view_info || a.view_pair_tile);
     if (e == cudaSuccess && paired) {
         const int ptx = (a.width + 3) / 4, pty = (a.rows + 3) / 4;
         const long long pair_tiles = a.view_info ? a.total_pair_tiles : static_cast<long long>(ptx) * pty * a.views;
         e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, true>, THREADS, s, a, counter, pair_tiles, ptx,
-            ptx * pty, stream);
+            ptx * pty, fetch, stream);
     } else if (e == cudaSuccess) {
         e = launch_tiles(camera_tiles_kernel<THREADS, MIN_BLOCKS, CAP, false>, THREADS, s, a, counter, tiles, tiles_x,
-            tiles_per_view, stream);
+            tiles_per_view, fetch, stream);
     }
     mark(after_camera);
     if (e != cudaSuccess || !a.rgb) {
@@ -990,7 +991,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         return launch_shadows_persistent(s, a, counter, stream);
     } else {
         return launch_tiles(shadow_tiles_kernel<THREADS, MIN_BLOCKS, CAP>, THREADS, s, a, counter, tiles, tiles_x,
-            tiles_per_view, stream);
+            tiles_per_view, fetch, stream);
     }
 }
 
@@ -1002,29 +1003,29 @@ cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *
     // capacity: 32 for worlds of up to 32 instances, else TILE_MAX_INSTANCES; larger worlds walk their tree
     // as a packet (capacity 0).
     if (s.instance_count > 0 && s.per_world > TILE_MAX_INSTANCES) {
-        if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8, 0>(s, a, counter, stream, after_camera, after_shade);
-        if (t.threads == 128 && t.registers == 56) return launch_variant<128, 9, 0>(s, a, counter, stream, after_camera, after_shade);
-        if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10, 0>(s, a, counter, stream, after_camera, after_shade);
-        if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6, 0>(s, a, counter, stream, after_camera, after_shade);
-        if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4, 0>(s, a, counter, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 64) return launch_variant<128, 8, 0>(s, a, counter, t, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 56) return launch_variant<128, 9, 0>(s, a, counter, t, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 48) return launch_variant<128, 10, 0>(s, a, counter, t, stream, after_camera, after_shade);
+        if (t.threads == 128 && t.registers == 80) return launch_variant<128, 6, 0>(s, a, counter, t, stream, after_camera, after_shade);
+        if (t.threads == 256 && t.registers == 64) return launch_variant<256, 4, 0>(s, a, counter, t, stream, after_camera, after_shade);
         return cudaErrorInvalidValue;
     }
     const bool small = s.per_world <= 32;
     if (t.threads == 128 && t.registers == 64)
-        return small ? launch_variant<128, 8, 32>(s, a, counter, stream, after_camera, after_shade)
-                     : launch_variant<128, 8, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+        return small ? launch_variant<128, 8, 32>(s, a, counter, t, stream, after_camera, after_shade)
+                     : launch_variant<128, 8, TILE_MAX_INSTANCES>(s, a, counter, t, stream, after_camera, after_shade);
     if (t.threads == 128 && t.registers == 56)
-        return small ? launch_variant<128, 9, 32>(s, a, counter, stream, after_camera, after_shade)
-                     : launch_variant<128, 9, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+        return small ? launch_variant<128, 9, 32>(s, a, counter, t, stream, after_camera, after_shade)
+                     : launch_variant<128, 9, TILE_MAX_INSTANCES>(s, a, counter, t, stream, after_camera, after_shade);
     if (t.threads == 128 && t.registers == 48)
-        return small ? launch_variant<128, 10, 32>(s, a, counter, stream, after_camera, after_shade)
-                     : launch_variant<128, 10, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+        return small ? launch_variant<128, 10, 32>(s, a, counter, t, stream, after_camera, after_shade)
+                     : launch_variant<128, 10, TILE_MAX_INSTANCES>(s, a, counter, t, stream, after_camera, after_shade);
     if (t.threads == 128 && t.registers == 80)
-        return small ? launch_variant<128, 6, 32>(s, a, counter, stream, after_camera, after_shade)
-                     : launch_variant<128, 6, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+        return small ? launch_variant<128, 6, 32>(s, a, counter, t, stream, after_camera, after_shade)
+                     : launch_variant<128, 6, TILE_MAX_INSTANCES>(s, a, counter, t, stream, after_camera, after_shade);
     if (t.threads == 256 && t.registers == 64)
-        return small ? launch_variant<256, 4, 32>(s, a, counter, stream, after_camera, after_shade)
-                     : launch_variant<256, 4, TILE_MAX_INSTANCES>(s, a, counter, stream, after_camera, after_shade);
+        return small ? launch_variant<256, 4, 32>(s, a, counter, t, stream, after_camera, after_shade)
+                     : launch_variant<256, 4, TILE_MAX_INSTANCES>(s, a, counter, t, stream, after_camera, after_shade);
     return cudaErrorInvalidValue;
 }
 

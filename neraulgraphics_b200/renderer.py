@@ -429,6 +429,11 @@ class BatchRenderer:
         check(self._lib.ngb_set_tuning(self._h, int(kernel), int(threads_per_block), int(refill_lanes), int(registers),
                                        int(leaf_batch)), self._h)
 
+    def set_tile_shape(self, tiles_per_fetch=1, paired=True):
+        """The tile kernels' work shape: tiles of 32 rays a warp takes per fetch (1 to 8), and whether a pixel's
+        picture and centre rays share a 4 x 4 tile (paired) or run as 8 x 4 tiles of one kind. Same images."""
+        check(self._lib.ngb_set_tile_shape(self._h, int(tiles_per_fetch), 1 if paired else 0), self._h)
+
     def set_build(self, mode=0):
         """Instance-tree build: 0 automatic (per-world groups up to 1024 instances per world, else global),
         1 per-world, 2 global. Both make the same tree."""

@@ -386,6 +386,26 @@ def test_tile_kernel_tunings_agree(torch_cuda):
             first = got
         else:
             assert_same_images(got, first, rgb_tol=0)
+    for fetch in (1, 2, 3, 8):
+        for paired in (True, False):
+            r.set_tuning(kernel=3, threads_per_block=128, registers=56)
+            r.set_tile_shape(fetch, paired)
+            assert_same_images(r.render(wl.cameras, 1.0, 1, **out), first, rgb_tol=0)
+
+
+def test_tile_shapes_agree_on_uneven_worlds(torch_cuda):
+    """Tiles per fetch and paired or one-kind camera tiles: the same images bit for bit on worlds of uneven sizes."""
+    worlds, meshes, floor, lights, mats, cams = uneven_scene(seed=6)
+    u = ng.UnevenBatchRenderer(worlds, lights=lights, floor=floor, meshes=meshes, device="cuda:0")
+    u.set_instance_transforms(mats)
+    first = u.render(cams, 1.0, 1, **ALL, frame=1)
+    for fetch in (1, 2, 4):
+        for paired in (True, False):
+            u.set_tile_shape(fetch, paired)
+            got = u.render(cams, 1.0, 1, **ALL, frame=1)
+            for k in first:
+                assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint8),
+                                      np.ascontiguousarray(first[k]).view(np.uint8)), (k, fetch, paired)
 
 
 def test_tile_kernel_on_worlds_of_one_to_256_instances(torch_cuda):
