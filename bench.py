@@ -184,22 +184,34 @@ def algorithmic_bytes_per_image(wl, blas_bytes):
     return out + inputs + build
 
 
-def l2_copy_gbs(torch, dev, mib=16, repeats=200):
-    """Copy bandwidth between two buffers that stay in L2 (2 x 16 MiB), read + write bytes over CUDA-event time:
-    this GPU's on-chip figure for byte rates served from cache."""
-    a = torch.empty(mib << 18, dtype=torch.float32, device=dev)
+def l2_copy_gbs(torch, dev, mib=32, copies=50, replays=10):
+    """Copy bandwidth between two buffers that stay in L2 (2 x 32 MiB), read + write bytes over CUDA-event time, the
+    copies captured in a CUDA graph so that launches do not separate them: this GPU's on-chip figure for byte rates
+    served from cache (9.75 TB/s measured on a B200, against 6.44 TB/s for a copy through HBM)."""
+    a = torch.ones(mib << 18, dtype=torch.float32, device=dev)
     b = torch.empty_like(a)
-    a.fill_(1.0)
-    for _ in range(10):
-        b.copy_(a)
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            b.copy_(a)
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(copies):
+            b.copy_(a)
+    graph.replay()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(repeats):
-        b.copy_(a)
+    for _ in range(replays):
+        graph.replay()
     e1.record()
     e1.synchronize()
-    return 2 * a.numel() * 4 * repeats / (e0.elapsed_time(e1) / 1000.0) / 1e9
+    gbs = 2 * a.numel() * 4 * copies * replays / (e0.elapsed_time(e1) / 1000.0) / 1e9
+    del graph
+    return gbs
 
 
 def cpu_baseline(wl, steps_poses, seconds, sample_worlds=64, count_worlds=16):
@@ -439,7 +451,8 @@ def run_ours(args, rank, world, local_rank, dist):
             "frac_of_l2_copy": round(counts["traversal_bytes_per_image"] * value / 1e9 / l2_gbs, 3),
             "what": "bytes the reference's walks fetch per image (32 per node, 64 per child-box pair, 48 per "
                     "instance inverse, 48 per triangle; the oracle's count) at this build's images/s, against "
-                    "this GPU's copy bandwidth between two buffers resident in L2, measured in this run"},
+                    "this GPU's copy bandwidth between two buffers resident in L2 (graph-captured copies), measured "
+                    "in this run"},
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "steps": KE, "path": "pinned host poses and cameras -> device (copy) -> BatchRenderer.set_body_poses + render(into= one of "
                         "two device image sets) -> pinned host images on a copy stream, overlapping the next step"},
