@@ -315,8 +315,9 @@ int ngb_set_sync(ngb_renderer *r, int32_t synchronous, double timeout_seconds);
  * light, no material with reflectivity >= 1e-3; else the per-pixel kernel), 1 the per-pixel kernel,
  * 2 the persistent kernel where it applies, 3 the tile kernels where the persistent kernel applies (worlds of
  * at most 256 instances through per-tile candidate lists, larger ones walking their tree as a warp packet).
- * Ray queries (ngb_cast_rays) take the persistent kernel in a shape of their own (256/64, refill 28, no leaf
- * batching) unless kernel 2 is chosen, whose shape they then take, or kernel 1 (the per-thread ray kernel).
+ * Ray queries (ngb_cast_rays), unless ngb_set_ray_kernel chose otherwise, take warp packets in worlds above 256
+ * instances (kernel 0 or 3) and else the persistent kernel in a shape of their own (256/64, refill 28, no leaf
+ * batching), unless kernel 2 is chosen, whose shape they then take, or kernel 1 (the per-thread ray kernel).
  * With kernel 3 the call sets the tile kernel's shape: threads_per_block and registers as one of 128/48,
  * 128/56, 128/64, 128/80, 256/64 (default 128/56); refill_lanes and leaf_batch are not read.
  * Otherwise it sets the persistent kernel's shape: threads_per_block and registers (the register budget per
@@ -332,6 +333,14 @@ int ngb_set_tuning(ngb_renderer *r, int32_t kernel, int32_t threads_per_block, i
  * rays on adjacent lanes of a 4 x 4 tile, one pass; 0: 8 x 4 tiles of one kind of ray, two passes. The images
  * are the same bit for bit either way. No counterpart in the reference. */
 int ngb_set_tile_shape(ngb_renderer *r, int32_t tiles_per_fetch, int32_t paired);
+
+/* Which kernel answers ray queries (ngb_cast_rays): 0 automatic (warp packets for worlds above 256 instances, else
+ * as ngb_set_tuning describes), 1 one thread per ray, 2 the persistent kernel (lanes refilled as their rays end),
+ * 3 warp packets: 32 consecutive rays of a world per
+ * warp walking the world's tree together, each lane entering only what its own ray enters (for rays of one
+ * sensor in scan order, such as a LiDAR's beams). The same hits every way, up to which of two equally distant hits
+ * is kept. No counterpart in the reference. */
+int ngb_set_ray_kernel(ngb_renderer *r, int32_t kernel);
 
 /* How the instance trees are built. mode 0 (default): one fused launch of per-world groups when a world
  * holds at most 1024 instances, else the global build; 1: always the per-world build (at most 1024 instances

@@ -78,6 +78,7 @@ def lib():
     L.ngb_set_tuning.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.ngb_set_build.argtypes = [_vp, C.c_int32]
     L.ngb_set_tile_shape.argtypes = [_vp, C.c_int32, C.c_int32]
+    L.ngb_set_ray_kernel.argtypes = [_vp, C.c_int32]
     L.ngb_make_camera.argtypes = [_abi.Vec3, _abi.Vec3, _abi.Vec3, C.c_float, C.c_int32, C.c_int32,
                                   C.POINTER(_abi.CameraC)]
     L.ngb_render_view.argtypes = [_vp, C.POINTER(_abi.CameraC), C.c_int32, C.c_int32, _vp]

@@ -153,6 +153,8 @@ cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, 
 cudaError_t launch_shadows_persistent(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream);
 cudaError_t launch_rays_persistent(const SceneParams &s, const RayArgs &r, int *counter, const PersistentTuning &t,
     cudaStream_t stream);
+// Ray queries as warp packets over each world's tree: 32 consecutive rays of a world per warp (see tiles.cu).
+cudaError_t launch_rays_packets(const SceneParams &s, const RayArgs &r, int *counter, cudaStream_t stream);
 
 // The tile render: the persistent kernel's cases, for worlds of at most TILE_MAX_INSTANCES instances (see
 // tiles.cu). Of the tuning, threads and registers are read: 128/48, 128/56, 128/64, 128/80 or 256/64.

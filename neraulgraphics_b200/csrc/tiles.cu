@@ -920,6 +920,56 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
     }
 }
 
+// Ray queries as warp packets (cast_ray, src/render_core.h:331-349): a warp takes 32 consecutive rays of one world
+// and walks the world's tree as a packet (packet_walk: every node some lane's ray enters, visited once for all
+// lanes, each lane entering only the instances its own ray enters), then each lane resolves its own hit. Rays
+// from one sensor in scan order (a LiDAR's neighbouring beams) enter nearly the same nodes, so the warp's lanes
+// share the walk instead of each walking alone; every ray still gets its own walk's closest hit (up to which of
+// two equally distant hits is kept).
+template <int THREADS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(THREADS, MIN_BLOCKS) ray_packets_kernel(const __grid_constant__ SceneParams s,
+    const RayArgs r, int *counter, long long groups, int groups_per_world) {
+    __shared__ WarpSmem<0> warp_smem[THREADS / 32];
+    WarpSmem<0> &sm = warp_smem[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int max_steps = s.blas_node_count + 2;
+    for (;;) {
+        const long long g = fetch_tiles(counter, lane, 1);
+        if (g >= groups) break;
+        const int world = static_cast<int>(g / groups_per_world);
+        const int local = static_cast<int>(g % groups_per_world) * 32 + lane;
+        const bool valid = local < r.rays_per_world;
+        const long long i = static_cast<long long>(world) * r.rays_per_world + local;
+        float3 o = mk3(0.0f, 0.0f, 0.0f), d = mk3(0.0f, 0.0f, 1.0f);
+        bool live = false;
+        if (valid) {
+            o = mk3(__ldg(r.origins + 3 * i), __ldg(r.origins + 3 * i + 1), __ldg(r.origins + 3 * i + 2));
+            d = mk3(__ldg(r.directions + 3 * i), __ldg(r.directions + 3 * i + 1), __ldg(r.directions + 3 * i + 2));
+            const float len2 = dot(d, d);
+            live = len2 > 1e-30f && len2 < 1e30f;  // compared with >, so a NaN direction is a miss too
+            if (live) d = d * (1.0f / sqrtf(len2));
+            else d = mk3(0.0f, 0.0f, 1.0f);
+        }
+        int best_sphere = -1;
+        bool hit_floor = false;
+        float tmax = live ? spheres_and_floor(s, o, d, best_sphere, hit_floor) : 0.0f;
+        int hit_inst = -1, hit_tri = -1;
+        float hu = 0.0f, hv = 0.0f;
+        packet_walk(s, sm, lane, world, live, o, d, tmax, hit_inst, hit_tri, hu, hv, max_steps, r.error_flag);
+        if (!valid) continue;
+        const bool found = live && (hit_inst >= 0 || best_sphere >= 0 || hit_floor) && tmax <= r.max_distance;
+        float3 normal = mk3(0.0f, 0.0f, 0.0f);
+        DevMaterial mat{};
+        int object = OBJECT_NONE;
+        if (found) resolve(s, world, o + d * tmax, d, hit_inst, hit_tri, hu, hv, best_sphere, hit_floor, normal, mat, object);
+        r.distance[i] = found ? tmax : __int_as_float(0x7f800000);
+        r.normal[3 * i] = normal.x;
+        r.normal[3 * i + 1] = normal.y;
+        r.normal[3 * i + 2] = normal.z;
+        r.object_id[i] = found ? object : OBJECT_NONE;
+    }
+}
+
 template <class Kernel>
 cudaError_t launch_tiles(Kernel kernel, int threads, const SceneParams &s, const RenderArgs &a, int *counter,
     long long tiles, int tiles_x, int tiles_per_view, int fetch, cudaStream_t stream) {
@@ -996,6 +1046,27 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
 }
 
 }  // namespace
+
+cudaError_t launch_rays_packets(const SceneParams &s, const RayArgs &r, int *counter, cudaStream_t stream) {
+    if (r.count <= 0 || r.rays_per_world <= 0) return cudaSuccess;
+    constexpr int THREADS = 128;
+    auto kernel = ray_packets_kernel<THREADS, 9>;
+    const int groups_per_world = (r.rays_per_world + 31) / 32;
+    const long long groups = static_cast<long long>(groups_per_world) * (r.count / r.rays_per_world);
+    int device = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long blocks = static_cast<long long>(sms) * per_sm;
+    const long long needed = (groups + THREADS / 32 - 1) / (THREADS / 32);
+    if (blocks > needed) blocks = needed;
+    e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    kernel<<<static_cast<unsigned>(blocks), THREADS, 0, stream>>>(s, r, counter, groups, groups_per_world);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_render_tiles(const SceneParams &s, const RenderArgs &a, int *counter, const PersistentTuning &t,
     cudaStream_t stream, cudaEvent_t after_camera, cudaEvent_t after_shade) {

@@ -434,6 +434,11 @@ class BatchRenderer:
         picture and centre rays share a 4 x 4 tile (paired) or run as 8 x 4 tiles of one kind. Same images."""
         check(self._lib.ngb_set_tile_shape(self._h, int(tiles_per_fetch), 1 if paired else 0), self._h)
 
+    def set_ray_kernel(self, kernel=0):
+        """Which kernel answers cast_rays: 0 automatic, 1 one thread per ray, 2 persistent (lane refill), 3 warp
+        packets (32 consecutive rays per warp walking the world tree together). Same hits."""
+        check(self._lib.ngb_set_ray_kernel(self._h, int(kernel)), self._h)
+
     def set_build(self, mode=0):
         """Instance-tree build: 0 automatic (per-world groups up to 1024 instances per world, else global),
         1 per-world, 2 global. Both make the same tree."""

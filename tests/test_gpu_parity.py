@@ -435,12 +435,14 @@ def test_large_world_renders_and_casts_rays(torch_cuda):
     e, a = np.meshgrid(el, az, indexing="ij")
     dirs = np.stack([np.cos(e) * np.sin(a), np.sin(e), -np.cos(e) * np.cos(a)], -1).reshape(1, -1, 3).astype(np.float32)
     origins = np.tile(np.float32([0.0, 0.0, -40.0]), (1, dirs.shape[1], 1))
-    got = r.cast_rays(origins, dirs, 100.0)
     exp = o.cast_rays(origins, dirs, 100.0)
-    assert (got["object_id"] >= 34).mean() > 0.2
-    assert np.array_equal(got["object_id"], exp["object_id"])
-    assert np.array_equal(bits(got["distance"]), bits(exp["distance"]))
-    assert np.array_equal(bits(got["normal"]), bits(exp["normal"]))
+    for kernel in (0, 2, 1):  # automatic (warp packets in a world this large), persistent, per thread
+        r.set_ray_kernel(kernel)
+        got = r.cast_rays(origins, dirs, 100.0)
+        assert (got["object_id"] >= 34).mean() > 0.2
+        assert np.array_equal(got["object_id"], exp["object_id"])
+        assert np.array_equal(bits(got["distance"]), bits(exp["distance"]))
+        assert np.array_equal(bits(got["normal"]), bits(exp["normal"]))
 
 
 def uneven_scene(seed=4):
@@ -534,9 +536,9 @@ def test_uneven_step_captured_in_a_cuda_graph_is_the_eager_step(torch_cuda):
 
 
 def test_ray_queries_on_both_kernels(torch_cuda):
-    """Ray queries through the persistent kernel's walk (the default) and the per-thread kernel: the same
-    distances, normals and IDs, with rays of zero length, rays stopped by max_distance and rays in worlds
-    of their own."""
+    """Ray queries through the persistent kernel's walk (the default here), the per-thread kernel and warp
+    packets: the same distances, normals and IDs, with rays of zero length, rays stopped by max_distance and rays
+    in worlds of their own (500 rays a world: a partial packet at each world's end)."""
     wl = workloads.body_worlds(worlds=8, seed=6)
     r, o = product(wl.desc), O.Oracle(wl.desc)
     for x in (r, o):
@@ -548,12 +550,15 @@ def test_ray_queries_on_both_kernels(torch_cuda):
     dirs[:, ::50] = 0.0  # no direction: a miss
     want = o.cast_rays(origins, dirs, 4.0)
     got = r.cast_rays(origins, dirs, 4.0)
+    r.set_ray_kernel(3)
+    packets = r.cast_rays(origins, dirs, 4.0)
+    r.set_ray_kernel(0)
     r.set_tuning(kernel=1)
     per_thread = r.cast_rays(origins, dirs, 4.0)
     assert (want["object_id"] > 0).mean() > 0.2 and np.isinf(want["distance"]).mean() > 0.1
     for k in ("object_id", "distance", "normal"):
-        assert np.array_equal(np.asarray(got[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
-        assert np.array_equal(np.asarray(per_thread[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
+        for each in (got, per_thread, packets):
+            assert np.array_equal(np.asarray(each[k]).view(np.uint32), np.asarray(want[k]).view(np.uint32)), k
 
 
 def l_prism(depth=0.6):
