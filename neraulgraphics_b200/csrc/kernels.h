@@ -106,6 +106,11 @@ struct RenderArgs {
     // its samples this frame) goes to radiance instead of bytes to rgb, for launch_accumulate.
     int basis_given;
     float4 *radiance;
+    // The tile kernels' per-view candidate order (views x order_stride): instances by the eye's distance to their
+    // boxes, and those distances (see tiles.cu view_order_kernel).
+    int *view_order;
+    float *view_bound;
+    int order_stride;
 };
 
 // The running average of a single-view renderer's pictures (render_pixel, src/render_core.h:288-301): per pixel

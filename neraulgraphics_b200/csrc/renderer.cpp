@@ -156,6 +156,8 @@ struct Renderer {
     DevBuf<float4> camera_basis;              // the persistent and tile renders' per-view cameras
     DevBuf<float4> pic_hit, shadow_o, shadow_d;  // the tile render's per-pixel hand-over between its kernels
     DevBuf<int> pic_code, shadow_self;
+    DevBuf<int> view_order;                   // the tile render's per-view candidate order, and its bounds
+    DevBuf<float> view_bound;
     DevBuf<float> srgb_table;                 // 256 sRGB byte thresholds
     // Single-view renders (ngb_render_view): the running sums of the picture (zeroed when made, so a first render
     // with frame > 0 adds to zero), this frame's radiance, and the average's 0xAARRGGBB pixels.
@@ -564,6 +566,7 @@ void Renderer::teardown() {
     large_aabb.release(), large_bounds.release(), large_ids_a.release(), large_ids_b.release();
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
     pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release(), shadow_self.release();
+    view_order.release(), view_bound.release();
     leaf_of.release(), slot_hull.release();
     camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
@@ -1001,6 +1004,11 @@ void Renderer::render(const float *cams, float fov, int spp, unsigned outputs, i
     if (timed) CK(cudaEventRecord(ev_start, stream));
     if (tiles) {
         a.camera_basis = camera_basis.ensure(3 * static_cast<size_t>(views));
+        if (per_world > 0 && per_world <= TILE_MAX_INSTANCES) {
+            a.view_order = view_order.ensure(static_cast<size_t>(views) * per_world);
+            a.view_bound = view_bound.ensure(static_cast<size_t>(views) * per_world);
+            a.order_stride = per_world;
+        }
         if (uneven) {
             a.view_info = view_info.p;
             a.total_pixels = total_pixels;

@@ -39,14 +39,12 @@ constexpr int TILE_W = 8, TILE_H = 4;
 constexpr int WALK_STACK = 64;      // a mesh's tree is at most 60 deep
 
 // A tile's candidate instances as its warp holds them: each one's position in its world's run of sorted
-// leaves and the distance below which no camera ray of the tile can enter its box, collected in leaf order,
-// then sorted by that distance. CAP: the most instances a world holds (32 or TILE_MAX_INSTANCES).
+// leaves and the distance below which no camera ray of the tile can enter its box, in the view's order of those
+// distances (view_order_kernel). CAP: the most instances a world holds (32 or TILE_MAX_INSTANCES).
 template <int CAP>
 struct WarpSmem {
-    int leaf[CAP];           // sorted: the candidates' leaves, smallest entry bound first
+    int leaf[CAP];           // the candidates' leaves, smallest entry bound first (the view's order)
     float bound[CAP];        // and their bounds
-    int leaf_in[CAP];        // collected, in leaf order
-    float bound_in[CAP];
 };
 // CAP 0: worlds of any size, walked as a packet (packet_walk); the warp's stack of the world tree's nodes.
 template <>
@@ -428,6 +426,41 @@ __device__ __forceinline__ TileAt pair_tile_at(const RenderArgs &a, long long ti
     return t;
 }
 
+// One CTA per view: its world's instances in the order the view's tiles walk their candidates, nearest bound first
+// (the eye's distance to the instance's leaf box, 1e-5 under it: no camera ray of the view can enter the box
+// closer), ties by leaf order. The bound depends on the eye alone, so every tile of the view takes this order and
+// keeps only its own candidates.
+template <int CAP>
+__global__ void __launch_bounds__(128) view_order_kernel(const __grid_constant__ SceneParams s, const RenderArgs a) {
+    __shared__ float bound[CAP];
+    const int view = blockIdx.x;
+    const int world = view / a.cameras_per_world;
+    const int P = s.instance_count > 0 ? world_count_of(s, world) : 0;
+    const float4 c0 = __ldg(a.camera_basis + 3 * view);
+    const float3 eye = mk3(c0.x, c0.y, c0.z);
+    const float4 *leaves = world_leaves(s, world);
+    for (int j = threadIdx.x; j < P; j += blockDim.x) {
+        const float4 lo = __ldg(leaves + 2 * j), hi = __ldg(leaves + 2 * j + 1);
+        const float dx = fmaxf(fmaxf(lo.x - eye.x, eye.x - hi.x), 0.0f);
+        const float dy = fmaxf(fmaxf(lo.y - eye.y, eye.y - hi.y), 0.0f);
+        const float dz = fmaxf(fmaxf(lo.z - eye.z, eye.z - hi.z), 0.0f);
+        bound[j] = sqrtf(dx * dx + dy * dy + dz * dz) * 0.99999f;
+    }
+    __syncthreads();
+    int *order = a.view_order + static_cast<long long>(view) * a.order_stride;
+    float *order_bound = a.view_bound + static_cast<long long>(view) * a.order_stride;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const float bi = bound[i];
+        int rank = 0;
+        for (int k = 0; k < P; ++k) {
+            const float bk = bound[k];
+            rank += (bk < bi) || (bk == bi && k < i);
+        }
+        order[rank] = i;
+        order_bound[rank] = bi;
+    }
+}
+
 // A warp's next run of tiles, fetch of them from one atomic (32 rays each; a tuning choice: 1 gives the finest
 // balance at the end of a launch, more fewer atomics); first >= tiles when none are left.
 __device__ __forceinline__ long long fetch_tiles(int *counter, int lane, int fetch) {
@@ -496,7 +529,8 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
             const float sy_hi = fmaxf(sya, syb) + 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));
 
-            // Every instance of the world against the pyramid, 32 at a time: the candidates, in leaf order.
+            // Every instance of the world against the pyramid, 32 at a time, in the view's order (nearest bound
+            // first, ties by leaf order): the candidates, already in the order they are walked.
             const float3 k00 = right * sx_lo + up * sy_lo + fwd, k10 = right * sx_hi + up * sy_lo + fwd;
             const float3 k11 = right * sx_hi + up * sy_hi + fwd, k01 = right * sx_lo + up * sy_hi + fwd;
             const float3 mid = k00 + k11;
@@ -504,12 +538,17 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
 #pragma unroll
             for (int e = 0; e < 4; ++e)
                 if (dot(planes[e], mid) < 0.0f) planes[e] = -planes[e];
+            const int *order = a.view_order + static_cast<long long>(T.view) * a.order_stride;
+            const float *order_bound = a.view_bound + static_cast<long long>(T.view) * a.order_stride;
             __syncwarp();
             for (int base = 0; base < P; base += 32) {
-                const int j = base + lane;
+                const int k = base + lane;
                 bool cand = false;
+                int j = 0;
                 float bound = 0.0f;
-                if (j < P) {
+                if (k < P) {
+                    j = __ldg(order + k);
+                    bound = __ldg(order_bound + k);
                     const float4 lo = __ldg(leaves + 2 * j), hi = __ldg(leaves + 2 * j + 1);
                     const float3 c = mk3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
                     const float3 h = mk3(0.5f * (hi.x - lo.x), 0.5f * (hi.y - lo.y), 0.5f * (hi.z - lo.z));
@@ -522,32 +561,14 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
                         const float reach = dot(n, rel) + abs_dot(n, h) + pad * (fabsf(n.x) + fabsf(n.y) + fabsf(n.z));
                         if (reach < 0.0f) cand = false;
                     }
-                    // No ray of the tile can enter the box closer than the eye's distance to it (the rays are
-                    // unit length); the bound sits 1e-5 below that, far beyond the slab test's rounding.
-                    const float dx = fmaxf(fmaxf(lo.x - eye.x, eye.x - hi.x), 0.0f);
-                    const float dy = fmaxf(fmaxf(lo.y - eye.y, eye.y - hi.y), 0.0f);
-                    const float dz = fmaxf(fmaxf(lo.z - eye.z, eye.z - hi.z), 0.0f);
-                    bound = sqrtf(dx * dx + dy * dy + dz * dz) * 0.99999f;
                 }
                 const unsigned cmask = __ballot_sync(FULL, cand);
                 if (cand) {
                     const int at = ncand + __popc(cmask & below);
-                    sm.leaf_in[at] = j;
-                    sm.bound_in[at] = bound;
+                    sm.leaf[at] = j;
+                    sm.bound[at] = bound;
                 }
                 ncand += __popc(cmask);
-            }
-            __syncwarp();
-            // Sorted by bound (ties by leaf order): each candidate's rank is the number before it.
-            for (int i = lane; i < ncand; i += 32) {
-                const float bi = sm.bound_in[i];
-                int rank = 0;
-                for (int k = 0; k < ncand; ++k) {
-                    const float bk = sm.bound_in[k];
-                    rank += (bk < bi) || (bk == bi && k < i);
-                }
-                sm.leaf[rank] = sm.leaf_in[i];
-                sm.bound[rank] = bi;
             }
             __syncwarp();
             }
@@ -1007,6 +1028,12 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, int *count
         return e;
     }
     if (!a.basis_given) e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
+    if constexpr (CAP > 0) {
+        if (e == cudaSuccess && a.views > 0) {
+            view_order_kernel<CAP><<<static_cast<unsigned>(a.views), 128, 0, stream>>>(s, a);
+            e = cudaGetLastError();
+        }
+    }
     // Both kinds of camera ray: paired 4 x 4 tiles (pair_tile_at).
     const bool paired = t.tile_pairs && a.rgb && aov && (!a.view_info || a.view_pair_tile);
     if (e == cudaSuccess && paired) {
