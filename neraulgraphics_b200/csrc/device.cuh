@@ -112,6 +112,9 @@ struct SceneParams {
     // leaves (leaf node n - 1 + leaf_of[g]).
     const float4 *slot_hull;
     const int *leaf_of;
+    // Per slot (per instance for uneven worlds): a sphere in mesh space holding its mesh (host.h: mesh_sphere), or
+    // w = -1 for none (a mesh rebuilt on the device).
+    const float4 *slot_sphere;
 };
 
 // The first instance of world w, its instance count, and the slot-table entry of its instance g.

@@ -503,6 +503,24 @@ std::array<float, 4> mesh_hull(const ngb_mesh &mesh) {
     return out;
 }
 
+std::array<float, 4> mesh_sphere(const ngb_mesh &mesh) {
+    const int V = mesh.vertex_count;
+    if (V <= 0) return {0.0f, 0.0f, 0.0f, -1.0f};
+    double c[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < V; ++i)
+        for (int k = 0; k < 3; ++k) c[k] += mesh.vertices[3 * i + k];
+    for (int k = 0; k < 3; ++k) c[k] /= V;
+    const float cf[3] = {static_cast<float>(c[0]), static_cast<float>(c[1]), static_cast<float>(c[2])};
+    double radius = 0.0;  // from the float centre, as the kernels hold it
+    for (int i = 0; i < V; ++i) {
+        double d2 = 0.0;
+        for (int k = 0; k < 3; ++k) d2 += (mesh.vertices[3 * i + k] - static_cast<double>(cf[k])) *
+            (mesh.vertices[3 * i + k] - static_cast<double>(cf[k]));
+        radius = std::max(radius, std::sqrt(d2));
+    }
+    return {cf[0], cf[1], cf[2], static_cast<float>(radius * (1.0 + 1e-5) + 1e-30)};
+}
+
 uint8_t srgb_byte(float v) {
     const float x = std::fmin(std::fmax(v, 0.0f), 1.0f);
     const float c = x <= 0.0031308f ? 12.92f * x : 1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f;

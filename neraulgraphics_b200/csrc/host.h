@@ -72,6 +72,10 @@ BuiltMeshes build_meshes(const ngb_scene &s, bool node_capacity = false);
 // not checked (-1).
 std::array<float, 4> mesh_hull(const ngb_mesh &mesh);
 
+// A sphere holding every vertex of the mesh (so every triangle): the vertices' mean (x, y, z) rounded to float, and
+// in w their largest distance from that point, rounded up; -1 for a mesh without vertices.
+std::array<float, 4> mesh_sphere(const ngb_mesh &mesh);
+
 // The sRGB byte of a linear value, (uint8)(saturate(srgb(saturate(v))) * 255 + 0.5) with srgb's 1/2.4 power
 // taken by the host's powf (src/geom_dev.h:169-182, render_core.h:280-282), as 255 thresholds: t[k] (k = 1..255)
 // is the smallest float whose byte is k or more, t[0] = 0. The byte of v is the number of k >= 1 with

@@ -143,7 +143,7 @@ struct Renderer {
     DevBuf<float4> inst, tlas;
     DevBuf<unsigned long long> keys;
     DevBuf<int> sorted_ids, roots, parent, arrivals, leaf_of;
-    DevBuf<float4> slot_hull;
+    DevBuf<float4> slot_hull, slot_sphere;
     // The global build's scratch (worlds of more than MAX_PER_WORLD instances, or when asked for).
     int build_mode = 0;  // 0: automatic, 1: the per-world build, 2: the global build
     DevBuf<float4> large_aabb;
@@ -188,6 +188,7 @@ struct Renderer {
     DevBuf<uint32_t> mesh_indices;
     DevBuf<float> mesh_normals, mesh_stage;
     DevBuf<int> slot_mesh;
+    std::vector<int> slot_mesh_host;
     DevBuf<float> mb_box, mb_centre, mb_node_box;
     DevBuf<uint32_t> mb_order;
     DevBuf<int> mb_lpos, mb_rpos, mb_begin, mb_end, mb_left, mb_depth, mb_index, mb_counter, mb_starts, mb_top, mb_prefix;
@@ -451,6 +452,13 @@ void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
     }
     for (int i = 0; i < slots; ++i) hull_of_slot[i] = hull_of_mesh[s.instances[i].mesh];
     upload(slot_hull, hull_of_slot);
+    std::vector<float4> sphere_of_mesh(s.mesh_count), sphere_of_slot(slots);
+    for (int m = 0; m < s.mesh_count; ++m) {
+        const std::array<float, 4> b = mesh_sphere(s.meshes[m]);
+        sphere_of_mesh[m] = make_float4(b[0], b[1], b[2], b[3]);
+    }
+    for (int i = 0; i < slots; ++i) sphere_of_slot[i] = sphere_of_mesh[s.instances[i].mesh];
+    upload(slot_sphere, sphere_of_slot);
     std::vector<int> tri_base_of_slot(slots);
     for (int i = 0; i < slots; ++i) tri_base_of_slot[i] = mesh_base[s.instances[i].mesh];
     upload(slot_tri_base, tri_base_of_slot);
@@ -482,6 +490,7 @@ void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
         std::vector<int> mesh_of_slot(slots);
         for (int i = 0; i < slots; ++i) mesh_of_slot[i] = s.instances[i].mesh;
         if (slots > 0) upload(slot_mesh, mesh_of_slot);
+        slot_mesh_host = mesh_of_slot;
     }
     tlas_pairs.ensure(4 * std::max<long long>(n - 1, 1));
     upload(slot_bounds, bounds_of_slot);
@@ -512,6 +521,7 @@ void Renderer::init(const ngb_scene &s, const UnevenLayout *layout) {
     params.slot_bounds = slot_bounds.p;
     params.tlas_internal = static_cast<int>(n - 1);
     params.slot_hull = slot_hull.p;
+    params.slot_sphere = slot_sphere.p;
     params.leaf_of = leaf_of.p;
 
     // Every world starts with the transforms the instances were given (src/cuda_backend.cu:765-770).
@@ -567,7 +577,7 @@ void Renderer::teardown() {
     large_keys_a.release(), large_keys_b.release(), large_counts.release();
     pic_hit.release(), shadow_o.release(), shadow_d.release(), pic_code.release(), shadow_self.release();
     view_order.release(), view_bound.release();
-    leaf_of.release(), slot_hull.release();
+    leaf_of.release(), slot_hull.release(), slot_sphere.release();
     camera_basis.release(), srgb_table.release();
     cameras.release(), ray_origins.release(), ray_directions.release(), out_rgb.release(), out_depth.release();
     out_normal.release(), out_id.release(), ray_distance.release(), ray_normal.release(), ray_id.release();
@@ -870,6 +880,12 @@ void Renderer::update_mesh(int mesh, const float *vertices, const float *normals
     // the new tree's last are zero, as at creation); its node count comes back for inspection.
     CK(launch_mesh_build(a, t, slot_mesh.p, slot_mesh.p ? static_cast<int>(slot_mesh.n) : 0, mesh, slot_root.p,
         slot_bounds.p, slot_hull.p, stream));
+    // The new shape has no bounding sphere: its slots' walks go without the sphere test.
+    static const float no_sphere = -1.0f;
+    for (size_t i = 0; i < slot_mesh_host.size(); ++i)
+        if (slot_mesh_host[i] == mesh)
+            CK(cudaMemcpyAsync(reinterpret_cast<float *>(slot_sphere.p + i) + 3, &no_sphere, sizeof(float),
+                cudaMemcpyHostToDevice, stream));
     CK(cudaMemcpyAsync(host_count, t.counter, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CK(cudaEventRecord(ev_done, stream));
     wait(ev_done, timeout);

@@ -74,8 +74,9 @@ __device__ __forceinline__ const float4 *world_leaves(const SceneParams &s, int 
 // and its stack lives in this function's own frame.
 template <bool ANY>
 __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, const float *__restrict__ slot_bounds,
-    const int2 *__restrict__ slot_root, const float4 *__restrict__ pairs, const float4 *__restrict__ tris, int id,
-    float3 o, float3 d, float &tmax, int &hit_tri, float &hu, float &hv, int max_steps, int *err) {
+    const int2 *__restrict__ slot_root, const float4 *__restrict__ pairs, const float4 *__restrict__ tris,
+    const float4 *__restrict__ slot_sphere, int id, float3 o, float3 d, float &tmax, int &hit_tri, float &hu,
+    float &hv, int max_steps, int *err) {
     const float4 *rec = inst + 4 * static_cast<long long>(id);
     InstanceRec r;
     r.r0 = __ldg(rec);
@@ -84,6 +85,15 @@ __device__ __noinline__ bool instance_walk(const float4 *__restrict__ inst, cons
     const int slot = __float_as_int(__ldg(rec + 3).y);
     o = to_local_point(r, o);
     d = to_local_dir(r, d);
+    // A ray that passes farther from the mesh's sphere centre than its radius meets none of its triangles: the
+    // squared distance |m x d|^2 / |d|^2 (m from the centre to the origin), against r^2 with a margin of 1e-3
+    // relative plus 1e-4 |m|^2, far above the float rounding of the products.
+    const float4 sph = __ldg(slot_sphere + slot);
+    if (sph.w > 0.0f) {
+        const float3 m = o - mk3(sph.x, sph.y, sph.z);
+        const float dd = dot(d, d), b = dot(m, d), mm = dot(m, m);
+        if (mm * dd - b * b > (sph.w * sph.w * 1.001f + 1e-4f * mm) * dd) return false;
+    }
     const float3 inv = safe_inverse(d);
     const float *b = slot_bounds + 6 * slot;
     const float4 blo = make_float4(__ldg(b), __ldg(b + 1), __ldg(b + 2), 0.0f);
@@ -189,7 +199,7 @@ __device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpS
         const float4 lo = __ldg(leaf), hi = __ldg(leaf + 1);
         if (reach && box_entry(lo, hi, o, inv, tmax) < NO_HIT) {
             const int id = ~__float_as_int(lo.w);
-            if (instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax, hit_tri,
+            if (instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, s.slot_sphere, id, o, d, tmax, hit_tri,
                     hu, hv, max_steps, err))
                 hit_inst = id;
         }
@@ -209,7 +219,7 @@ __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &s
     const float3 inv = safe_inverse(d);
     // The instance whose leaf box the lane's ray entered: walked by that lane.
     auto walk = [&](int id, bool enters) {
-        if (enters && instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, o, d, tmax,
+        if (enters && instance_walk<false>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, s.slot_sphere, id, o, d, tmax,
                           hit_tri, hu, hv, max_steps, err))
             hit_inst = id;
     };
@@ -915,7 +925,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 if (box_entry(__ldg(leaf), __ldg(leaf + 1), so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, self, so, sd,
+                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, s.slot_sphere, self, so, sd,
                         tm, ht, hu, hv, max_steps, a.error_flag);
                 }
             }
@@ -928,7 +938,7 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) shadow_tiles_kernel(const
                 if (open && id != self && box_entry(lo, hi, so, sinv, sdist) < NO_HIT) {
                     float tm = sdist, hu, hv;
                     int ht;
-                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, id, so, sd, tm,
+                    blocked = instance_walk<true>(s.inst, s.slot_bounds, s.slot_root, s.blas_pairs, s.tris, s.slot_sphere, id, so, sd, tm,
                         ht, hu, hv, max_steps, a.error_flag);
                 }
             }
