@@ -179,6 +179,10 @@ __global__ void __launch_bounds__(G < 128 ? 128 : G) build_worlds_kernel(const B
         } else {
             const float *mi = a.matrices_in + 12 * g;
             for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+            if (a.matrices_out) {  // matrices in the caller's memory: kept for inspection
+                float *mo = a.matrices_out + 12 * g;
+                for (int k = 0; k < 12; ++k) mo[k] = m[k];
+            }
         }
         float inv[12];
         invert_affine(m, inv);
@@ -406,6 +410,10 @@ __global__ void __launch_bounds__(128) place_kernel(const BuildArgs a, float4 *a
     } else {
         const float *mi = a.matrices_in + 12 * g;
         for (int k = 0; k < 12; ++k) m[k] = __ldg(mi + k);
+        if (valid && a.matrices_out) {  // matrices in the caller's memory: kept for inspection
+            float *mo = a.matrices_out + 12 * g;
+            for (int k = 0; k < 12; ++k) mo[k] = m[k];
+        }
     }
     float inv[12];
     invert_affine(m, inv);

@@ -235,6 +235,13 @@ def test_device_inputs_and_zero_copy(torch_cuda):
     assert second.data_ptr() == first.data_ptr() and not torch.equal(first, kept)
     with pytest.raises(ValueError, match="cameras on the GPU need zero_copy=True"):
         dev.render(torch.from_numpy(wl.cameras).cuda(), wl.fov)
+    # Matrices given in device memory are the ones inspection reports, on both builds.
+    moved = wl.matrices.copy()
+    moved[..., 3] += np.float32(0.25)
+    for build in (1, 2):
+        dev.set_build(build)
+        dev.set_instance_transforms(torch.from_numpy(moved).cuda())
+        assert np.array_equal(bits(dev.inspect_tlas()["matrices"].reshape(moved.shape)), bits(moved))
 
 
 def test_body_poses_from_a_gpu_tensor(torch_cuda):
