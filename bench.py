@@ -73,7 +73,10 @@ def workload_config(worlds, extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+    """nvidia-smi clocks and throttle reasons, sampled every 50 ms while running. Entering waits (up to 5 s) for
+    nvidia-smi's first sample, so that its start-up (NVML initialisation, which can hold up this process's launches
+    for milliseconds) ends before the timed region begins; the summary counts only the samples taken after that,
+    or the last earlier one when the region was shorter than one sampling period."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -83,6 +86,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.start = 0
 
     def __enter__(self):
         try:
@@ -93,6 +97,10 @@ class ClockSampler:
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+        end = time.monotonic() + 5.0
+        while self.proc and not self.lines and self.proc.poll() is None and time.monotonic() < end:
+            time.sleep(0.01)
+        self.start = len(self.lines)
         return self
 
     def _read(self):
@@ -110,7 +118,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = self.lines[self.start:] or self.lines[-1:]
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -468,8 +477,9 @@ def run_ours(args, rank, world, local_rank, dist):
                      "issue": issue_figures()},
         "cpu_baseline": cpu,
         # Per step: the tree build (compose + per-world build, inter-world links) and the render: the camera-basis
-        # kernel and the camera, shade and shadow kernels (tile path), or the camera-basis and one render kernel.
-        "gpu_launches": (2 + (4 if len(stage_ms) == 3 else 2)) * K,
+        # kernel, the per-view candidate order and the camera, shade and shadow kernels (tile path), or the
+        # camera-basis and one render kernel.
+        "gpu_launches": (2 + (5 if len(stage_ms) == 3 else 2)) * K,
         "kernel_shape": None if tuned is None else {k: tuned[k] for k in ("kernel", "threads", "registers", "refill",
                                                                             "leaf_batch", "fetch", "paired", "ms")},
         # The renderers' own device arrays (scene, trees, per-pixel scratch; ngb_device_bytes), not the images.
@@ -775,7 +785,7 @@ def uneven_figures(dev, K, W, seed=0, buckets=False):
            "shape_timings_ms": {f"{t['threads']}/{t['registers']} fetch {t['fetch']} "
                                 f"{'paired' if t['paired'] else 'one kind'}": round(t["ms"], 4)
                                 for t in tuned["timings"]},
-           "graph_matches_eager": same, "gpu_launches_per_step": 6,
+           "graph_matches_eager": same, "gpu_launches_per_step": 7,
            "workload": f"uneven_worlds: {views} worlds, {int(first[-1])} instances, {r.pixel_count} pixels; six "
                        "meshes of 12 to 20480 triangles; one light, spp 1, RGB+depth+ID"}
     if not buckets:

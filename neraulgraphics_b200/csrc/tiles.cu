@@ -346,6 +346,19 @@ __device__ __forceinline__ void put_rgb(uint8_t *rgb, long long pix, int bytes) 
 }
 
 
+// i / per and i % per (per > 0), in 32 bits whenever i fits: a 64-bit division is a long instruction
+// sequence, paid once per tile by every kernel that walks tiles.
+__device__ __forceinline__ int split_index(long long i, int per, int &rem) {
+    if (i <= 0xffffffffLL) {
+        const unsigned u = static_cast<unsigned>(i), p = static_cast<unsigned>(per);
+        const unsigned q = u / p;
+        rem = static_cast<int>(u - q * p);
+        return static_cast<int>(q);
+    }
+    rem = static_cast<int>(i % per);
+    return static_cast<int>(i / per);
+}
+
 // The tile kernels' common start: which tile of which view, and the pixel of this lane.
 struct TileAt {
     int view, world, x0, y0, x, y;
@@ -371,11 +384,10 @@ __device__ __forceinline__ TileAt tile_at(const RenderArgs &a, long long tile, i
         row0 = 0;
         row_end = v.y;
     } else {
-        t.view = static_cast<int>(tile / tiles_per_view);
+        t.view = split_index(tile, tiles_per_view, q);
         t.width = a.width;
         t.height = a.height;
         t.aspect = a.aspect;
-        q = static_cast<int>(tile % tiles_per_view);
         first_pixel = static_cast<long long>(t.view) * a.rows * a.width;
         row0 = a.row_first;
         row_end = a.row_first + a.rows;
@@ -416,11 +428,10 @@ __device__ __forceinline__ TileAt pair_tile_at(const RenderArgs &a, long long ti
         row0 = 0;
         row_end = v.y;
     } else {
-        t.view = static_cast<int>(tile / tiles_per_view);
+        t.view = split_index(tile, tiles_per_view, q);
         t.width = a.width;
         t.height = a.height;
         t.aspect = a.aspect;
-        q = static_cast<int>(tile % tiles_per_view);
         first_pixel = static_cast<long long>(t.view) * a.rows * a.width;
         row0 = a.row_first;
         row_end = a.row_first + a.rows;
@@ -530,10 +541,13 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) camera_tiles_kernel(const
             if constexpr (CAP > 0) {
             // The tile's pyramid: the tangent-plane offsets of its pixel edges (every jittered and centre ray of
             // the tile lies inside), widened by 1e-3, and the four side planes through the eye, facing inwards.
-            const float sxa = (2.0f * static_cast<float>(T.x0) / fw - 1.0f) * fs * asp;
-            const float sxb = (2.0f * static_cast<float>(T.x0 + TW) / fw - 1.0f) * fs * asp;
-            const float sya = -(2.0f * static_cast<float>(T.y0) / fh - 1.0f) * fs;
-            const float syb = -(2.0f * static_cast<float>(T.y0 + TH) / fh - 1.0f) * fs;
+            // The offsets need no exact division: their rounding (a few ulp from the fast reciprocal) lies far
+            // inside the widening.
+            const float rw = __fdividef(2.0f, fw), rh = __fdividef(2.0f, fh);
+            const float sxa = (static_cast<float>(T.x0) * rw - 1.0f) * fs * asp;
+            const float sxb = (static_cast<float>(T.x0 + TW) * rw - 1.0f) * fs * asp;
+            const float sya = -(static_cast<float>(T.y0) * rh - 1.0f) * fs;
+            const float syb = -(static_cast<float>(T.y0 + TH) * rh - 1.0f) * fs;
             const float sx_lo = fminf(sxa, sxb) - 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sx_hi = fmaxf(sxa, sxb) + 1e-3f * (1.0f + fabsf(sxa) + fabsf(sxb));
             const float sy_lo = fminf(sya, syb) - 1e-3f * (1.0f + fabsf(sya) + fabsf(syb));

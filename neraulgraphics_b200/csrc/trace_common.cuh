@@ -17,13 +17,28 @@ __device__ __forceinline__ float3 safe_inverse(float3 d) {
     return mk3(recip(x), recip(y), recip(z));
 }
 
-// Slab test (src/mesh_dev.h:66-74): where the ray enters the box, or NO_HIT.
+// The largest and smallest of three (sm_100's three-input max.f32 / min.f32: max(max(a, b), c), one
+// instruction instead of two).
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Slab test (src/mesh_dev.h:66-74): where the ray enters the box, or NO_HIT. The entry is the largest of the
+// three near planes and 0, the exit the smallest of the three far planes and tmax; no operand is a NaN (the
+// inverse direction is finite), so grouping the maxima and minima in threes gives the reference's values.
 __device__ __forceinline__ float box_entry(float4 lo, float4 hi, float3 o, float3 inv_d, float tmax) {
     const float tx0 = (lo.x - o.x) * inv_d.x, tx1 = (hi.x - o.x) * inv_d.x;
     const float ty0 = (lo.y - o.y) * inv_d.y, ty1 = (hi.y - o.y) * inv_d.y;
     const float tz0 = (lo.z - o.z) * inv_d.z, tz1 = (hi.z - o.z) * inv_d.z;
-    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-    const float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    const float tn = max3(fminf(tx0, tx1), fminf(ty0, ty1), fmaxf(fminf(tz0, tz1), 0.0f));
+    const float tf = min3(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fminf(fmaxf(tz0, tz1), tmax));
     return tn <= tf ? tn : NO_HIT;
 }
 
