@@ -507,8 +507,8 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
 /* ---- a tree build that allocates nothing ------------------------------------------------------------- */
 
 /* No counterpart in the reference. The per-world instance-tree build of ngb_set_instance_transforms, for
- * callers that cannot call cudaMalloc: a loop captured into a CUDA graph (no allocation during capture), or
- * a framework whose own pool holds the GPU's memory. Inputs and outputs are the caller's device buffers:
+ * callers that cannot call cudaMalloc, such as a framework whose own pool holds the GPU's memory. Inputs and
+ * outputs are the caller's device buffers:
  * matrices (world_count * P * 12 floats), per slot its mesh's box in mesh space (P * 6) and its mesh's
  * BLAS root (P); out: instance records (n * 16 floats: three world->mesh rows, then blas_root and slot as
  * int bits), keys (n), sorted_ids (n), tlas_nodes ((2n - 1) * 8 words, bvh::TlasNode) and roots
@@ -517,8 +517,8 @@ int ngb_build_meshes(const ngb_mesh *meshes, int32_t mesh_count, int32_t *node_c
  * The build's scratch lives in a static device array of the library: at most 65536 instances over all
  * worlds (and 1024 per world); larger calls return NGB_INVALID_ARGUMENT. Every GPU that loads the library
  * keeps that array (about 0.8 MB) until exit. The first call in a CUDA context (and the first after the
- * calling thread's current context changed, as after cudaDeviceReset) looks up the array's address, so make
- * it before any stream capture. All calls share the array: calls that overlap on the GPU race.
+ * calling thread's current context changed, as after cudaDeviceReset) looks up the array's address on the
+ * host. All calls share the array: calls that overlap on the GPU race.
  * error_word (device memory, 4-byte aligned, or NULL): set to 0 by the call's work on the stream, then to a
  * nonzero code if the build's bottom-up box climb ran past the step limit a valid tree allows (3: within a
  * world, 4: between worlds), which leaves the tree malformed. Read it once the stream has passed the call. */

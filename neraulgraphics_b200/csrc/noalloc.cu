@@ -1,8 +1,6 @@
 // A tree build for callers that cannot allocate device memory.
 //
-// Who needs it: a simulator or RL training loop that captures its whole step (physics, pose compose, the
-// instance-tree rebuild, policy) into a CUDA graph cannot call cudaMalloc while the stream is being
-// captured, and frameworks that reserve most of the GPU for their own memory pool up front (JAX's
+// Who needs it: frameworks that reserve most of the GPU for their own memory pool up front (JAX's
 // preallocation, for one) may find a stray cudaMalloc fails or fragments their pool. Such a caller owns
 // every input and output buffer already, but the build also needs scratch space (each node's parent and an
 // arrival counter per internal node), which the renderer otherwise allocates with cudaMalloc.
@@ -14,8 +12,7 @@
 //   - every GPU that loads this library holds the array (about 0.8 MB) until the process exits;
 //   - the array's device address is looked up by the first call made in a CUDA context (a device's primary
 //     context, or one the caller made current), and again whenever the calling thread's current context is
-//     a different one (after cudaDeviceReset, say); make the first call in a context before any stream capture
-//     begins;
+//     a different one (after cudaDeviceReset, say);
 //   - every call shares the one array: two calls whose work overlaps on the GPU (different streams, or
 //     different host threads, without ordering between them) race and corrupt each other's trees. Order them
 //     on one stream, or serialise them;

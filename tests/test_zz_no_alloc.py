@@ -1,8 +1,7 @@
 """The tree build that allocates nothing (ngb_build_tlas_noalloc), against the renderer's own build.
 
-This entry point serves callers that cannot call cudaMalloc -- a step captured into a CUDA graph, or a
-framework that owns the GPU's memory through its own pool -- so its scratch lives in a static device array
-instead. Here the test allocates the inputs and outputs (with PyTorch) and checks that two calls in a row
+This entry point serves callers that cannot call cudaMalloc, such as a framework that owns the GPU's memory
+through its own pool, so its scratch lives in a static device array instead. Here the test allocates the inputs and outputs (with PyTorch) and checks that two calls in a row
 give exactly the trees ngb_set_instance_transforms builds for the same matrices, and that the caller's error
 word reads 0 after each (a build whose box climb overran would set it). It sorts last, so a run that
 stops at its first failure has run every other test first, and it passes alone in a fresh process as well.
