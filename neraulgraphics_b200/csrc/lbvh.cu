@@ -439,8 +439,33 @@ __global__ void __launch_bounds__(128) place_kernel(const BuildArgs a, float4 *a
         aabb[2 * g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
         aabb[2 * g + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
     }
-    // The world's centre bounds: a warp whose lanes all sit in one world (a large world's case) reduces first
-    // and adds one atomic per bound; otherwise every lane adds its own.
+    // The world's centre bounds: a block whose instances all sit in one world (a large world's case) reduces
+    // them in shared memory and adds one atomic per bound; else a warp in one world reduces first and adds one
+    // atomic per bound; otherwise every lane adds its own. (Same-address atomics serialise: 100,000 instances
+    // of one world made 19,000 of them per build with one per warp.)
+    const long long first = blockIdx.x * static_cast<long long>(blockDim.x);
+    const long long wb = (first < a.n ? first : a.n - 1) / a.per_world;
+    if (__syncthreads_and(w == wb)) {
+        __shared__ int red[32][6];  // per warp: the three minima, then the three maxima
+        const int warp = threadIdx.x >> 5;
+        for (int ax = 0; ax < 3; ++ax) {
+            const int c = to_ordered(0.5f * (lo[ax] + hi[ax]));
+            const int mn = __reduce_min_sync(0xffffffffu, c), mx = __reduce_max_sync(0xffffffffu, c);
+            if ((threadIdx.x & 31) == 0) {
+                red[warp][ax] = mn;
+                red[warp][3 + ax] = mx;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            const int k = threadIdx.x;
+            int v = red[0][k];
+            for (int q = 1; q < static_cast<int>(blockDim.x >> 5); ++q) v = k < 3 ? min(v, red[q][k]) : max(v, red[q][k]);
+            if (k < 3) atomicMin(&bounds[6 * w + k], v);
+            else atomicMax(&bounds[6 * w + k], v);
+        }
+        return;
+    }
     const bool one_world = __all_sync(0xffffffffu, w == __shfl_sync(0xffffffffu, w, 0));
     for (int ax = 0; ax < 3; ++ax) {
         int cmin = to_ordered(0.5f * (lo[ax] + hi[ax])), cmax = cmin;
@@ -477,8 +502,11 @@ __global__ void __launch_bounds__(128) keys_kernel(const BuildArgs a, const floa
     ids_sort[g] = static_cast<int>(g);
 }
 
-constexpr int SORT_BLOCK = 1024;  // keys per block of a radix pass, one per thread
-constexpr int RADIX = 256;        // 8-bit digits
+constexpr int SORT_BLOCK = 1024;   // threads per block of a radix pass
+constexpr int SORT_ROUNDS = 2;     // runs of SORT_BLOCK consecutive keys per block, taken in order
+constexpr long long SORT_TILE = static_cast<long long>(SORT_BLOCK) * SORT_ROUNDS;  // keys per block
+constexpr int RADIX = 256;         // 8-bit digits
+constexpr int SCAN_ITEMS = 16;     // consecutive counts per thread in the scan
 
 // Radix pass, step 1: each block's count of each digit, stored digit-major (counts[digit * blocks + block]),
 // so that one exclusive scan gives every (digit, block) its first output position.
@@ -487,24 +515,33 @@ __global__ void __launch_bounds__(SORT_BLOCK) radix_count_kernel(const unsigned 
     __shared__ unsigned hist[RADIX];
     if (threadIdx.x < RADIX) hist[threadIdx.x] = 0;
     __syncthreads();
-    const long long i = blockIdx.x * static_cast<long long>(SORT_BLOCK) + threadIdx.x;
-    if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (RADIX - 1)], 1u);
+    const long long start = blockIdx.x * SORT_TILE;
+    for (int r = 0; r < SORT_ROUNDS; ++r) {
+        const long long i = start + static_cast<long long>(r) * SORT_BLOCK + threadIdx.x;
+        if (i < n) atomicAdd(&hist[(keys[i] >> shift) & (RADIX - 1)], 1u);
+    }
     __syncthreads();
     if (threadIdx.x < RADIX) counts[static_cast<long long>(threadIdx.x) * blocks + blockIdx.x] = hist[threadIdx.x];
 }
 
 // Radix pass, step 2: exclusive prefix sum of the counts in place, one block: the block walks the array in
-// chunks of 1024 (coalesced), each chunk scanned with warp shuffles and a scan of the 32 warp totals.
+// chunks of 1024 x SCAN_ITEMS, each thread summing its SCAN_ITEMS consecutive counts, the thread sums scanned
+// with warp shuffles and a scan of the 32 warp totals (one chunk holds the counts of 1,600 blocks of keys).
 __global__ void __launch_bounds__(1024) radix_scan_kernel(unsigned *counts, long long total) {
     __shared__ unsigned warp_sum[32];
     __shared__ unsigned carry;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (long long base = 0; base < total; base += 1024) {
-        const long long k = base + threadIdx.x;
-        const unsigned v = k < total ? counts[k] : 0u;
-        unsigned x = v;  // inclusive scan within the warp
+    for (long long base = 0; base < total; base += 1024LL * SCAN_ITEMS) {
+        const long long k0 = base + static_cast<long long>(threadIdx.x) * SCAN_ITEMS;
+        unsigned v[SCAN_ITEMS], sum = 0;
+#pragma unroll
+        for (int j = 0; j < SCAN_ITEMS; ++j) {
+            v[j] = k0 + j < total ? counts[k0 + j] : 0u;
+            sum += v[j];
+        }
+        unsigned x = sum;  // inclusive scan of the thread sums within the warp
         for (int off = 1; off < 32; off <<= 1) {
             const unsigned y = __shfl_up_sync(0xffffffffu, x, off);
             if (lane >= off) x += y;
@@ -520,36 +557,54 @@ __global__ void __launch_bounds__(1024) radix_scan_kernel(unsigned *counts, long
             warp_sum[lane] = t;  // inclusive over the warps
         }
         __syncthreads();
-        const unsigned before = carry + (warp > 0 ? warp_sum[warp - 1] : 0u) + x - v;
-        if (k < total) counts[k] = before;
+        unsigned run = carry + (warp > 0 ? warp_sum[warp - 1] : 0u) + x - sum;
+#pragma unroll
+        for (int j = 0; j < SCAN_ITEMS; ++j) {
+            if (k0 + j < total) counts[k0 + j] = run;
+            run += v[j];
+        }
         __syncthreads();
-        if (threadIdx.x == 1023) carry = before + v;
+        if (threadIdx.x == 1023) carry = run;
         __syncthreads();
     }
 }
 
-// Radix pass, step 3: every key to its position, stable: its block's first position for its digit, plus the
-// keys of that digit before it in the block (in earlier warps, counted in shared memory, and earlier lanes of
-// its own warp, from the lanes holding the same digit).
+// Radix pass, step 3: every key to its position, stable: its block's running position for its digit (the
+// block's first position, advanced by the digit's keys of the block's earlier rounds), plus the keys of that
+// digit before it in the round (in earlier warps, counted in shared memory, and earlier lanes of its own warp,
+// from the lanes holding the same digit).
 __global__ void __launch_bounds__(SORT_BLOCK) radix_scatter_kernel(const unsigned long long *keys_in, const int *ids_in,
     unsigned long long *keys_out, int *ids_out, long long n, int shift, const unsigned *offsets, int blocks) {
     __shared__ unsigned warp_count[SORT_BLOCK / 32][RADIX];
+    __shared__ unsigned next[RADIX];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = threadIdx.x; k < (SORT_BLOCK / 32) * RADIX; k += SORT_BLOCK) (&warp_count[0][0])[k] = 0;
-    __syncthreads();
-    const long long i = blockIdx.x * static_cast<long long>(SORT_BLOCK) + threadIdx.x;
-    const bool valid = i < n;
-    const unsigned long long key = valid ? keys_in[i] : 0ull;
-    const int digit = valid ? static_cast<int>((key >> shift) & (RADIX - 1)) : RADIX;
-    const unsigned peers = __match_any_sync(0xffffffffu, digit);
-    const unsigned rank_in_warp = __popc(peers & ((1u << lane) - 1u));
-    if (valid && rank_in_warp == 0) warp_count[warp][digit] = __popc(peers);
-    __syncthreads();
-    if (!valid) return;
-    unsigned pos = offsets[static_cast<long long>(digit) * blocks + blockIdx.x] + rank_in_warp;
-    for (int w = 0; w < warp; ++w) pos += warp_count[w][digit];
-    keys_out[pos] = key;
-    ids_out[pos] = ids_in[i];
+    if (threadIdx.x < RADIX) next[threadIdx.x] = offsets[static_cast<long long>(threadIdx.x) * blocks + blockIdx.x];
+    const long long start = blockIdx.x * SORT_TILE;
+    for (int r = 0; r < SORT_ROUNDS; ++r) {
+        for (int k = threadIdx.x; k < (SORT_BLOCK / 32) * RADIX; k += SORT_BLOCK) (&warp_count[0][0])[k] = 0;
+        __syncthreads();
+        const long long i = start + static_cast<long long>(r) * SORT_BLOCK + threadIdx.x;
+        const bool valid = i < n;
+        const unsigned long long key = valid ? keys_in[i] : 0ull;
+        const int digit = valid ? static_cast<int>((key >> shift) & (RADIX - 1)) : RADIX;
+        const unsigned peers = __match_any_sync(0xffffffffu, digit);
+        const unsigned rank_in_warp = __popc(peers & ((1u << lane) - 1u));
+        if (valid && rank_in_warp == 0) warp_count[warp][digit] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            unsigned pos = next[digit] + rank_in_warp;
+            for (int w = 0; w < warp; ++w) pos += warp_count[w][digit];
+            keys_out[pos] = key;
+            ids_out[pos] = ids_in[i];
+        }
+        __syncthreads();
+        if (threadIdx.x < RADIX) {
+            unsigned t = 0;
+            for (int w = 0; w < SORT_BLOCK / 32; ++w) t += warp_count[w][threadIdx.x];
+            next[threadIdx.x] += t;
+        }
+        __syncthreads();  // the sums are read before the next round clears the counts
+    }
 }
 
 // The leaves in sorted order (make_leaves, cuda_tlas.cuh:162-175), the sorted ids, and each world of one
@@ -660,7 +715,7 @@ cudaError_t launch_group(const BuildArgs &a, cudaStream_t stream) {
 
 }  // namespace
 
-int large_sort_blocks(long long n) { return static_cast<int>((n + SORT_BLOCK - 1) / SORT_BLOCK); }
+int large_sort_blocks(long long n) { return static_cast<int>((n + SORT_TILE - 1) / SORT_TILE); }
 
 cudaError_t launch_build_large(const BuildArgs &a, const LargeBuildScratch &t, cudaStream_t stream) {
     if (a.n == 0) return cudaSuccess;
