@@ -47,3 +47,46 @@ def test_reference_arm_without_a_counterpart_says_why():
 
 def test_reference_arm_on_a_rank_other_than_0_prints_nothing():
     assert run(["--impl", "reference", "--steps", "1", "--warmup", "0"], env={"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def _bench():
+    sys.path.insert(0, ROOT)
+    import bench
+    return bench
+
+
+def test_clock_summary_takes_the_samples_of_the_timed_region():
+    """nvidia-smi lines (index, clocks.sm, clocks.max.sm, power, active mask, then hw_slowdown,
+    hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap): only those from the timed region's start count, or
+    the last one before it when the region was shorter than one sampling period."""
+    c = _bench().ClockSampler(0)
+    c.lines = ["0, 1200, 1965, 300.0, 0x0, Not Active, Not Active, Not Active, Not Active",
+               "0, 1965, 1965, 900.5, 0x4, Not Active, Not Active, Not Active, Active",
+               "0, 1950, 1965, 950.0, 0x4, Not Active, Not Active, Not Active, Active",
+               "garbled"]
+    c.start = 1
+    assert c.summary() == {"sm_mhz": 1957.5, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 2}
+    c.lines = c.lines[:3]
+    c.start = 3
+    s = c.summary()
+    assert s["samples"] == 1 and s["sm_mhz"] == 1950.0
+    c.lines, c.start = [], 0
+    assert c.summary()["samples"] == 0
+
+
+def test_algorithmic_bytes_and_profile_figures_the_bench_reports():
+    """B_img of the body-worlds image (outputs, inputs and tree build, counted once; 52,068 bytes) and the
+    camera kernel's ncu figures the bench line carries, read from the committed profile."""
+    import neraulgraphics_b200 as ng
+    from neraulgraphics_b200 import workloads
+    bench = _bench()
+    wl = workloads.body_worlds(worlds=4096, seed=0)
+    built = ng.build_meshes(wl.desc.meshes)
+    b = bench.algorithmic_bytes_per_image(wl, built["nodes"].nbytes + built["triangles"].nbytes)
+    assert round(b) == 52068
+    assert 64 * 64 * 11 < b < 64 * 64 * 11 + 8000
+    traffic = bench.traffic_per_image()
+    assert traffic is not None and 45056 <= traffic < 1e6
+    f = bench.issue_figures()
+    assert 0 < f["threads_per_warp_instruction"] <= 32 and 0 < f["issue_active_pct"] <= 100
+    assert 0 < f["warps_active_pct"] <= 100
