@@ -208,7 +208,7 @@ __device__ __forceinline__ void closest_meshes(const SceneParams &s, const WarpS
 // A world's tree walked by the whole warp together (a packet), for the camera rays of worlds too large for
 // candidate lists: every internal node that some lane's ray enters before its closest hit so far is visited
 // once for all lanes, from child-pair records, the child the lanes enter first (least entry distance over the
-// lanes) before the other; an instance whose box a lane's ray enters is walked by that lane (instance_walk).
+// lanes) before the other; an instance whose box a lane's ray enters is walked by that lane (instance_walk_body).
 // Each lane gets the hit its own walk of the tree finds, up to which of two equally distant hits is kept (the
 // instance order differs from a single ray's). The stack lives in the warp's shared memory.
 __device__ __forceinline__ void packet_walk(const SceneParams &s, WarpSmem<0> &sm, int lane, int world, bool active,
