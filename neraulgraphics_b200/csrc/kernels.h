@@ -153,9 +153,6 @@ struct PersistentTuning {
 cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, int *counter,
     const PersistentTuning &t, cudaStream_t stream);
 // Ray queries on the persistent kernel: each lane a ray, refilled from the queue as its walk ends.
-// The shadow rays a tile render's shade kernel left (shadow_o / shadow_d per pixel), as persistent-kernel jobs
-// with lane refill; each writes its pixel's RGB (rgb from pic_code when blocked, else shadow_d.w).
-cudaError_t launch_shadows_persistent(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream);
 cudaError_t launch_rays_persistent(const SceneParams &s, const RayArgs &r, int *counter, const PersistentTuning &t,
     cudaStream_t stream);
 // Ray queries as warp packets over each world's tree: 32 consecutive rays of a world per warp (see tiles.cu).

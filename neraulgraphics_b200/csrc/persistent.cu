@@ -33,9 +33,8 @@ using namespace tr;
 constexpr int STACK = 128;
 constexpr int MARKER = INT_MIN;   // stack entry that returns the walk from a mesh to its world's tree
 constexpr int ST_IDLE = 0, ST_WALK = 1, ST_DONE = 2;
-constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3, JOB_RAY = 4, JOB_SHADOW_PIXEL = 5;
+constexpr int JOB_RGB = 1, JOB_SHADOW = 2, JOB_AOV = 3, JOB_RAY = 4;
 constexpr int KINDS_RAYS = 4;     // a launch of ray queries (cast_rays) instead of views
-constexpr int KINDS_SHADOWS = 5;  // a launch of the shadow rays the tile render's shade kernel left per pixel
 constexpr unsigned FULL = 0xffffffffu;
 
 // A lane's hot state, in registers: the current ray (world space, or mesh space inside an instance), the
@@ -232,27 +231,6 @@ __device__ __forceinline__ void walk_leaf(const SceneParams &s, Lane &L, const C
 // then (when both are asked for) the picture ray and the centre ray of a pixel.
 __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs &a, const RayArgs &ra, Lane &L,
     const ColdRef &cold, long long item, int kinds, int tiles_x, int tiles_per_view) {
-    if (kinds == KINDS_SHADOWS) {
-        // Pixel item's shadow ray, if the shade kernel left one (origin, light distance in shadow_o; direction
-        // in shadow_d): any hit in the meshes, spheres and the floor having been tested there.
-        const float4 o4 = a.shadow_o[item];
-        if (!(o4.w > 0.0f)) {
-            L.state = ST_IDLE;
-            return;
-        }
-        const float4 d4 = a.shadow_d[item];
-        L.job = JOB_SHADOW_PIXEL;
-        cold.put_pix(item);
-        const int view = a.view_info ? view_of(a.view_info, a.views, item, false)
-                                     : static_cast<int>(item / (static_cast<long long>(a.width) * a.rows));
-        L.world = view / a.cameras_per_world;
-        L.o = mk3(o4.x, o4.y, o4.z);
-        L.d = mk3(d4.x, d4.y, d4.z);
-        L.tmax = o4.w;
-        L.any = true;
-        start_walk(s, L);
-        return;
-    }
     if (kinds == KINDS_RAYS) {
         // A ray query (cast_ray, src/render_core.h:331-349): the direction normalised, a miss if its length is
         // out of range; spheres and the floor, then the meshes; a hit beyond max_distance is a miss.
@@ -365,20 +343,6 @@ __device__ __forceinline__ void start_job(const SceneParams &s, const RenderArgs
 __device__ __forceinline__ void complete(const SceneParams &s, const RenderArgs &a, const RayArgs &ra, Lane &L,
     const ColdRef &cold) {
     const long long pix = cold.pix();
-    if (L.job == JOB_SHADOW_PIXEL && a.radiance) {  // a single-view render: the shadowed radiance, over pic_hit
-        if (L.blocked) a.radiance[pix] = a.pic_hit[pix];
-        L.state = ST_IDLE;
-        return;
-    }
-    if (L.job == JOB_SHADOW_PIXEL) {  // the shade kernel's bytes: shadowed over pic_code, lit in shadow_d.w
-        const int bytes = L.blocked ? a.pic_code[pix] : __float_as_int(a.shadow_d[pix].w);
-        uint8_t *o = a.rgb + 3 * static_cast<size_t>(pix);
-        o[0] = static_cast<uint8_t>(bytes);
-        o[1] = static_cast<uint8_t>(bytes >> 8);
-        o[2] = static_cast<uint8_t>(bytes >> 16);
-        L.state = ST_IDLE;
-        return;
-    }
     if (L.job == JOB_SHADOW) {
         write_rgb(s.srgb_table, a.rgb, pix, cold.get3(L.blocked ? C_SHADOW : C_LIT));
         L.state = ST_IDLE;
@@ -573,14 +537,12 @@ __global__ void __launch_bounds__(THREADS, MIN_BLOCKS) render_persistent_kernel(
 
 template <int THREADS, int MIN_BLOCKS>
 cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayArgs *rays, int *counter, int refill,
-    int leaf_batch, cudaStream_t stream, bool shadows = false) {
+    int leaf_batch, cudaStream_t stream) {
     const int tiles_x = (a.width + 3) / 4, tiles_y = (a.rows + 3) / 4;
     const int tiles_per_view = tiles_x * tiles_y;
-    const int kinds = shadows ? KINDS_SHADOWS : rays ? KINDS_RAYS
-        : (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
+    const int kinds = rays ? KINDS_RAYS : (a.rgb ? 1 : 0) | ((a.depth || a.normal || a.object_id || a.hit_instance) ? 2 : 0);
     if (kinds == 0) return cudaSuccess;
-    const long long total = shadows ? (a.view_info ? a.total_pixels : static_cast<long long>(a.views) * a.width * a.rows)
-        : rays ? rays->count : 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
+    const long long total = rays ? rays->count : 16LL * tiles_per_view * a.views * (kinds == 3 ? 2 : 1);
     if (total == 0) return cudaSuccess;
     const RayArgs ra = rays ? *rays : RayArgs{};
     auto kernel = render_persistent_kernel<THREADS, MIN_BLOCKS>;
@@ -597,7 +559,7 @@ cudaError_t launch_variant(const SceneParams &s, const RenderArgs &a, const RayA
     if (blocks > needed) blocks = needed;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    if (!rays && !shadows) {
+    if (!rays) {
         if (!a.basis_given) e = launch_prepare_cameras(a.cameras, a.views, a.camera_basis, stream);
         if (e != cudaSuccess) return e;
     }
@@ -628,12 +590,6 @@ cudaError_t launch_render_persistent(const SceneParams &s, const RenderArgs &a, 
 cudaError_t launch_rays_persistent(const SceneParams &s, const RayArgs &r, int *counter, const PersistentTuning &t,
     cudaStream_t stream) {
     return launch_persistent(s, RenderArgs{}, &r, counter, t, stream);
-}
-
-cudaError_t launch_shadows_persistent(const SceneParams &s, const RenderArgs &a, int *counter, cudaStream_t stream) {
-    // Shadow rays are ray queries: the shape measured best for them (256 threads, 64 registers, a refill at
-    // 28 free lanes, no leaf batching).
-    return launch_variant<256, 4>(s, a, nullptr, counter, 28, 1, stream, true);
 }
 
 }  // namespace ngb
